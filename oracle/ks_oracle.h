@@ -1,0 +1,84 @@
+/*
+ * ks_oracle.h -- C interface of the CPU f64 oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY. The oracle is a single-threaded (optionally OpenMP)
+ * f64 restatement of the reference's CPU Kohn-Sham solver, crate `qm`
+ * (crates/qm/src/{grid,stencil,xc,nuclear,poisson,eigen,scf,forces}.rs). It is the
+ * checker of the CUDA solver: only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline / reference arm may load it. The product never calls it.
+ *
+ * Grid layout of every array here: the reference's `qm::Grid`, idx = i + n*(j + n*k),
+ * cubic n^3, origin = -(n-1)h/2 on every axis (crates/qm/src/grid.rs:1-16).
+ */
+#ifndef KS_ORACLE_H
+#define KS_ORACLE_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { double pos[3]; int z; } ora_nucleus;
+
+/* Settings of one SCF (crates/qm/src/scf.rs:375 ScfSettings, Aufbau occupations only). */
+typedef struct {
+    double sigma, tol, mixing, eig_tol;
+    int max_iter, diis_history, stall_window;
+} ora_settings;
+
+typedef struct {
+    int iterations;
+    double delta_rho;
+    double kinetic, external_, hartree, xc, nuclear, total;
+    double boundary_density, max_eigen_residual, poisson_residual;
+    int poisson_iterations;
+    double electrons[2];
+    int status;          /* 0 ok, 1 not converged, 2 stalled, 3 coincident nuclei */
+} ora_stats;
+
+/* thread count for the parallel loops (stencils, pointwise); sums stay sequential */
+void ora_set_threads(int n);
+
+/* ---- grid and pointwise pieces ---- */
+double ora_neumaier(const double* v, size_t n);
+void ora_laplacian(int n, double h, const double* f, double* out);
+void ora_hamiltonian(int n, double h, const double* f, const double* v, double* out);
+void ora_exc_point(double nu, double nd, double* e, double* vu, double* vd);
+void ora_lsda(size_t len, const double* nu, const double* nd, double* e, double* vu, double* vd);
+void ora_nuclear_potential(int n, double h, const ora_nucleus* nuc, int nn, double sigma, double* out);
+void ora_deposit_charge(int n, double h, const ora_nucleus* nuc, int nn, double sigma, double* out);
+int  ora_nuclear_repulsion(const ora_nucleus* nuc, int nn, double* e);
+void ora_initial_orbitals(int n, double h, const ora_nucleus* nuc, int nn, int k, unsigned long long seed, double* out);
+void ora_solid_harmonics(const double r[3], double out[49]);
+double ora_jacobi_omega(void);
+void ora_jacobi_precond(int n, double h, const double* v, double lambda, const double* r, double* w);
+
+/* ---- sub-solvers ---- */
+/* Jacobi-CG Poisson with l<=6 multipole ghosts; v is guess and output. Returns iterations. */
+int ora_poisson_solve(int n, double h, const double* rho, double* v, double tol, int max_iter, double* residual);
+void ora_multipole_moments(int n, double h, const double* rho, double q[49]);
+/* LOBPCG (MGS-orthonormalised [X,W,P], Jacobi preconditioner at lambda when precond != 0). */
+int ora_lobpcg(int n, double h, const double* v, int k, double* x, double* evals, int precond, double lambda,
+               double tol, int max_iter, double* max_residual);
+/* Cyclic Jacobi symmetric eigen-decomposition (column-major evecs), unsorted like the reference's. */
+void ora_sym_eigen(int m, const double* a, double* evals, double* evecs);
+/* bordered Pulay system on a Gram matrix (m x m row-major). Returns 1 and c on success. */
+int ora_diis_coefficients(int m, const double* gram, double* c);
+
+/* ---- SCF, state and forces ---- */
+typedef struct ora_state ora_state;
+/* Runs the Aufbau SCF. warm may be NULL. Returns a new state (owned by the caller) or NULL on
+   coincident nuclei; stats->status carries convergence. */
+ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, int n_dn,
+                   const ora_settings* s, const ora_state* warm, ora_stats* stats);
+void ora_state_free(ora_state* st);
+int  ora_state_counts(const ora_state* st, int* n_up, int* n_dn);
+void ora_state_evals(const ora_state* st, double* up, double* dn);
+void ora_state_density(const ora_state* st, double* rho_up, double* rho_dn);
+void ora_state_potentials(const ora_state* st, double* v_nuc, double* v_h);
+void ora_state_orbitals(const ora_state* st, int spin, double* out);
+int  ora_forces(const ora_state* st, const ora_nucleus* nuc, int nn, double sigma, double* out3n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,276 @@
+"""ctypes binding of the CPU f64 oracle (``oracle/libksoracle.so``).
+
+TEST INFRASTRUCTURE ONLY: the oracle checks the CUDA solver. It is loaded by ``tests/``,
+``__graft_entry__.smoke()`` and the CPU legs of ``bench.py`` and by nothing in the product.
+Array layout is the reference's ``qm::Grid``: a flat n^3 array, idx = i + n*(j + n*k)
+(crates/qm/src/grid.rs:1-16).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libksoracle.so")
+
+
+class Nucleus(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_double * 3), ("z", ctypes.c_int)]
+
+
+class Settings(ctypes.Structure):
+    _fields_ = [("sigma", ctypes.c_double), ("tol", ctypes.c_double), ("mixing", ctypes.c_double),
+                ("eig_tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("diis_history", ctypes.c_int),
+                ("stall_window", ctypes.c_int)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("delta_rho", ctypes.c_double),
+                ("kinetic", ctypes.c_double), ("external", ctypes.c_double), ("hartree", ctypes.c_double),
+                ("xc", ctypes.c_double), ("nuclear", ctypes.c_double), ("total", ctypes.c_double),
+                ("boundary_density", ctypes.c_double), ("max_eigen_residual", ctypes.c_double),
+                ("poisson_residual", ctypes.c_double), ("poisson_iterations", ctypes.c_int),
+                ("electrons", ctypes.c_double * 2), ("status", ctypes.c_int)]
+
+
+def build():
+    """Compiles the oracle in place (make)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "ks_oracle.cpp")):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.ora_neumaier.restype = ctypes.c_double
+        L.ora_jacobi_omega.restype = ctypes.c_double
+        L.ora_scf.restype = ctypes.c_void_p
+        L.ora_scf.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                              ctypes.POINTER(Settings), ctypes.c_void_p, ctypes.POINTER(Stats)]
+        L.ora_state_free.argtypes = [ctypes.c_void_p]
+        L.ora_state_counts.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.ora_state_evals.argtypes = [ctypes.c_void_p, dp, dp]
+        L.ora_state_density.argtypes = [ctypes.c_void_p, dp, dp]
+        L.ora_state_potentials.argtypes = [ctypes.c_void_p, dp, dp]
+        L.ora_state_orbitals.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+        L.ora_forces.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, dp]
+        _lib = L
+    return _lib
+
+
+def set_threads(n):
+    lib().ora_set_threads(int(n))
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _f64(a, size=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if size is not None:
+        assert a.size == size, (a.size, size)
+    return a
+
+
+def nuclei_array(nuclei):
+    """[(x, y, z, Z), ...] -> ctypes array of Nucleus."""
+    arr = (Nucleus * max(len(nuclei), 1))()
+    for i, (x, y, z, Z) in enumerate(nuclei):
+        arr[i].pos[0], arr[i].pos[1], arr[i].pos[2] = x, y, z
+        arr[i].z = int(Z)
+    return arr
+
+
+def grid_points(n, h):
+    """(x, y, z) coordinate arrays of the cubic grid, flat in the reference's order."""
+    half = (n - 1) * h / 2.0
+    c = -half + np.arange(n) * h
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    return x.ravel(), y.ravel(), z.ravel()
+
+
+def neumaier(v):
+    v = _f64(v)
+    return lib().ora_neumaier(_p(v), ctypes.c_size_t(v.size))
+
+
+def laplacian(n, h, f):
+    f = _f64(f, n ** 3)
+    out = np.empty_like(f)
+    lib().ora_laplacian(n, ctypes.c_double(h), _p(f), _p(out))
+    return out
+
+
+def hamiltonian(n, h, f, v):
+    f, v = _f64(f, n ** 3), _f64(v, n ** 3)
+    out = np.empty_like(f)
+    lib().ora_hamiltonian(n, ctypes.c_double(h), _p(f), _p(v), _p(out))
+    return out
+
+
+def lsda(nu, nd):
+    nu, nd = _f64(nu), _f64(nd)
+    e, vu, vd = np.empty_like(nu), np.empty_like(nu), np.empty_like(nu)
+    lib().ora_lsda(ctypes.c_size_t(nu.size), _p(nu), _p(nd), _p(e), _p(vu), _p(vd))
+    return e, vu, vd
+
+
+def exc_point(nu, nd):
+    e, vu, vd = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    lib().ora_exc_point(ctypes.c_double(nu), ctypes.c_double(nd), ctypes.byref(e), ctypes.byref(vu), ctypes.byref(vd))
+    return e.value, vu.value, vd.value
+
+
+def nuclear_potential(n, h, nuclei, sigma):
+    out = np.empty(n ** 3)
+    lib().ora_nuclear_potential(n, ctypes.c_double(h), nuclei_array(nuclei), len(nuclei), ctypes.c_double(sigma), _p(out))
+    return out
+
+
+def deposit_charge(n, h, nuclei, sigma):
+    out = np.empty(n ** 3)
+    lib().ora_deposit_charge(n, ctypes.c_double(h), nuclei_array(nuclei), len(nuclei), ctypes.c_double(sigma), _p(out))
+    return out
+
+
+def nuclear_repulsion(nuclei):
+    e = ctypes.c_double()
+    rc = lib().ora_nuclear_repulsion(nuclei_array(nuclei), len(nuclei), ctypes.byref(e))
+    if rc != 0:
+        raise ValueError("coincident nuclei")
+    return e.value
+
+
+def initial_orbitals(n, h, nuclei, k, seed):
+    out = np.empty(max(k, 1) * n ** 3)
+    lib().ora_initial_orbitals(n, ctypes.c_double(h), nuclei_array(nuclei), len(nuclei), k, ctypes.c_ulonglong(seed), _p(out))
+    return out[: k * n ** 3].reshape(k, n ** 3)
+
+
+def solid_harmonics(r):
+    rr = _f64(r, 3)
+    out = np.empty(49)
+    lib().ora_solid_harmonics(_p(rr), _p(out))
+    return out
+
+
+def jacobi_omega():
+    return lib().ora_jacobi_omega()
+
+
+def jacobi_precond(n, h, v, lam, r):
+    v, r = _f64(v, n ** 3), _f64(r, n ** 3)
+    w = np.empty_like(r)
+    lib().ora_jacobi_precond(n, ctypes.c_double(h), _p(v), ctypes.c_double(lam), _p(r), _p(w))
+    return w
+
+
+def poisson_solve(n, h, rho, v0=None, tol=1e-10, max_iter=5000):
+    rho = _f64(rho, n ** 3)
+    v = np.zeros(n ** 3) if v0 is None else _f64(v0, n ** 3).copy()
+    res = ctypes.c_double()
+    it = lib().ora_poisson_solve(n, ctypes.c_double(h), _p(rho), _p(v), ctypes.c_double(tol), max_iter, ctypes.byref(res))
+    return v, it, res.value
+
+
+def multipole_moments(n, h, rho):
+    rho = _f64(rho, n ** 3)
+    q = np.empty(49)
+    lib().ora_multipole_moments(n, ctypes.c_double(h), _p(rho), _p(q))
+    return q
+
+
+def lobpcg(n, h, v, x0, tol=1e-6, max_iter=500, precond_lambda=None):
+    x = _f64(x0).copy()
+    k = x.shape[0]
+    ev = np.empty(k)
+    mr = ctypes.c_double()
+    it = lib().ora_lobpcg(n, ctypes.c_double(h), _p(_f64(v, n ** 3)), k, _p(x), _p(ev), int(precond_lambda is not None),
+                          ctypes.c_double(precond_lambda or 0.0), ctypes.c_double(tol), max_iter, ctypes.byref(mr))
+    if it < 0:
+        raise RuntimeError("oracle lobpcg lost rank")
+    return ev, x, it, mr.value
+
+
+def sym_eigen(a):
+    a = _f64(a)
+    m = a.shape[0]
+    ev, vec = np.empty(m), np.empty(m * m)
+    lib().ora_sym_eigen(m, _p(a), _p(ev), _p(vec))
+    return ev, vec.reshape(m, m).T  # columns are eigenvectors
+
+
+def diis_coefficients(gram):
+    g = _f64(gram)
+    m = g.shape[0]
+    c = np.empty(m)
+    ok = lib().ora_diis_coefficients(m, _p(g), _p(c))
+    return c if ok else None
+
+
+class State:
+    """A converged oracle state (orbitals, eigenvalues, densities, potentials)."""
+
+    def __init__(self, ptr, n):
+        self.ptr, self.n = ptr, n
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().ora_state_free(self.ptr)
+            self.ptr = None
+
+    def counts(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        lib().ora_state_counts(self.ptr, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def evals(self):
+        nu, nd = self.counts()
+        up, dn = np.empty(max(nu, 1)), np.empty(max(nd, 1))
+        lib().ora_state_evals(self.ptr, _p(up), _p(dn))
+        return up[:nu], dn[:nd]
+
+    def density(self):
+        up, dn = np.empty(self.n ** 3), np.empty(self.n ** 3)
+        lib().ora_state_density(self.ptr, _p(up), _p(dn))
+        return up, dn
+
+    def potentials(self):
+        a, b = np.empty(self.n ** 3), np.empty(self.n ** 3)
+        lib().ora_state_potentials(self.ptr, _p(a), _p(b))
+        return a, b
+
+    def orbitals(self, spin):
+        nu, nd = self.counts()
+        k = nd if spin else nu
+        out = np.empty(max(k, 1) * self.n ** 3)
+        lib().ora_state_orbitals(self.ptr, spin, _p(out))
+        return out[: k * self.n ** 3].reshape(k, self.n ** 3)
+
+
+def scf(n, h, nuclei, n_up, n_dn, sigma=None, tol=1e-6, mixing=0.3, eig_tol=1e-6, max_iter=200, diis_history=6,
+        stall_window=50, warm=None):
+    """Aufbau SCF (crates/qm/src/scf.rs:909). Returns (State or None, stats dict)."""
+    s = Settings(h if sigma is None else sigma, tol, mixing, eig_tol, max_iter, diis_history, stall_window)
+    st = Stats()
+    ptr = lib().ora_scf(n, ctypes.c_double(h), nuclei_array(nuclei), len(nuclei), n_up, n_dn, ctypes.byref(s),
+                        warm.ptr if warm is not None else None, ctypes.byref(st))
+    stats = {f[0]: getattr(st, f[0]) for f in Stats._fields_}
+    stats["electrons"] = list(st.electrons)
+    return (State(ptr, n) if ptr else None), stats
+
+
+def forces(state, nuclei, sigma):
+    out = np.empty(3 * len(nuclei))
+    rc = lib().ora_forces(state.ptr, nuclei_array(nuclei), len(nuclei), ctypes.c_double(sigma), _p(out))
+    if rc != 0:
+        raise ValueError("coincident nuclei")
+    return out.reshape(-1, 3)
