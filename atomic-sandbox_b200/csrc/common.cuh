@@ -1,0 +1,67 @@
+// common.cuh -- field layout, launch helpers and error plumbing shared by the kernels and the host
+// orchestration of the B200 Kohn-Sham solver.
+//
+// Field layout in HBM (the "pitched cube"): a real-space field on the cubic n^3 grid is stored
+// x-fastest with a row pitch P = n rounded up to a multiple of 4 floats (16 B):
+//     element (i, j, k) at  (k*n + j)*P + i,     field stride F = n*n*P floats.
+// There are no ghost cells: the Dirichlet zero outside the box comes from the TMA loads' out-of-
+// bounds fill (the tensor map's extent is n on every axis), so a field costs n*n*P floats instead
+// of the reference's (n+8)^3 (crates/qm-gpu/src/grid.rs:3-27). The pad columns i in [n, P) hold 0:
+// kernels that generate a field write 0 there, arithmetic kernels map 0 to 0, and the reductions
+// therefore sum the pads harmlessly. Blocks of fields (LOBPCG's X, W, P, ...) are contiguous with
+// stride F, which makes one 4-D tensor map (n, n, n, count) cover a whole block.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace ks {
+
+struct Layout {
+    int n = 0;       // points per axis
+    int P = 0;       // row pitch (floats), multiple of 4
+    long long F = 0; // floats per field
+    double h = 0;    // spacing (Bohr)
+    double origin = 0; // coordinate of index 0 on every axis: -(n-1)h/2 (crates/qm/src/grid.rs:11-14)
+    static Layout make(int n, double h) {
+        Layout L;
+        L.n = n;
+        L.P = (n + 3) & ~3;
+        L.F = (long long)n * n * L.P;
+        L.h = h;
+        L.origin = -((double)(n - 1) * h / 2.0);
+        return L;
+    }
+    long long interior() const { return (long long)n * n * n; }
+};
+
+// A CUDA error inside the library becomes this exception; the C ABI turns it into KS_DEVICE.
+struct DeviceError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+// Broken numerics (NaN Gram, non-SPD CG, lost rank) become this; the C ABI maps it to KS_NUMERICAL.
+struct NumericalError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+inline void check_cuda(cudaError_t e, const char* what, const char* file, int line) {
+    if (e != cudaSuccess) {
+        char buf[512];
+        snprintf(buf, sizeof buf, "%s failed at %s:%d: %s", what, file, line, cudaGetErrorString(e));
+        throw DeviceError(buf);
+    }
+}
+#define KS_CUDA(call) ::ks::check_cuda((call), #call, __FILE__, __LINE__)
+#define KS_LAUNCH_CHECK() ::ks::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Number of SMs of the current device (148 on B200), cached per process.
+int sm_count();
+// A device int that kernels with bounded waits set to nonzero when a wait gives up; the host reads
+// and clears it after each solve step (allocated once per process).
+int* device_error_flag();
+
+}  // namespace ks

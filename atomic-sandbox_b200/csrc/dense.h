@@ -1,0 +1,35 @@
+// dense.h -- small dense f64 linear algebra on the host: the Rayleigh-Ritz and DIIS solves of the
+// SCF (matrices of a few dozen rows). Row-major storage unless stated.
+#pragma once
+#include <vector>
+
+namespace ks {
+namespace dense {
+
+using Mat = std::vector<double>;  // row-major n x n
+
+// Symmetric eigen-decomposition, checked like the reference's `qm::eigen::sym_eigen`
+// (crates/qm/src/eigen.rs:150-173): Householder tridiagonalisation + implicit QL, then every
+// pair's residual |A v - lambda v| against 1e-11 (1 + max|lambda|); a failing decomposition is
+// refined by cyclic Jacobi (crates/qm/src/eigen.rs:175-211). evals unsorted; evecs column-major
+// (evecs[i + n*k] = component i of eigenvector k).
+void sym_eigen(int n, const Mat& a, std::vector<double>& evals, std::vector<double>& evecs);
+// The cyclic Jacobi method alone (the reference's fallback).
+void jacobi_eigen(int n, Mat a, std::vector<double>& evals, std::vector<double>& evecs);
+// Householder + implicit QL alone (no check).
+void tridiag_ql_eigen(int n, const Mat& a, std::vector<double>& evals, std::vector<double>& evecs);
+
+// Cholesky A = L L^T of an SPD matrix (lower factor in place). False if a pivot is not positive.
+bool cholesky(int n, Mat& a);
+// Solves L L^T X = B for q right-hand sides (B row-major n x q, overwritten by X).
+void cholesky_solve(int n, const Mat& l, int q, std::vector<double>& b);
+// Gaussian elimination with partial pivoting; false on a zero pivot (nalgebra's `lu().solve`).
+bool lu_solve(int n, Mat a, std::vector<double>& b);
+
+// Bordered Pulay system on a residual Gram matrix (m x m row-major), scaled by its largest
+// diagonal with a 1e-12 relative diagonal shift (crates/qm/src/scf.rs:681-697). False when the
+// solve fails or gives non-finite coefficients.
+bool diis_coefficients(int m, const Mat& gram, std::vector<double>& c);
+
+}  // namespace dense
+}  // namespace ks

@@ -1,0 +1,1062 @@
+// solver.cu -- host orchestration of the B200 Kohn-Sham SCF: the device reducer, the MG-PCG
+// Hartree solve, LOBPCG with host f64 Rayleigh-Ritz, the Aufbau SCF driver and the forces.
+//
+// Algorithm sources (the reference's GPU solver, whose decisions this follows):
+//   SCF driver      crates/qm-gpu/src/scf.rs:1237-1708 (eig tol tied to dRho, guess band, DIIS restart
+//                   on a re-solved frozen set, charge renormalisation to the output charge)
+//   LOBPCG          crates/qm-gpu/src/eigen.rs:685-1000 (raw [X, W, P], generalised Rayleigh-Ritz with
+//                   the conditioning guard, X columns of A through the residuals, P orthogonalised to X,
+//                   formation check, f32 floor stop)
+//   Poisson         crates/qm-gpu/src/poisson.rs:284-342 (MG-PCG, true-residual floor detection)
+//   DIIS            crates/qm-gpu/src/scf.rs:558-646
+//   Forces          crates/qm-gpu/src/forces.rs:187-300
+// What changes on the B200: every reduction is finished on the device, the CG scalars never
+// leave it, the preconditioner/H-products/Ritz updates run as block kernels over all vectors of a
+// channel at once, and the SCF's charge renormalisation is a device-side scale.
+#include "solver.h"
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include "dense.h"
+
+namespace ks {
+
+// ------------------------------------------------------------------ process-wide device facts
+int sm_count() {
+    static int dev_cached = -1, count = 0;
+    int dev = 0;
+    KS_CUDA(cudaGetDevice(&dev));
+    if (dev != dev_cached) {
+        KS_CUDA(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev));
+        dev_cached = dev;
+    }
+    return count;
+}
+
+int* device_error_flag() {
+    static int* flags[64] = {nullptr};
+    int dev = 0;
+    KS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw DeviceError("device index out of range");
+    if (!flags[dev]) {
+        KS_CUDA(cudaMalloc(&flags[dev], sizeof(int)));
+        KS_CUDA(cudaMemset(flags[dev], 0, sizeof(int)));
+    }
+    return flags[dev];
+}
+
+namespace {
+
+constexpr double PI = 3.14159265358979323846;
+const double COEFF0 = -205.0 / 72.0;
+const double COEFF[5] = {-205.0 / 72.0, 8.0 / 5.0, -1.0 / 5.0, 8.0 / 315.0, -1.0 / 560.0};
+
+// LOBPCG constants (crates/qm-gpu/src/eigen.rs:276-317)
+constexpr int STALL_WINDOW = 12;
+constexpr double FLOOR_BAND = 10.0;
+constexpr double RR_DROP = 1e-6;
+constexpr double RITZ_FORM_SLACK = 1e-6;
+constexpr double RITZ_FORM_RES = 1e-4;
+constexpr int MAX_FORM_RESTORES = 3;
+constexpr double ALPHA_MAX = 2.0;
+constexpr double ALPHA_RESIDUAL_FRACTION = 0.1;
+constexpr double GUESS_DEP = 1e-4;
+constexpr int MAX_RESEED_ROUNDS = 3;
+// SCF constants (crates/qm-gpu/src/scf.rs:359-399)
+constexpr double POISSON_TOL = 1e-8;
+constexpr int POISSON_MAX_ITER = 5000;
+constexpr int EIGEN_MAX_ITER = 200;
+constexpr double EIG_TOL_FLOOR_FACTOR = 3.0;
+constexpr double EIG_GUESS_FACTOR = 1.5;
+constexpr double EIG_TOL_FRACTION = 0.0015;
+constexpr double EIG_TOL_MAX = 1e-3;
+constexpr double LAST_STEP_RESIDUAL_FACTOR = 3.0;
+constexpr double BOUNDARY_DENSITY_WARN = 1e-5;
+constexpr double STALL_LEVEL_PER_ELECTRON = 1e-3;
+// multigrid (crates/qm-gpu/src/multigrid.rs:62-72)
+constexpr int PRE_SWEEPS = 2, POST_SWEEPS = 2, COARSEST_SWEEPS = 12;
+constexpr double MG_OMEGA = 6.0 / 7.0;
+constexpr int FUSED_MAX_N = 24;
+constexpr int CHECK_EVERY = 5;
+
+double jacobi_omega() {
+    double symbol_pi = COEFF[0] + 2.0 * (-COEFF[1] + COEFF[2] - COEFF[3] + COEFF[4]);
+    return 4.0 / (3.0 * (symbol_pi / COEFF[0]));
+}
+
+using clk = std::chrono::steady_clock;
+double secs(clk::time_point a) { return std::chrono::duration<double>(clk::now() - a).count(); }
+
+// pinned host staging for coefficient uploads (one per process; every upload is followed by a
+// synchronising readback before the buffer is rewritten)
+double* upload_buffer(size_t doubles) {
+    static double* buf = nullptr;
+    static size_t cap = 0;
+    if (doubles > cap) {
+        if (buf) cudaFreeHost(buf);
+        KS_CUDA(cudaMallocHost(&buf, doubles * sizeof(double)));
+        cap = doubles;
+    }
+    return buf;
+}
+
+// Columns of a Gram matrix within rel^(1/2) of the span of the earlier ones
+// (crates/qm-gpu/src/eigen.rs:491-509).
+std::vector<int> dependent_columns(int m, const std::vector<double>& b, double rel) {
+    std::vector<double> l((size_t)m * m, 0.0);
+    std::vector<int> kept, dep;
+    for (int i = 0; i < m; ++i) {
+        double d = b[(size_t)i * m + i];
+        for (int j : kept) {
+            double s = b[(size_t)i * m + j];
+            for (int q : kept) {
+                if (q >= j) break;
+                s -= l[(size_t)i * m + q] * l[(size_t)j * m + q];
+            }
+            l[(size_t)i * m + j] = s / l[(size_t)j * m + j];
+            d -= l[(size_t)i * m + j] * l[(size_t)i * m + j];
+        }
+        bool independent = d > rel * b[(size_t)i * m + i] && b[(size_t)i * m + i] > 0.0;
+        if (independent) {
+            l[(size_t)i * m + i] = std::sqrt(d);
+            kept.push_back(i);
+        } else {
+            dep.push_back(i);
+        }
+    }
+    return dep;
+}
+
+}  // namespace
+
+double residual_floor_estimate(double h) {
+    double s = 1.0 / (2.0 * h * h);
+    double mean = 3.0 * std::fabs(COEFF[0]) * s;
+    double c2 = 0.0;
+    for (int m = 1; m <= 4; ++m) c2 += COEFF[m] * COEFF[m];
+    double var = 3.0 * 2.0 * c2 * s * s;
+    return 2.4e-8 * std::sqrt(mean * mean + var);
+}
+
+double rayleigh_ritz(int m, const std::vector<double>& A, const std::vector<double>& B, int nk, std::vector<double>& theta,
+                     std::vector<double>& C) {
+    for (int i = 0; i < m; ++i)
+        if (!(B[(size_t)i * m + i] > 0.0))
+            throw NumericalError("lobpcg: column " + std::to_string(i) + " of S has non-positive norm");
+    std::vector<double> d(m);
+    for (int i = 0; i < m; ++i) d[i] = 1.0 / std::sqrt(B[(size_t)i * m + i]);
+    dense::Mat an((size_t)m * m), bn((size_t)m * m);
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+            an[(size_t)i * m + j] = A[(size_t)i * m + j] * d[i] * d[j];
+            bn[(size_t)i * m + j] = B[(size_t)i * m + j] * d[i] * d[j];
+        }
+    std::vector<double> sb, ub;
+    dense::sym_eigen(m, bn, sb, ub);
+    double smax = 0.0;
+    for (double x : sb) smax = std::max(smax, x);
+    std::vector<int> keep;
+    for (int i = 0; i < m; ++i)
+        if (sb[i] > RR_DROP * smax) keep.push_back(i);
+    const int nkp = (int)keep.size();
+    if (nkp < nk)
+        throw NumericalError("lobpcg: the subspace lost rank (" + std::to_string(nkp) + " of " + std::to_string(m) + " kept)");
+    std::vector<double> T((size_t)m * nkp);  // m x nkp row-major
+    for (int i = 0; i < m; ++i)
+        for (int c = 0; c < nkp; ++c) T[(size_t)i * nkp + c] = ub[i + (size_t)m * keep[c]] / std::sqrt(sb[keep[c]]);
+    std::vector<double> at((size_t)m * nkp, 0.0);  // an * T
+    for (int i = 0; i < m; ++i)
+        for (int c = 0; c < nkp; ++c) {
+            double s = 0.0;
+            for (int j = 0; j < m; ++j) s += an[(size_t)i * m + j] * T[(size_t)j * nkp + c];
+            at[(size_t)i * nkp + c] = s;
+        }
+    dense::Mat ah((size_t)nkp * nkp);
+    for (int a = 0; a < nkp; ++a)
+        for (int b = 0; b < nkp; ++b) {
+            double s = 0.0;
+            for (int i = 0; i < m; ++i) s += T[(size_t)i * nkp + a] * at[(size_t)i * nkp + b];
+            ah[(size_t)a * nkp + b] = s;
+        }
+    for (int a = 0; a < nkp; ++a)
+        for (int b = a + 1; b < nkp; ++b) {
+            double s = 0.5 * (ah[(size_t)a * nkp + b] + ah[(size_t)b * nkp + a]);
+            ah[(size_t)a * nkp + b] = ah[(size_t)b * nkp + a] = s;
+        }
+    std::vector<double> ea, va;
+    dense::sym_eigen(nkp, ah, ea, va);
+    std::vector<int> order(nkp);
+    for (int i = 0; i < nkp; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return ea[x] < ea[y]; });
+    theta.resize(nk);
+    for (int c = 0; c < nk; ++c) theta[c] = ea[order[c]];
+    double alpha = 0.0;
+    for (int c = 0; c < nk; ++c) {
+        double s = 0.0;
+        for (int q = 0; q < nkp; ++q) {
+            double y = va[q + (size_t)nkp * order[c]];
+            s += y * y / sb[keep[q]];
+        }
+        alpha = std::max(alpha, std::sqrt(s));
+    }
+    C.assign((size_t)m * nk, 0.0);  // column-major m x nk
+    for (int c = 0; c < nk; ++c)
+        for (int i = 0; i < m; ++i) {
+            double s = 0.0;
+            for (int q = 0; q < nkp; ++q) s += T[(size_t)i * nkp + q] * va[q + (size_t)nkp * order[c]];
+            C[i + (size_t)m * c] = d[i] * s;
+        }
+    return alpha;
+}
+
+// ------------------------------------------------------------------ buffers
+void DevBuf::alloc(size_t n) {
+    release();
+    if (n == 0) return;
+    KS_CUDA(cudaMalloc(&p, n));
+    bytes = n;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+void Block::create(const Layout& L, int c) {
+    count = c;
+    F = L.F;
+    buf.alloc((size_t)std::max(c, 1) * L.F * sizeof(float));
+    KS_CUDA(cudaMemset(buf.p, 0, buf.bytes));
+    make_field_tmap(&tmap, L, buf.f(), std::max(c, 1));
+}
+
+// ------------------------------------------------------------------ reducer
+void Reducer::init(const Layout& L, cudaStream_t s, size_t partial_doubles) {
+    L_ = L;
+    s_ = s;
+    blocks_ = reduce_blocks(L.F);
+    gram_blocks_ = 2 * sm_count();
+    partials_.alloc(std::max(partial_doubles, (size_t)1 << 16) * sizeof(double));
+    res_.alloc(RES_CAP * sizeof(double));
+    KS_CUDA(cudaMallocHost(&host_, RES_CAP * sizeof(double)));
+    KS_CUDA(cudaMallocHost(&host_flag_, sizeof(int)));
+}
+
+Reducer::~Reducer() {
+    if (host_) cudaFreeHost(host_);
+    if (host_flag_) cudaFreeHost(host_flag_);
+}
+
+void Reducer::dots(const std::vector<std::pair<const float*, const float*>>& pairs, int off, double scale) {
+    for (size_t c0 = 0; c0 < pairs.size(); c0 += Pairs::MAX) {
+        Pairs p;
+        p.count = (int)std::min(pairs.size() - c0, (size_t)Pairs::MAX);
+        for (int q = 0; q < p.count; ++q) { p.a[q] = pairs[c0 + q].first; p.b[q] = pairs[c0 + q].second; }
+        launch_dots(L_.F, p, partials_.d(), blocks_, s_);
+        launch_finish(partials_.d(), blocks_, p.count, scale, res_.d() + off + c0, s_);
+    }
+}
+
+void Reducer::gram(int m, const float* S, int mt, const float* T, int off, double scale) {
+    const size_t need = (size_t)gram_blocks_ * m * (m + mt);
+    if (need * sizeof(double) > partials_.bytes) partials_.alloc(need * sizeof(double));
+    launch_gram(L_.F, m, S, mt, T, partials_.d(), gram_blocks_, s_);
+    launch_finish(partials_.d(), gram_blocks_, m * (m + mt), scale, res_.d() + off, s_);
+}
+
+const double* Reducer::read(int count) {
+    if (count > RES_CAP) throw std::invalid_argument("reducer: result overflow");
+    if (count > 0) KS_CUDA(cudaMemcpyAsync(host_, res_.d(), (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    KS_CUDA(cudaMemcpyAsync(host_flag_, device_error_flag(), sizeof(int), cudaMemcpyDeviceToHost, s_));
+    KS_CUDA(cudaStreamSynchronize(s_));
+    ++readbacks;
+    if (*host_flag_) {
+        KS_CUDA(cudaMemsetAsync(device_error_flag(), 0, sizeof(int), s_));
+        throw DeviceError("a kernel's bounded wait gave up (TMA copy did not complete)");
+    }
+    return host_;
+}
+
+// ------------------------------------------------------------------ Poisson (MG-PCG)
+void Poisson::init(const Layout& L, cudaStream_t s, Reducer* red) {
+    L_ = L;
+    s_ = s;
+    red_ = red;
+    r_.create(L, 1); p_.create(L, 1); ap_.create(L, 1); b_.create(L, 1); z_.create(L, 1); res0_.create(L, 1); tmp0_.create(L, 1);
+    ghost_.alloc(24 * (size_t)L.n * L.n * sizeof(double));
+    scal_.alloc(8 * sizeof(double));
+    KS_CUDA(cudaMemset(scal_.p, 0, 8 * sizeof(double)));
+    q_.alloc(49 * sizeof(double));
+    // hierarchy (crates/qm-gpu/src/multigrid.rs:105-118): odd-index coarsening down to n <= 2
+    MgLevel l0{L.n, L.P, L.F, L.h, 0.f, 0.f};
+    lvdesc_.push_back(l0);
+    double d_low = 1.0, d_high = 1.0;
+    int n = L.n;
+    double h = L.h;
+    while (n > 2) {
+        int nc = n / 2;
+        double dl = (d_low + 1.0) / 2.0;
+        double dh = (d_high + (double)(n - 2 * nc)) / 2.0;
+        Layout C = Layout::make(nc, 2.0 * h);
+        MgLevel lv{nc, C.P, C.F, 2.0 * h, (float)(1.0 - 1.0 / dl), (float)(1.0 - 1.0 / dh)};
+        lvdesc_.push_back(lv);
+        n = nc;
+        h = 2.0 * h;
+        d_low = dl;
+        d_high = dh;
+    }
+    levels_.resize(lvdesc_.size());
+    for (size_t l = 1; l < lvdesc_.size(); ++l) {
+        size_t bytes = (size_t)lvdesc_[l].F * sizeof(float);
+        levels_[l].lv = lvdesc_[l];
+        levels_[l].x.alloc(bytes); levels_[l].b.alloc(bytes); levels_[l].res.alloc(bytes); levels_[l].tmp.alloc(bytes);
+        KS_CUDA(cudaMemset(levels_[l].x.p, 0, bytes)); KS_CUDA(cudaMemset(levels_[l].b.p, 0, bytes));
+        KS_CUDA(cudaMemset(levels_[l].res.p, 0, bytes)); KS_CUDA(cudaMemset(levels_[l].tmp.p, 0, bytes));
+    }
+    fused_from_ = (int)lvdesc_.size() - 1;
+    for (size_t l = 0; l < lvdesc_.size(); ++l)
+        if (lvdesc_[l].n <= FUSED_MAX_N) { fused_from_ = (int)l; break; }
+}
+
+void Poisson::cycle(int l, float* x, const float* b) {
+    const int nl = (int)lvdesc_.size();
+    auto res_of = [&](int i) { return i == 0 ? res0_.at(0) : levels_[i].res.f(); };
+    auto tmp_of = [&](int i) { return i == 0 ? tmp0_.at(0) : levels_[i].tmp.f(); };
+    if (l >= fused_from_) {
+        MgCoarse c;
+        c.nlev = nl - l;
+        if (c.nlev > MgCoarse::MAXL) throw std::logic_error("multigrid: too many fused levels");
+        for (int i = l; i < nl; ++i) {
+            int q = i - l;
+            c.lv[q] = lvdesc_[i];
+            c.x[q] = i == l ? x : levels_[i].x.f();
+            c.b[q] = i == l ? const_cast<float*>(b) : levels_[i].b.f();
+            c.res[q] = res_of(i);
+            c.tmp[q] = tmp_of(i);
+        }
+        launch_mg_coarse(c, (float)MG_OMEGA, PRE_SWEEPS, POST_SWEEPS, COARSEST_SWEEPS, s_);
+        return;
+    }
+    const MgLevel& lv = lvdesc_[l];
+    launch_fill(x, 0.0f, lv.F, s_);
+    for (int sw = 0; sw < PRE_SWEEPS; ++sw) {
+        if (sw & 1) launch_mg_jacobi(lv, tmp_of(l), b, x, (float)MG_OMEGA, s_);
+        else launch_mg_jacobi(lv, x, b, tmp_of(l), (float)MG_OMEGA, s_);
+    }
+    launch_mg_residual(lv, x, b, res_of(l), s_);
+    launch_mg_restrict(lvdesc_[l + 1], lv, res_of(l), levels_[l + 1].b.f(), s_);
+    cycle(l + 1, levels_[l + 1].x.f(), levels_[l + 1].b.f());
+    launch_mg_prolong_add(lvdesc_[l + 1], lv, levels_[l + 1].x.f(), x, s_);
+    for (int sw = 0; sw < POST_SWEEPS; ++sw) {
+        if (sw & 1) launch_mg_jacobi(lv, tmp_of(l), b, x, (float)MG_OMEGA, s_);
+        else launch_mg_jacobi(lv, x, b, tmp_of(l), (float)MG_OMEGA, s_);
+    }
+}
+
+void Poisson::vcycle(const float* rhs, float* z) { cycle(0, z, rhs); }
+
+void Poisson::moments(const float* rho, double* dst) {
+    launch_moments(L_, rho, red_->partials(), red_->blocks(), s_);
+    launch_finish(red_->partials(), red_->blocks(), 49, L_.h * L_.h * L_.h, dst, s_);
+}
+
+void Poisson::true_residual(const float* v, const CUtensorMap& v_map) {
+    StencilArgs a;
+    a.mode = ST_LAPLACIAN;
+    a.scale = (float)(1.0 / (L_.h * L_.h));
+    launch_stencil(L_, v_map, 1, a, ap_.at(0), s_);
+    Terms t;
+    t.count = 2;
+    t.x[0] = b_.at(0); t.c[0] = 1.f;
+    t.x[1] = ap_.at(0); t.c[1] = 1.f;
+    launch_lincomb(L_.F, 1, ap_.at(0), t, s_);
+    red_->dots({{ap_.at(0), ap_.at(0)}}, 0, 1.0);
+}
+
+PoissonStats Poisson::solve(const float* rho, float* v, const CUtensorMap& v_map, double tol, int max_iter) {
+    PoissonStats st;
+    const int rb0 = red_->readbacks;
+    double* scal = scal_.d();
+    moments(rho, q_.d());
+    launch_poisson_rhs(L_, rho, q_.d(), ghost_.d(), b_.at(0), s_);
+    // r = b - A v = b + L v; z = M^-1 r; p = z
+    StencilArgs lap;
+    lap.mode = ST_LAPLACIAN;
+    lap.scale = (float)(1.0 / (L_.h * L_.h));
+    launch_stencil(L_, v_map, 1, lap, ap_.at(0), s_);
+    Terms t;
+    t.count = 2;
+    t.x[0] = b_.at(0); t.c[0] = 1.f;
+    t.x[1] = ap_.at(0); t.c[1] = 1.f;
+    launch_lincomb(L_.F, 1, r_.at(0), t, s_);
+    vcycle(r_.at(0), z_.at(0));
+    Terms cp;
+    cp.count = 1;
+    cp.x[0] = z_.at(0); cp.c[0] = 1.f;
+    launch_lincomb(L_.F, 1, p_.at(0), cp, s_);
+    // scal[1 + 2s] = r.z, scal[2 + 2s] = r.r for parity s
+    red_->dots({{r_.at(0), z_.at(0)}, {r_.at(0), r_.at(0)}, {b_.at(0), b_.at(0)}}, 0, 1.0);
+    KS_CUDA(cudaMemcpyAsync(scal + 1, red_->res(), 2 * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+    const double* h = red_->read(3);
+    const double bb = h[2];
+    double rz = h[0], rr = h[1];
+    if (!(std::isfinite(bb) && std::isfinite(rr) && std::isfinite(rz)))
+        throw NumericalError("Poisson: non-finite |b|, |r| or <r, z> (NaN in rho or V)");
+    const double b_norm2 = std::max(bb, 1e-300);
+    double residual = std::sqrt(rr / b_norm2);
+    int it = 0, par = 0;
+    double last_true = INFINITY;
+    int stop = -1;
+    StencilArgs lapd = lap;
+    while (residual > tol && it < max_iter) {
+        if (!(rz > 0.0))
+            throw NumericalError("Poisson: the multigrid preconditioner lost positive-definiteness (r.z = " + std::to_string(rz) + ")");
+        // ap = L p and p.Ap = -sum p (L p)
+        lapd.dot_partials = red_->partials();
+        int ctas = launch_stencil(L_, p_.tmap, 1, lapd, ap_.at(0), s_);
+        launch_finish(red_->partials(), ctas, 1, -1.0, scal, s_);
+        launch_cg_update(L_.F, v, r_.at(0), p_.at(0), ap_.at(0), scal, 1 + 2 * par, s_);
+        vcycle(r_.at(0), z_.at(0));
+        const int nxt = 1 - par;
+        red_->dots({{r_.at(0), z_.at(0)}, {r_.at(0), r_.at(0)}}, 1, 1.0);
+        KS_CUDA(cudaMemcpyAsync(scal + 1 + 2 * nxt, red_->res() + 1, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+        launch_cg_direction(L_.F, p_.at(0), z_.at(0), scal, 1 + 2 * par, 1 + 2 * nxt, s_);
+        KS_CUDA(cudaMemcpyAsync(red_->res(), scal, sizeof(double), cudaMemcpyDeviceToDevice, s_));
+        h = red_->read(3);
+        const double pap = h[0];
+        rz = h[1];
+        rr = h[2];
+        if (!(pap > 0.0)) throw NumericalError("Poisson: A lost positive-definiteness (p.Ap = " + std::to_string(pap) + ")");
+        par = nxt;
+        ++it;
+        residual = std::sqrt(rr / b_norm2);
+        if (it % CHECK_EVERY == 0 && residual > tol) {
+            true_residual(v, v_map);
+            double tr = std::sqrt(red_->read(1)[0] / b_norm2);
+            if (!std::isfinite(tr)) throw NumericalError("Poisson: non-finite true residual");
+            // crates/qm-gpu/src/poisson.rs:188-190
+            if (tr >= 4.0 * residual) { stop = 1; break; }
+            if (tr >= 2.0 * residual && tr >= last_true) { stop = 2; break; }
+            last_true = tr;
+        }
+    }
+    if (stop < 0) stop = residual <= tol ? 0 : 3;
+    true_residual(v, v_map);
+    double tr = std::sqrt(red_->read(1)[0] / b_norm2);
+    if (!std::isfinite(tr)) throw NumericalError("Poisson: non-finite true residual");
+    st.iterations = it;
+    st.residual = tr;
+    st.stop = stop;
+    st.readbacks = red_->readbacks - rb0;
+    return st;
+}
+
+// ------------------------------------------------------------------ channels
+void Channel::create(const Layout& L, int kk) {
+    k = kk;
+    A[0].create(L, 3 * k);
+    A[1].create(L, 3 * k);
+    cur = 0;
+    T.create(L, 3 * k);
+    HX.create(L, k);
+    Q.create(L, k);
+    theta_d.alloc((size_t)(2 * k + 6 * k * k) * sizeof(double));  // [theta | lambda | coef 3k x 2k]
+    evals.assign(k, -1.0);
+}
+
+// ------------------------------------------------------------------ solver
+Solver::Solver(int n, double h, const SolverOptions& o) : L_(Layout::make(n, h)), opt_(o) {
+    if (n < 5 || !(h > 0)) throw std::invalid_argument("grid: n >= 5 and h > 0 required");
+    KS_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    red_.init(L_, s_, 1 << 20);
+    poisson_.init(L_, s_, &red_);
+    for (Block* b : {&vnuc_, &vh_, &in_up_, &in_dn_, &out_up_, &out_dn_, &rho_tot_, &v_up_, &v_dn_, &exc_, &ones_}) b->create(L_, 1);
+    launch_fill(ones_.at(0), 1.0f, L_.F, s_);
+    floor_ = residual_floor_estimate(h);
+    KS_CUDA(cudaStreamSynchronize(s_));
+}
+
+Solver::~Solver() {
+    if (s_) {
+        cudaStreamSynchronize(s_);
+        cudaStreamDestroy(s_);
+    }
+}
+
+void Solver::ensure_channel(int spin, int k) {
+    if (ch_[spin].k != k) {
+        ch_[spin] = Channel();
+        if (k > 0) ch_[spin].create(L_, k);
+    }
+}
+
+void Solver::gram_checked(int m, const float* S, int mt, const float* T) {
+    if (opt_.gram_mode != 0) throw std::invalid_argument("gram_mode 1 (tensor cores) is not built in this library");
+    red_.gram(m, S, mt, T, 0, L_.h * L_.h * L_.h);  // the L2 product <a, b> = h^3 sum a b
+}
+
+EigenStats Solver::lobpcg(Channel& ch, const float* V, double tol, double guess_tol, int max_iter, int checked) {
+    EigenStats es;
+    const int k = ch.k;
+    const int rb0 = red_.readbacks;
+    const double omega = jacobi_omega();
+    const double diag_t = -1.5 * COEFF0 / (L_.h * L_.h);
+    const float ham_scale = (float)(-0.5 / (L_.h * L_.h));
+    double* theta_d = ch.theta_d.d();
+    double* lambda_d = theta_d + k;
+    double* coef_d = theta_d + 2 * k;
+    auto apply_h = [&](const Block& in, int vec0, int count, float* out) {
+        StencilArgs a;
+        a.mode = ST_HAMILTONIAN;
+        a.scale = ham_scale;
+        a.V = V;
+        a.vec0 = vec0;
+        launch_stencil(L_, in.tmap, count, a, out, s_);
+    };
+    // --- guess: one readback of X^T X and <x_i, H x_i>; dependent columns are re-seeded
+    std::vector<double> theta(k), lambda(k);
+    for (int round = 0;; ++round) {
+        if (round >= MAX_RESEED_ROUNDS) throw NumericalError("lobpcg: could not generate independent guess vectors");
+        apply_h(ch.A[ch.cur], 0, k, ch.HX.at(0));
+        gram_checked(k, ch.X(), k, ch.HX.at(0));
+        const double* g = red_.read(k * 2 * k);
+        std::vector<double> B((size_t)k * k);
+        for (int i = 0; i < k; ++i)
+            for (int j = 0; j < k; ++j) B[(size_t)i * k + j] = 0.5 * (g[(size_t)i * 2 * k + j] + g[(size_t)j * 2 * k + i]);
+        std::vector<int> dep = dependent_columns(k, B, GUESS_DEP);
+        if (dep.empty()) {
+            for (int i = 0; i < k; ++i) {
+                theta[i] = g[(size_t)i * 2 * k + k + i] / B[(size_t)i * k + i];
+                if (!std::isfinite(theta[i])) throw NumericalError("lobpcg: non-finite Rayleigh quotient of a guess vector");
+            }
+            break;
+        }
+        // deterministic noise under a Gaussian envelope (crates/qm-gpu/src/eigen.rs:376-389)
+        const long long N = L_.interior();
+        std::vector<double> noise(N);
+        DevBuf tmp((size_t)N * sizeof(double));
+        for (int slot : dep) {
+            unsigned long long seed = 0x9E3779B97F4A7C15ULL ^ ((unsigned long long)slot << 32) ^ (unsigned long long)(round + 1);
+            const int n = L_.n;
+            double sigma2 = std::pow((n - 1) * L_.h / 4.0, 2);
+            long long q = 0;
+            for (int kk = 0; kk < n; ++kk)
+                for (int j = 0; j < n; ++j)
+                    for (int i = 0; i < n; ++i) {
+                        seed = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+                        double u = (double)(seed >> 11) / 9007199254740992.0;
+                        double x = L_.origin + i * L_.h, y = L_.origin + j * L_.h, z = L_.origin + kk * L_.h;
+                        noise[q++] = (u - 0.5) * std::exp(-(x * x + y * y + z * z) / (2.0 * sigma2));
+                    }
+            KS_CUDA(cudaMemcpyAsync(tmp.p, noise.data(), N * sizeof(double), cudaMemcpyHostToDevice, s_));
+            launch_pack(L_, 1, tmp.d(), ch.A[ch.cur].at(slot), s_);
+            KS_CUDA(cudaStreamSynchronize(s_));
+        }
+    }
+    lambda = theta;
+    auto upload = [&](const std::vector<double>& th, const std::vector<double>& la, const std::vector<double>* coef) {
+        size_t nd = 2 * (size_t)k + (coef ? coef->size() : 0);
+        double* up = upload_buffer(nd);
+        std::copy(th.begin(), th.end(), up);
+        std::copy(la.begin(), la.end(), up + k);
+        if (coef) std::copy(coef->begin(), coef->end(), up + 2 * k);
+        KS_CUDA(cudaMemcpyAsync(theta_d, up, nd * sizeof(double), cudaMemcpyHostToDevice, s_));
+    };
+    upload(theta, lambda, nullptr);
+    int np = 0, iterations = 0, best_it = 0;
+    double best = INFINITY;
+    bool have_prev = false;
+    std::vector<double> prev_theta;
+    std::vector<double> res(k);
+    for (;;) {
+        Block& S = ch.A[ch.cur];
+        // 1. R = HX - theta X with the first Jacobi sweep fused (into Q), then 3 damped sweeps Q -> W -> Q -> W
+        double* norm_partials = red_.partials();
+        const int nb = red_.blocks();
+        launch_residual_precond(L_, k, ch.HX.at(0), ch.X(), theta_d, V, lambda_d, diag_t, ch.T.at(0), ch.Q.at(0), norm_partials, nb, s_);
+        const int m = 2 * k + np;
+        const int off_norm = m * 2 * m;
+        launch_finish(norm_partials, nb, k, L_.h * L_.h * L_.h, red_.res() + off_norm, s_);
+        StencilArgs jac;
+        jac.mode = ST_JACOBI;
+        jac.scale = ham_scale;
+        jac.V = V;
+        jac.R = ch.T.at(0);
+        jac.lambda = lambda_d;
+        jac.omega = (float)omega;
+        jac.diag_t = (float)diag_t;
+        jac.vec0 = 0;
+        launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), s_);       // Q -> W
+        jac.vec0 = k;
+        launch_stencil(L_, S.tmap, k, jac, ch.Q.at(0), s_);       // W -> Q
+        jac.vec0 = 0;
+        launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), s_);       // Q -> W
+        // 2. HW and HP in one launch (W and P are contiguous after X)
+        apply_h(S, k, k + np, ch.T.at(k));
+        // 3. the readback: G = S^T [S | T] and |r_i|^2
+        gram_checked(m, S.at(0), m, ch.T.at(0));
+        const double* g = red_.read(off_norm + k);
+        const int mc = 2 * m;
+        std::vector<double> A((size_t)m * m), B((size_t)m * m);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j <= i; ++j) {
+                double bv = g[(size_t)i * mc + j];
+                double av = g[(size_t)i * mc + m + j];
+                if (j < k) av += theta[j] * bv;  // <s_i, H x_j> = <s_i, r_j> + theta_j <s_i, x_j>
+                B[(size_t)i * m + j] = B[(size_t)j * m + i] = bv;
+                A[(size_t)i * m + j] = A[(size_t)j * m + i] = av;
+            }
+        for (double x : A)
+            if (!std::isfinite(x)) throw NumericalError("lobpcg: non-finite Gram entry (NaN in a vector or in V)");
+        for (double x : B)
+            if (!std::isfinite(x)) throw NumericalError("lobpcg: non-finite Gram entry (NaN in a vector or in V)");
+        double max_res = 0.0, stop_res = 0.0;
+        for (int i = 0; i < k; ++i) {
+            double xx = B[(size_t)i * m + i];
+            lambda[i] = A[(size_t)i * m + i] / xx;
+            res[i] = std::sqrt(g[off_norm + i] / xx);
+            if (!std::isfinite(res[i]) || !std::isfinite(lambda[i])) throw NumericalError("lobpcg: non-finite residual");
+            max_res = std::max(max_res, res[i]);
+            if (i < checked) stop_res = std::max(stop_res, res[i]);
+        }
+        ch.evals = lambda;
+        // formation check (crates/qm-gpu/src/eigen.rs:800-825): undo a step whose moved columns' stored
+        // Rayleigh quotients rose above their Ritz values
+        if (have_prev) {
+            have_prev = false;
+            double rise = 0.0, slack = 0.0;
+            for (int i = 0; i < k; ++i) {
+                rise += lambda[i] - theta[i];
+                slack += RITZ_FORM_SLACK * (1.0 + std::fabs(theta[i])) + RITZ_FORM_RES * res[i];
+            }
+            bool bad = !(rise <= slack);
+            if (bad && es.restores >= MAX_FORM_RESTORES) es.restores_exhausted = true;
+            if (bad && es.restores < MAX_FORM_RESTORES) {
+                ++es.restores;
+                ch.cur ^= 1;
+                theta = prev_theta;
+                lambda = theta;
+                np = 0;
+                upload(theta, lambda, nullptr);
+                apply_h(ch.A[ch.cur], 0, k, ch.HX.at(0));
+                continue;
+            }
+        }
+        if (stop_res < 0.5 * best) { best = stop_res; best_it = iterations; }
+        // stop decision (crates/qm-gpu/src/eigen.rs:322-329)
+        int stop = -1;
+        if (stop_res < tol || (iterations == 0 && stop_res < guess_tol)) stop = 0;
+        else if (stop_res <= FLOOR_BAND * floor_ && iterations - best_it >= STALL_WINDOW) stop = 1;
+        else if (iterations >= max_iter) stop = 2;
+        if (stop >= 0) {
+            es.iterations = iterations;
+            es.max_residual = max_res;
+            es.stop = stop;
+            break;
+        }
+        ++iterations;
+        // 4. Rayleigh-Ritz with the conditioning guard; fallback: drop P and redo on [X, W]
+        std::vector<double> th, C;
+        double alpha = rayleigh_ritz(m, A, B, k, th, C);
+        es.alpha_worst = std::max(es.alpha_worst, alpha);
+        int mm = m;
+        if (!(alpha <= std::max(ALPHA_MAX, ALPHA_RESIDUAL_FRACTION * stop_res / floor_)) && np > 0) {
+            ++es.fallbacks;
+            const int m2 = 2 * k;
+            std::vector<double> A2((size_t)m2 * m2), B2((size_t)m2 * m2);
+            for (int i = 0; i < m2; ++i)
+                for (int j = 0; j < m2; ++j) { A2[(size_t)i * m2 + j] = A[(size_t)i * m + j]; B2[(size_t)i * m2 + j] = B[(size_t)i * m + j]; }
+            std::vector<double> C2;
+            rayleigh_ritz(m2, A2, B2, k, th, C2);
+            C.assign((size_t)m * k, 0.0);
+            for (int c = 0; c < k; ++c)
+                for (int i = 0; i < m2; ++i) C[i + (size_t)m * c] = C2[i + (size_t)m2 * c];
+            mm = m2;
+        }
+        (void)mm;
+        // 5. X_new = S C, P_new = X_new - X (X^T X)^-1 X^T X_new = S C_p
+        std::vector<double> bxx((size_t)k * k), rhs((size_t)k * k, 0.0);
+        for (int i = 0; i < k; ++i)
+            for (int j = 0; j < k; ++j) bxx[(size_t)i * k + j] = B[(size_t)i * m + j];
+        if (!dense::cholesky(k, bxx)) throw NumericalError("lobpcg: Cholesky of X^T X failed (X lost rank)");
+        for (int i = 0; i < k; ++i)
+            for (int c = 0; c < k; ++c) {
+                double s = 0.0;
+                for (int j = 0; j < m; ++j) s += B[(size_t)i * m + j] * C[j + (size_t)m * c];
+                rhs[(size_t)i * k + c] = s;
+            }
+        dense::cholesky_solve(k, bxx, k, rhs);
+        std::vector<double> coef((size_t)m * 2 * k);
+        for (int c = 0; c < k; ++c)
+            for (int i = 0; i < m; ++i) {
+                coef[i + (size_t)m * c] = C[i + (size_t)m * c];
+                coef[i + (size_t)m * (k + c)] = C[i + (size_t)m * c] - (i < k ? rhs[(size_t)i * k + c] : 0.0);
+            }
+        prev_theta = theta;
+        have_prev = true;
+        theta = th;
+        upload(theta, lambda, &coef);
+        const int next = ch.cur ^ 1;
+        launch_block_lincomb(L_.F, m, S.at(0), 2 * k, coef_d, ch.A[next].at(0), k, k, s_);
+        ch.cur = next;
+        np = k;
+        // 6. HX of the new X
+        apply_h(ch.A[ch.cur], 0, k, ch.HX.at(0));
+    }
+    es.readbacks = red_.readbacks - rb0;
+    return es;
+}
+
+ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,
+                        void* user, ks_stats* out) {
+    auto t0 = clk::now();
+    std::memset(out, 0, sizeof(*out));
+    profile = ks_profile{};
+    const int rb0 = red_.readbacks;
+    if (nn < 0 || n_up < 0 || n_dn < 0 || (nn > 0 && !nuc)) { error = "invalid arguments"; return KS_INVALID; }
+    if (nn > 32) { error = "at most 32 nuclei"; return KS_INVALID; }
+    // E_nn (crates/qm/src/nuclear.rs:277-289)
+    double e_nn = 0.0;
+    for (int i = 0; i < nn; ++i)
+        for (int j = i + 1; j < nn; ++j) {
+            double dx = nuc[i].pos[0] - nuc[j].pos[0], dy = nuc[i].pos[1] - nuc[j].pos[1], dz = nuc[i].pos[2] - nuc[j].pos[2];
+            double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+            if (d < 1e-8) {
+                error = "nuclei " + std::to_string(i) + " and " + std::to_string(j) + " coincide";
+                converged_ = false;
+                return KS_COINCIDENT_NUCLEI;
+            }
+            e_nn += (double)nuc[i].z * (double)nuc[j].z / d;
+        }
+    std::vector<Nuc> hn(std::max(nn, 1));
+    double z_tot = 0.0;
+    for (int i = 0; i < nn; ++i) {
+        hn[i] = Nuc{nuc[i].pos[0], nuc[i].pos[1], nuc[i].pos[2], (double)nuc[i].z};
+        z_tot += nuc[i].z;
+    }
+    try {
+        nuc_d_.alloc(hn.size() * sizeof(Nuc));
+        KS_CUDA(cudaMemcpyAsync(nuc_d_.p, hn.data(), hn.size() * sizeof(Nuc), cudaMemcpyHostToDevice, s_));
+        const Nuc* dnuc = static_cast<const Nuc*>(nuc_d_.p);
+        const double dv = L_.h * L_.h * L_.h;
+        const double eig_lo = std::max(s.eig_tol, EIG_TOL_FLOOR_FACTOR * floor_);
+        const int nocc[2] = {n_up, n_dn};
+        int kk[2];
+        for (int sp = 0; sp < 2; ++sp) kk[sp] = nocc[sp] > 0 ? nocc[sp] + opt_.n_extra : 0;
+        const bool reuse = warm && have_warm_ && nocc_[0] == n_up && nocc_[1] == n_dn && ch_[0].k == kk[0] && ch_[1].k == kk[1];
+        converged_ = false;
+        have_warm_ = false;
+        auto t_start = clk::now();
+        if (!reuse) {
+            for (int sp = 0; sp < 2; ++sp) {
+                ensure_channel(sp, kk[sp]);
+                if (kk[sp] > 0) {
+                    ch_[sp].cur = 0;
+                    launch_initial_orbitals(L_, dnuc, nn, kk[sp], (unsigned long long)(sp + 1), opt_.init_mode, ch_[sp].X(), s_);
+                    ch_[sp].evals.assign(kk[sp], -1.0);
+                }
+            }
+            const double total = (double)(n_up + n_dn);
+            const double scale = z_tot > 0.0 ? total / z_tot : 0.0;
+            const double fu = total > 0.0 ? n_up / total : 0.0, fd = total > 0.0 ? n_dn / total : 0.0;
+            // the Aufbau cold density: sigma = 1 Bohr blobs of each nucleus' charge (crates/qm/src/nuclear.rs:212-214)
+            launch_deposit_charge(L_, dnuc, nn, 1.0, scale * fu, in_up_.at(0), s_);
+            launch_deposit_charge(L_, dnuc, nn, 1.0, scale * fd, in_dn_.at(0), s_);
+            launch_fill(vh_.at(0), 0.0f, L_.F, s_);
+        } else {
+            KS_CUDA(cudaMemcpyAsync(in_up_.at(0), out_up_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+            KS_CUDA(cudaMemcpyAsync(in_dn_.at(0), out_dn_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+        }
+        nocc_[0] = n_up;
+        nocc_[1] = n_dn;
+        launch_nuclear_potential(L_, dnuc, nn, s.sigma, vnuc_.at(0), s_);
+        if (!reuse) KS_CUDA(cudaStreamSynchronize(s_));
+        profile.start_s = reuse ? 0.0 : secs(t_start);
+
+        // DIIS history (crates/qm-gpu/src/scf.rs:558-646) in a pool of field quadruples
+        const int cap = std::max(s.diis_history, 1);
+        if ((int)diis_pool_.size() < cap + 1) {
+            diis_pool_.resize(cap + 1);
+            for (auto& e : diis_pool_)
+                if (e.r_up.count == 0) { e.rho_up.create(L_, 1); e.rho_dn.create(L_, 1); e.r_up.create(L_, 1); e.r_dn.create(L_, 1); }
+        }
+        std::vector<int> hist, free_list;
+        for (int i = (int)diis_pool_.size() - 1; i >= 0; --i) free_list.push_back(i);
+        std::vector<std::vector<double>> gram;
+        auto drop_oldest = [&]() {
+            free_list.push_back(hist.front());
+            hist.erase(hist.begin());
+            gram.erase(gram.begin());
+            for (auto& r : gram) r.erase(r.begin());
+        };
+
+        int iterations = 0;
+        double delta_rho = INFINITY, test_tol = s.tol;
+        double q_out[2] = {0, 0};
+        bool frozen = false, stalled = false;
+        double anchor = INFINITY, best = INFINITY;
+        int anchor_at = 0;
+        const double level = STALL_LEVEL_PER_ELECTRON * (n_up + n_dn);
+        double max_eig_res = 0.0, last_step_res = 0.0, pois_res = 0.0;
+        int pois_it_max = 0;
+        bool last_step_maxiter = false;
+        while (iterations < s.max_iter) {
+            if (abort_fn && abort_fn(user)) {
+                have_warm_ = true;  // park the iterate (orbitals, evals, input densities) as the next warm start
+                KS_CUDA(cudaMemcpyAsync(out_up_.at(0), in_up_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+                KS_CUDA(cudaMemcpyAsync(out_dn_.at(0), in_dn_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+                KS_CUDA(cudaStreamSynchronize(s_));
+                profile.steps = iterations;
+                profile.readbacks = red_.readbacks - rb0;
+                profile.wall_s = secs(t0);
+                error = "abandoned before SCF step " + std::to_string(iterations + 1);
+                return KS_ABORTED;
+            }
+            ++iterations;
+            const double step_tol = delta_rho < test_tol ? eig_lo
+                                                         : (std::isfinite(delta_rho) ? std::min(std::max(EIG_TOL_FRACTION * delta_rho, eig_lo),
+                                                                                                std::max(EIG_TOL_MAX, eig_lo))
+                                                                                       : eig_lo);
+            // Hartree potential of rho_in
+            Terms tsum;
+            tsum.count = 2;
+            tsum.x[0] = in_up_.at(0); tsum.c[0] = 1.f;
+            tsum.x[1] = in_dn_.at(0); tsum.c[1] = 1.f;
+            launch_lincomb(L_.F, 1, rho_tot_.at(0), tsum, s_);
+            auto tp = clk::now();
+            PoissonStats ps = poisson_.solve(rho_tot_.at(0), vh_.at(0), vh_.tmap, POISSON_TOL, POISSON_MAX_ITER);
+            profile.poisson_s += secs(tp);
+            profile.poisson_iterations += ps.iterations;
+            pois_res = std::max(pois_res, ps.residual);
+            pois_it_max = std::max(pois_it_max, ps.iterations);
+            if (ps.stop == 3) ++out->n_warnings;
+            // XC and the effective potentials
+            launch_xc_veff(L_.F, in_up_.at(0), in_dn_.at(0), vnuc_.at(0), vh_.at(0), exc_.at(0), v_up_.at(0), v_dn_.at(0), nullptr,
+                           nullptr, s_);
+            // eigensolves
+            int eig_its = 0;
+            last_step_res = 0.0;
+            last_step_maxiter = false;
+            auto te = clk::now();
+            for (int sp = 0; sp < 2; ++sp) {
+                if (nocc[sp] == 0) continue;
+                EigenStats es = lobpcg(ch_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, EIG_GUESS_FACTOR * step_tol, EIGEN_MAX_ITER, nocc[sp]);
+                ++profile.eigen_calls;
+                profile.eigen_iterations += es.iterations;
+                eig_its += es.iterations;
+                if (es.restores_exhausted) throw NumericalError("LOBPCG: a Ritz-vector formation failed again after its restores");
+                double tight = 0.0;
+                for (int i = 0; i < nocc[sp]; ++i) tight = std::max(tight, 0.0);
+                tight = es.max_residual;
+                if (step_tol <= eig_lo) max_eig_res = std::max(max_eig_res, tight);
+                last_step_res = std::max(last_step_res, tight);
+                if (es.stop == 2) last_step_maxiter = true;
+            }
+            profile.eigen_s += secs(te);
+            // output densities, residuals, dRho, output charges and the new DIIS Gram row in one readback
+            const int fe = free_list.back();
+            Entry& E = diis_pool_[fe];
+            const int nb = red_.blocks();
+            for (int sp = 0; sp < 2; ++sp) {
+                const Block& in = sp ? in_dn_ : in_up_;
+                Block& outb = sp ? out_dn_ : out_up_;
+                Block& r = sp ? E.r_dn : E.r_up;
+                if (nocc[sp] > 0)
+                    launch_density_residual(L_.F, nocc[sp], ch_[sp].X(), nullptr, in.at(0), outb.at(0), r.at(0), red_.partials(), nb, s_);
+                else
+                    launch_density_residual(L_.F, 0, in.at(0), nullptr, in.at(0), outb.at(0), r.at(0), red_.partials(), nb, s_);
+                launch_finish(red_.partials(), nb, 2, dv, red_.res() + 2 * sp, s_);
+            }
+            std::vector<std::pair<const float*, const float*>> pairs;
+            for (int e : hist) {
+                pairs.push_back({E.r_up.at(0), diis_pool_[e].r_up.at(0)});
+                pairs.push_back({E.r_dn.at(0), diis_pool_[e].r_dn.at(0)});
+            }
+            pairs.push_back({E.r_up.at(0), E.r_up.at(0)});
+            pairs.push_back({E.r_dn.at(0), E.r_dn.at(0)});
+            red_.dots(pairs, 4, dv);
+            const double* h = red_.read(4 + (int)pairs.size());
+            delta_rho = h[0] + h[2];
+            q_out[0] = h[1];
+            q_out[1] = h[3];
+            std::vector<double> row;
+            for (size_t q = 0; q + 1 < pairs.size(); q += 2) row.push_back(h[4 + q] + h[5 + q]);
+            // stall watch (crates/qm/src/scf.rs:440-480)
+            if (delta_rho < best) best = delta_rho;
+            if (std::isfinite(delta_rho) && (!std::isfinite(anchor) || delta_rho <= 0.5 * anchor)) { anchor = delta_rho; anchor_at = iterations; }
+            const int since = iterations - anchor_at;
+            test_tol = s.tol;
+            if (!std::isfinite(delta_rho) || (delta_rho < test_tol && step_tol <= eig_lo)) break;
+            if (!(delta_rho < test_tol) && s.stall_window > 0 && since >= s.stall_window && best >= level) { stalled = true; break; }
+            // DIIS restart when a frozen orbital set is re-solved (the map rho_in -> rho_out changed)
+            const bool step_frozen = eig_its == 0;
+            const bool map_changed = frozen && !step_frozen && !hist.empty();
+            if (map_changed) ++profile.diis_resets;
+            frozen = step_frozen;
+            // push: the entry takes the input densities; their old buffers receive the mix
+            free_list.pop_back();
+            std::swap(E.rho_up, in_up_);
+            std::swap(E.rho_dn, in_dn_);
+            if (map_changed) {
+                while (!hist.empty()) drop_oldest();
+                row.erase(row.begin(), row.end() - 1);
+            }
+            for (size_t i = 0; i < gram.size(); ++i) gram[i].push_back(row[i]);
+            gram.push_back(row);
+            hist.push_back(fe);
+            if ((int)hist.size() > cap) drop_oldest();
+            // coefficients: drop the oldest entries while the bordered solve fails
+            std::vector<double> c;
+            for (;;) {
+                const int m = (int)hist.size();
+                if (m == 1) { c.assign(1, 1.0); break; }
+                dense::Mat gm((size_t)m * m);
+                for (int i = 0; i < m; ++i)
+                    for (int j = 0; j < m; ++j) gm[(size_t)i * m + j] = gram[i][j];
+                if (dense::diis_coefficients(m, gm, c)) break;
+                drop_oldest();
+            }
+            const int m = (int)hist.size();
+            std::vector<const float*> rp(m), rr(m);
+            std::vector<float> cf(m), af(m);
+            for (int i = 0; i < m; ++i) { cf[i] = (float)c[i]; af[i] = (float)(s.mixing * c[i]); }
+            for (int sp = 0; sp < 2; ++sp) {
+                for (int i = 0; i < m; ++i) {
+                    const Entry& e = diis_pool_[hist[i]];
+                    rp[i] = sp ? e.rho_dn.at(0) : e.rho_up.at(0);
+                    rr[i] = sp ? e.r_dn.at(0) : e.r_up.at(0);
+                }
+                launch_diis_mix(L_.F, m, rp.data(), rr.data(), cf.data(), af.data(), sp ? in_dn_.at(0) : in_up_.at(0), s_);
+            }
+            // charge renormalisation to the step's output charge, on the device
+            red_.dots({{in_up_.at(0), ones_.at(0)}, {in_dn_.at(0), ones_.at(0)}}, 0, dv);
+            if (n_up > 0) launch_scale_ratio(L_.F, in_up_.at(0), red_.res() + 0, q_out[0], s_);
+            if (n_dn > 0) launch_scale_ratio(L_.F, in_dn_.at(0), red_.res() + 1, q_out[1], s_);
+        }
+        profile.steps = iterations;
+        out->iterations = iterations;
+        out->delta_rho = delta_rho;
+        out->poisson_residual = pois_res;
+        out->poisson_iterations = pois_it_max;
+        out->max_eigen_residual = max_eig_res;
+        out->tol_used = test_tol;
+        if (stalled) {
+            error = "SCF stalled: best dRho " + std::to_string(best) + " not improved 2x in " + std::to_string(s.stall_window) + " iterations";
+            profile.readbacks = red_.readbacks - rb0;
+            profile.wall_s = secs(t0);
+            return KS_STALLED;
+        }
+        if (!(delta_rho < test_tol)) {
+            error = "SCF did not converge after " + std::to_string(iterations) + " iterations (dRho = " + std::to_string(delta_rho) + ")";
+            profile.readbacks = red_.readbacks - rb0;
+            profile.wall_s = secs(t0);
+            return KS_NOT_CONVERGED;
+        }
+        // --- energy from the output density and orbitals
+        Terms tsum;
+        tsum.count = 2;
+        tsum.x[0] = out_up_.at(0); tsum.c[0] = 1.f;
+        tsum.x[1] = out_dn_.at(0); tsum.c[1] = 1.f;
+        launch_lincomb(L_.F, 1, rho_tot_.at(0), tsum, s_);
+        auto tp = clk::now();
+        PoissonStats ps = poisson_.solve(rho_tot_.at(0), vh_.at(0), vh_.tmap, POISSON_TOL, POISSON_MAX_ITER);
+        profile.poisson_s += secs(tp);
+        profile.poisson_iterations += ps.iterations;
+        out->poisson_residual = std::max(out->poisson_residual, ps.residual);
+        out->poisson_iterations = std::max(out->poisson_iterations, ps.iterations);
+        launch_xc_veff(L_.F, out_up_.at(0), out_dn_.at(0), vnuc_.at(0), vh_.at(0), exc_.at(0), nullptr, nullptr, nullptr, nullptr, s_);
+        std::vector<std::pair<const float*, const float*>> pairs = {
+            {rho_tot_.at(0), vnuc_.at(0)}, {rho_tot_.at(0), vh_.at(0)}, {exc_.at(0), ones_.at(0)}};
+        for (int sp = 0; sp < 2; ++sp) {
+            if (nocc[sp] == 0) continue;
+            StencilArgs kin;
+            kin.mode = ST_LAPLACIAN;
+            kin.scale = (float)(-0.5 / (L_.h * L_.h));
+            launch_stencil(L_, ch_[sp].A[ch_[sp].cur].tmap, nocc[sp], kin, ch_[sp].T.at(0), s_);
+            for (int i = 0; i < nocc[sp]; ++i) pairs.push_back({ch_[sp].A[ch_[sp].cur].at(i), ch_[sp].T.at(i)});
+        }
+        red_.dots(pairs, 0, dv);
+        const int nvals = (int)pairs.size();
+        launch_face_max(L_, rho_tot_.at(0), red_.partials(), red_.blocks(), s_);
+        launch_finish_max(red_.partials(), red_.blocks(), red_.res() + nvals, s_);
+        const double* h = red_.read(nvals + 1);
+        double kinetic = 0.0, comp = 0.0;
+        for (int q = 3; q < nvals; ++q) {  // Neumaier over the orbitals (crates/qm-gpu/src/scf.rs:1664-1667)
+            double x = h[q], t = kinetic + x;
+            if (std::fabs(kinetic) >= std::fabs(x)) comp += (kinetic - t) + x; else comp += (x - t) + kinetic;
+            kinetic = t;
+        }
+        kinetic += comp;
+        ks_energy& en = out->energy;
+        en.kinetic = kinetic;
+        en.external_ = h[0];
+        en.hartree = 0.5 * h[1];
+        en.xc = h[2];
+        en.nuclear = e_nn;
+        en.internal = en.kinetic + en.external_ + en.hartree + en.xc + en.nuclear;
+        en.ts = 0.0;
+        en.total = en.internal - en.ts;
+        out->boundary_density = h[nvals];
+        out->electrons[0] = q_out[0];
+        out->electrons[1] = q_out[1];
+        if (out->boundary_density > BOUNDARY_DENSITY_WARN) ++out->n_warnings;
+        if (last_step_maxiter || !(last_step_res <= LAST_STEP_RESIDUAL_FACTOR * eig_lo)) ++out->n_warnings;
+        converged_ = true;
+        have_warm_ = true;
+        profile.readbacks = red_.readbacks - rb0;
+        profile.wall_s = secs(t0);
+        return KS_OK;
+    } catch (const NumericalError& e) {
+        error = e.what();
+        converged_ = false;
+        have_warm_ = false;
+        return KS_NUMERICAL;
+    } catch (const DeviceError& e) {
+        error = e.what();
+        converged_ = false;
+        have_warm_ = false;
+        return KS_DEVICE;
+    }
+}
+
+ks_status Solver::forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n) {
+    if (!converged_) { error = "no converged state"; return KS_NO_STATE; }
+    if (nn <= 0 || nn > 32 || !nuc || !out3n) { error = "invalid arguments"; return KS_INVALID; }
+    try {
+        std::vector<Nuc> hn(nn);
+        for (int i = 0; i < nn; ++i) hn[i] = Nuc{nuc[i].pos[0], nuc[i].pos[1], nuc[i].pos[2], (double)nuc[i].z};
+        nuc_d_.alloc(hn.size() * sizeof(Nuc));
+        KS_CUDA(cudaMemcpyAsync(nuc_d_.p, hn.data(), hn.size() * sizeof(Nuc), cudaMemcpyHostToDevice, s_));
+        // rho = rho_up + rho_dn of the converged state
+        Terms tsum;
+        tsum.count = 2;
+        tsum.x[0] = out_up_.at(0); tsum.c[0] = 1.f;
+        tsum.x[1] = out_dn_.at(0); tsum.c[1] = 1.f;
+        launch_lincomb(L_.F, 1, rho_tot_.at(0), tsum, s_);
+        launch_forces(L_, rho_tot_.at(0), static_cast<const Nuc*>(nuc_d_.p), nn, sigma, red_.partials(), red_.blocks(), s_);
+        launch_finish(red_.partials(), red_.blocks(), 3 * nn, L_.h * L_.h * L_.h, red_.res(), s_);
+        const double* h = red_.read(3 * nn);
+        for (int i = 0; i < 3 * nn; ++i) out3n[i] = h[i];
+        // nuclear-nuclear part (crates/qm/src/forces.rs:219-226)
+        for (int a = 0; a < nn; ++a)
+            for (int b = 0; b < nn; ++b) {
+                if (a == b) continue;
+                double dv[3] = {nuc[a].pos[0] - nuc[b].pos[0], nuc[a].pos[1] - nuc[b].pos[1], nuc[a].pos[2] - nuc[b].pos[2]};
+                double d = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+                if (d < 1e-8) {
+                    error = "nuclei " + std::to_string(std::min(a, b)) + " and " + std::to_string(std::max(a, b)) + " coincide";
+                    return KS_COINCIDENT_NUCLEI;
+                }
+                double sc = (double)nuc[a].z * (double)nuc[b].z / (d * d * d);
+                for (int c = 0; c < 3; ++c) out3n[3 * a + c] += sc * dv[c];
+            }
+        return KS_OK;
+    } catch (const DeviceError& e) {
+        error = e.what();
+        return KS_DEVICE;
+    }
+}
+
+}  // namespace ks

@@ -1,0 +1,169 @@
+// solver.h -- the B200 Kohn-Sham solver behind the C ABI (include/ks_cuda.h).
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "kernels.cuh"
+#include "../../include/ks_cuda.h"
+
+namespace ks {
+
+// Owning device allocation.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t n) { alloc(n); }
+    ~DevBuf() { release(); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    void alloc(size_t n);
+    void release();
+    float* f() const { return static_cast<float*>(p); }
+    double* d() const { return static_cast<double*>(p); }
+};
+
+// A contiguous block of `count` pitched fields with a tensor map over it (stencil input).
+struct Block {
+    DevBuf buf;
+    int count = 0;
+    long long F = 0;
+    CUtensorMap tmap;
+    void create(const Layout& L, int count);
+    float* at(int i) const { return buf.f() + (long long)i * F; }
+};
+
+// Device reductions with a fixed grid (deterministic), results kept on the device until read.
+class Reducer {
+public:
+    void init(const Layout& L, cudaStream_t s, size_t partial_doubles);
+    // sum_p a_p b_p * scale for every pair, written to res()[off + i]
+    void dots(const std::vector<std::pair<const float*, const float*>>& pairs, int off, double scale);
+    // G = scale * S^T [S | T], written to res()[off...] row-major m x (m + mt)
+    void gram(int m, const float* S, int mt, const float* T, int off, double scale = 1.0);
+    double* res() const { return res_.d(); }
+    double* partials() const { return partials_.d(); }
+    int blocks() const { return blocks_; }
+    // copies res[0..count) to the host and synchronises; raises DeviceError on a failed kernel wait
+    const double* read(int count);
+    int readbacks = 0;
+    double* host() const { return host_; }
+    static constexpr int RES_CAP = 1 << 16;
+
+private:
+    Layout L_;
+    cudaStream_t s_ = nullptr;
+    DevBuf partials_, res_;
+    double* host_ = nullptr;
+    int* host_flag_ = nullptr;
+    int blocks_ = 1;
+    int gram_blocks_ = 1;
+
+public:
+    ~Reducer();
+};
+
+struct PoissonStats { int iterations = 0; double residual = 0; int stop = 0; int readbacks = 0; };
+
+// Multigrid-preconditioned CG Hartree solve (crates/qm-gpu/src/poisson.rs:111-343).
+class Poisson {
+public:
+    void init(const Layout& L, cudaStream_t s, Reducer* red);
+    PoissonStats solve(const float* rho, float* v, const CUtensorMap& v_map, double tol, int max_iter);
+    void moments(const float* rho, double* dst_dev);  // 49 f64, dV applied
+
+private:
+    struct Level { MgLevel lv; DevBuf x, b, res, tmp; };
+    void vcycle(const float* rhs, float* z);
+    void cycle(int l, float* x, const float* b);
+    void true_residual(const float* v, const CUtensorMap& v_map);
+    Layout L_;
+    cudaStream_t s_ = nullptr;
+    Reducer* red_ = nullptr;
+    Block r_, p_, ap_, b_, z_, res0_, tmp0_;
+    DevBuf ghost_, scal_, q_;
+    std::vector<Level> levels_;   // coarse levels 1..; level 0 is the fine grid (its x/b are z/r)
+    int fused_from_ = 0;          // first level handled by the single-CTA kernel
+    std::vector<MgLevel> lvdesc_;
+};
+
+struct EigenStats {
+    int iterations = 0;
+    double max_residual = 0;
+    int stop = 0;  // 0 converged, 1 floor, 2 max_iter
+    int readbacks = 0;
+    int restores = 0;
+    bool restores_exhausted = false;
+    double alpha_worst = 0;
+    int fallbacks = 0;
+};
+
+// One spin channel's LOBPCG work space: k vectors, [X | W | P] arenas (ping-pong), [R | HW | HP],
+// HX and the preconditioner scratch.
+struct Channel {
+    int k = 0;
+    Block A[2];
+    int cur = 0;
+    Block T, HX, Q;
+    DevBuf theta_d, lambda_d, coef_d;
+    std::vector<double> evals;
+    void create(const Layout& L, int k);
+    float* X() const { return A[cur].at(0); }
+};
+
+struct SolverOptions { int gram_mode = 0; int n_extra = 0; int init_mode = 0; };
+
+class Solver {
+public:
+    Solver(int n, double h, const SolverOptions& o);
+    ~Solver();
+    ks_status solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,
+                    void* user, ks_stats* out);
+    ks_status forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n);
+    EigenStats lobpcg(Channel& ch, const float* V, double tol, double guess_tol, int max_iter, int checked);
+    std::string error;
+    const Layout& layout() const { return L_; }
+    cudaStream_t stream() const { return s_; }
+    bool has_state() const { return converged_; }
+    int count(int spin) const { return nocc_[spin]; }
+    const Channel& channel(int spin) const { return ch_[spin]; }
+    const float* rho(int spin) const { return spin ? out_dn_.at(0) : out_up_.at(0); }
+    const float* v_nuc() const { return vnuc_.at(0); }
+    const float* v_h() const { return vh_.at(0); }
+    ks_profile profile{};
+    Poisson& poisson() { return poisson_; }
+    Reducer& reducer() { return red_; }
+
+private:
+    void ensure_channel(int spin, int k);
+    void gram_checked(int m, const float* S, int mt, const float* T);
+    Layout L_;
+    SolverOptions opt_;
+    cudaStream_t s_ = nullptr;
+    Reducer red_;
+    Poisson poisson_;
+    Channel ch_[2];
+    int nocc_[2] = {0, 0};
+    Block vnuc_, vh_, in_up_, in_dn_, out_up_, out_dn_, rho_tot_, v_up_, v_dn_, exc_, ones_, kin_;
+    struct Entry { Block rho_up, rho_dn, r_up, r_dn; };
+    std::vector<Entry> diis_pool_;
+    DevBuf nuc_d_;
+    bool converged_ = false;
+    bool have_warm_ = false;
+    double floor_;
+};
+
+// Residual floor model of an f32-stored eigenvector (crates/qm-gpu/src/eigen.rs:313-318).
+double residual_floor_estimate(double h);
+// Generalised Rayleigh-Ritz on a raw subspace (crates/qm-gpu/src/eigen.rs:515-542): lowest nk pairs
+// of A c = theta B c; C column-major m x nk. Throws NumericalError on a zero-norm column or rank loss.
+double rayleigh_ritz(int m, const std::vector<double>& A, const std::vector<double>& B, int nk, std::vector<double>& theta,
+                     std::vector<double>& C);
+
+}  // namespace ks

@@ -1,0 +1,382 @@
+"""Python mirror of the reference's ``qm_gpu::GpuSolver`` over the C ABI of ``libks_b200.so``.
+
+The reference's host side is Rust (crates/qm-gpu/src/scf.rs:1042-1235); this module is the
+binding a Python caller uses, with the reference's names and error behaviour:
+
+- ``GpuSolver(grid_n, h)``            -> ``GpuSolver::new`` (scf.rs:1083)
+- ``solver.solve(system, settings, warm)`` -> ``GpuSolver::solve`` (scf.rs:1195); raises the
+  ``QmError`` subclasses below on failure, as the reference returns ``Err(QmError)``
+- ``solver.forces(nuclei, sigma)``   -> ``GpuSolver::forces`` (forces.rs:239)
+- ``solver.evals()``, ``density()``, ``orbitals()``, ``potentials()`` -> ``state()`` / ``ks_state``
+
+The CUDA library is required: importing this module on a machine where ``libks_b200.so`` is
+missing or cannot be loaded raises at load time -- there is no CPU fallback.
+"""
+import ctypes
+import dataclasses
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libks_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "ks_cuda.h")
+
+
+class Nucleus(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_double * 3), ("z", ctypes.c_int)]
+
+
+class _Settings(ctypes.Structure):
+    _fields_ = [("sigma", ctypes.c_double), ("tol", ctypes.c_double), ("mixing", ctypes.c_double),
+                ("eig_tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("diis_history", ctypes.c_int),
+                ("stall_window", ctypes.c_int)]
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [("gram_mode", ctypes.c_int), ("n_extra", ctypes.c_int), ("init_mode", ctypes.c_int),
+                ("reserved", ctypes.c_int)]
+
+
+class _Energy(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("kinetic", "external", "hartree", "xc", "nuclear", "internal", "ts", "total")]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("delta_rho", ctypes.c_double), ("energy", _Energy),
+                ("boundary_density", ctypes.c_double), ("max_eigen_residual", ctypes.c_double),
+                ("poisson_residual", ctypes.c_double), ("poisson_iterations", ctypes.c_int),
+                ("electrons", ctypes.c_double * 2), ("tol_used", ctypes.c_double), ("n_warnings", ctypes.c_int)]
+
+
+class _Profile(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("steps", "readbacks", "eigen_iterations", "poisson_iterations", "eigen_calls",
+                                              "diis_resets")] + \
+               [(n, ctypes.c_double) for n in ("wall_s", "start_s", "poisson_s", "eigen_s")]
+
+
+ABORT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
+
+KS_OK, KS_COINCIDENT_NUCLEI, KS_NOT_CONVERGED, KS_STALLED, KS_NUMERICAL, KS_DEVICE, KS_INVALID, KS_ABORTED, KS_NO_STATE = range(9)
+
+
+class QmError(RuntimeError):
+    """qm::QmError (crates/qm/src/error.rs:4-31)."""
+
+
+class CoincidentNuclei(QmError):
+    pass
+
+
+class ScfNotConverged(QmError):
+    pass
+
+
+class ScfStalled(QmError):
+    pass
+
+
+class Numerical(QmError):
+    pass
+
+
+class Device(QmError):
+    pass
+
+
+class Aborted(QmError):
+    pass
+
+
+class NoState(QmError):
+    pass
+
+
+_ERRORS = {KS_COINCIDENT_NUCLEI: CoincidentNuclei, KS_NOT_CONVERGED: ScfNotConverged, KS_STALLED: ScfStalled,
+           KS_NUMERICAL: Numerical, KS_DEVICE: Device, KS_INVALID: ValueError, KS_ABORTED: Aborted, KS_NO_STATE: NoState}
+
+EXPORTED = [
+    "ks_solver_create", "ks_solver_destroy", "ks_solve", "ks_forces", "ks_last_error", "ks_state_counts", "ks_state_evals",
+    "ks_state_density", "ks_state_potentials", "ks_state_orbitals", "ks_profile_get", "ks_apply_hamiltonian",
+    "ks_apply_laplacian", "ks_apply_precond", "ks_xc_lsda", "ks_nuclear_potential", "ks_poisson_solve", "ks_gram", "ks_lobpcg",
+    "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device",
+]
+
+
+def build():
+    """Compiles libks_b200.so for sm_100a in place (make)."""
+    subprocess.run(["make", "-s", "-j8", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises OSError when it is missing: no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is not built (run make -C {HERE})")
+        L = ctypes.CDLL(LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.ks_solver_create.restype = ctypes.c_void_p
+        L.ks_solver_create.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(_Options)]
+        L.ks_solver_destroy.argtypes = [ctypes.c_void_p]
+        L.ks_last_error.restype = ctypes.c_char_p
+        L.ks_last_error.argtypes = [ctypes.c_void_p]
+        L.ks_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                               ctypes.POINTER(_Settings), ctypes.c_int, ABORT_FN, ctypes.c_void_p, ctypes.POINTER(_Stats)]
+        L.ks_forces.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, dp]
+        L.ks_state_counts.argtypes = [ctypes.c_void_p, ip, ip]
+        L.ks_state_evals.argtypes = [ctypes.c_void_p, dp, dp]
+        L.ks_state_density.argtypes = [ctypes.c_void_p, dp, dp]
+        L.ks_state_potentials.argtypes = [ctypes.c_void_p, dp, dp]
+        L.ks_state_orbitals.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+        L.ks_profile_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Profile)]
+        L.ks_apply_hamiltonian.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, dp, dp, dp]
+        L.ks_apply_laplacian.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
+        L.ks_apply_precond.argtypes = [ctypes.c_int, ctypes.c_double, dp, ctypes.c_double, dp, dp]
+        L.ks_xc_lsda.argtypes = [ctypes.c_size_t, dp, dp, dp, dp, dp]
+        L.ks_nuclear_potential.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, dp]
+        L.ks_poisson_solve.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp, ctypes.c_double, ctypes.c_int, dp, ip]
+        L.ks_gram.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int, dp]
+        L.ks_lobpcg.argtypes = [ctypes.c_int, ctypes.c_double, dp, ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                dp, ip]
+        L.ks_multipole_moments.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
+        L.ks_field_pitch.argtypes = [ctypes.c_int]
+        L.ks_hpsi_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _f64(a, size=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if size is not None and a.size != size:
+        raise ValueError(f"expected {size} values, got {a.size}")
+    return a
+
+
+def _check(status, handle=None):
+    if status != KS_OK:
+        msg = lib().ks_last_error(handle).decode(errors="replace")
+        raise _ERRORS.get(status, QmError)(msg)
+
+
+def nuclei_array(nuclei):
+    """[(x, y, z, Z), ...] (Bohr, atomic number) -> ctypes array."""
+    arr = (Nucleus * max(len(nuclei), 1))()
+    for i, (x, y, z, Z) in enumerate(nuclei):
+        arr[i].pos[0], arr[i].pos[1], arr[i].pos[2] = float(x), float(y), float(z)
+        arr[i].z = int(Z)
+    return arr
+
+
+@dataclasses.dataclass
+class ScfSettings:
+    """qm::ScfSettings (crates/qm/src/scf.rs:375) with Aufbau occupations; sigma None = h."""
+    sigma: float = None
+    tol: float = 1e-6
+    max_iter: int = 200
+    mixing: float = 0.3
+    eig_tol: float = 1e-6
+    diis_history: int = 6
+    stall_window: int = 50
+
+
+@dataclasses.dataclass
+class System:
+    """qm::System (crates/qm/src/scf.rs:329): nuclei [(x, y, z, Z)] and electrons per spin."""
+    nuclei: list
+    n_up: int
+    n_dn: int
+
+
+def spin_split(total, multiplicity=None):
+    """(n_up, n_dn) for `total` electrons (crates/qm/src/scf.rs:333-345)."""
+    if total < 0:
+        raise ValueError("negative electron count")
+    if multiplicity is None:
+        unpaired = total % 2
+    else:
+        m = int(multiplicity)
+        if not (m >= 1 and m - 1 <= total and (total - (m - 1)) % 2 == 0):
+            raise ValueError("bad multiplicity")
+        unpaired = m - 1
+    n_dn = (total - unpaired) // 2
+    return n_dn + unpaired, n_dn
+
+
+def neutral_system(nuclei, charge=0, multiplicity=None):
+    """System::new: N = sum Z - charge, the lowest multiplicity unless given."""
+    n_up, n_dn = spin_split(sum(int(z) for *_, z in nuclei) - charge, multiplicity)
+    return System(list(nuclei), n_up, n_dn)
+
+
+class GpuSolver:
+    """One grid, one CUDA stream, every device buffer of the solve (crates/qm-gpu/src/scf.rs:1042)."""
+
+    GRAM_FP32, GRAM_TENSOR = 0, 1
+
+    def __init__(self, n, h, gram_mode=0, n_extra=0, init_mode=0):
+        opts = _Options(gram_mode, n_extra, init_mode, 0)
+        self._h = lib().ks_solver_create(int(n), float(h), ctypes.byref(opts))
+        if not self._h:
+            raise Device(lib().ks_last_error(None).decode(errors="replace"))
+        self.n, self.h = int(n), float(h)
+        self._abort_ref = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ks_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def solve(self, system, settings=None, warm=False, should_abort=None):
+        """Runs the SCF; returns the stats dict (ScfStats) or raises a QmError subclass."""
+        s = settings or ScfSettings()
+        cs = _Settings(self.h if s.sigma is None else s.sigma, s.tol, s.mixing, s.eig_tol, s.max_iter, s.diis_history,
+                       s.stall_window)
+        st = _Stats()
+        arr = nuclei_array(system.nuclei)
+        cb = ABORT_FN(lambda _u: 1 if should_abort() else 0) if should_abort else ABORT_FN()
+        self._abort_ref = cb
+        rc = lib().ks_solve(self._h, arr, len(system.nuclei), int(system.n_up), int(system.n_dn), ctypes.byref(cs),
+                            1 if warm else 0, cb, None, ctypes.byref(st))
+        _check(rc, self._h)
+        e = st.energy
+        return {
+            "iterations": st.iterations, "delta_rho": st.delta_rho,
+            "energy": {n: getattr(e, n) for n, _ in _Energy._fields_},
+            "boundary_density": st.boundary_density, "max_eigen_residual": st.max_eigen_residual,
+            "poisson_residual": st.poisson_residual, "poisson_iterations": st.poisson_iterations,
+            "electrons": list(st.electrons), "tol_used": st.tol_used, "n_warnings": st.n_warnings,
+        }
+
+    def forces(self, nuclei, sigma=None):
+        out = np.empty(3 * len(nuclei))
+        _check(lib().ks_forces(self._h, nuclei_array(nuclei), len(nuclei), float(self.h if sigma is None else sigma), _p(out)), self._h)
+        return out.reshape(-1, 3)
+
+    def counts(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(lib().ks_state_counts(self._h, ctypes.byref(a), ctypes.byref(b)), self._h)
+        return a.value, b.value
+
+    def evals(self):
+        nu, nd = self.counts()
+        up, dn = np.empty(max(nu, 1)), np.empty(max(nd, 1))
+        _check(lib().ks_state_evals(self._h, _p(up), _p(dn)), self._h)
+        return up[:nu], dn[:nd]
+
+    def density(self):
+        up, dn = np.empty(self.n ** 3), np.empty(self.n ** 3)
+        _check(lib().ks_state_density(self._h, _p(up), _p(dn)), self._h)
+        return up, dn
+
+    def potentials(self):
+        a, b = np.empty(self.n ** 3), np.empty(self.n ** 3)
+        _check(lib().ks_state_potentials(self._h, _p(a), _p(b)), self._h)
+        return a, b
+
+    def orbitals(self, spin):
+        nu, nd = self.counts()
+        k = nd if spin else nu
+        out = np.empty(max(k, 1) * self.n ** 3)
+        _check(lib().ks_state_orbitals(self._h, int(spin), _p(out)), self._h)
+        return out[: k * self.n ** 3].reshape(k, self.n ** 3)
+
+    def profile(self):
+        p = _Profile()
+        _check(lib().ks_profile_get(self._h, ctypes.byref(p)), self._h)
+        return {n: getattr(p, n) for n, _ in _Profile._fields_}
+
+
+# ---- grid-kernel entry points (host f64 in/out)
+def apply_hamiltonian(n, h, psi, v):
+    psi = _f64(psi)
+    count = psi.size // n ** 3
+    out = np.empty(count * n ** 3)
+    _check(lib().ks_apply_hamiltonian(n, h, count, _p(psi), _p(_f64(v, n ** 3)), _p(out)))
+    return out.reshape(psi.shape)
+
+
+def apply_laplacian(n, h, f):
+    out = np.empty(n ** 3)
+    _check(lib().ks_apply_laplacian(n, h, _p(_f64(f, n ** 3)), _p(out)))
+    return out
+
+
+def apply_precond(n, h, v, lam, r):
+    out = np.empty(n ** 3)
+    _check(lib().ks_apply_precond(n, h, _p(_f64(v, n ** 3)), float(lam), _p(_f64(r, n ** 3)), _p(out)))
+    return out
+
+
+def xc_lsda(up, dn):
+    up, dn = _f64(up), _f64(dn, np.size(up))
+    e, vu, vd = np.empty_like(up), np.empty_like(up), np.empty_like(up)
+    _check(lib().ks_xc_lsda(ctypes.c_size_t(up.size), _p(up), _p(dn), _p(e), _p(vu), _p(vd)))
+    return e, vu, vd
+
+
+def nuclear_potential(n, h, nuclei, sigma):
+    out = np.empty(n ** 3)
+    _check(lib().ks_nuclear_potential(n, h, nuclei_array(nuclei), len(nuclei), float(sigma), _p(out)))
+    return out
+
+
+def poisson_solve(n, h, rho, v0=None, tol=1e-8, max_iter=5000):
+    v = np.zeros(n ** 3) if v0 is None else _f64(v0, n ** 3).copy()
+    res, it = ctypes.c_double(), ctypes.c_int()
+    _check(lib().ks_poisson_solve(n, h, _p(_f64(rho, n ** 3)), _p(v), float(tol), int(max_iter), ctypes.byref(res), ctypes.byref(it)))
+    return v, it.value, res.value
+
+
+def multipole_moments(n, h, rho):
+    q = np.empty(49)
+    _check(lib().ks_multipole_moments(n, h, _p(_f64(rho, n ** 3)), _p(q)))
+    return q
+
+
+def gram(n, s, t, gram_mode=0):
+    s = _f64(s).reshape(-1, n ** 3)
+    t = _f64(t).reshape(-1, n ** 3)
+    m, mt = s.shape[0], t.shape[0]
+    out = np.empty(m * (m + mt))
+    _check(lib().ks_gram(n, m, _p(s), mt, _p(t), int(gram_mode), _p(out)))
+    return out.reshape(m, m + mt)
+
+
+def lobpcg(n, h, v, x0, tol=1e-5, max_iter=500, gram_mode=0):
+    x = _f64(x0).copy()
+    k = x.shape[0]
+    ev = np.empty(k)
+    mr, it = ctypes.c_double(), ctypes.c_int()
+    _check(lib().ks_lobpcg(n, h, _p(_f64(v, n ** 3)), k, _p(x), _p(ev), float(tol), int(max_iter), int(gram_mode),
+                           ctypes.byref(mr), ctypes.byref(it)))
+    return ev, x, it.value, mr.value
+
+
+def field_pitch(n):
+    return lib().ks_field_pitch(int(n))
+
+
+def hpsi_device(stream, n, h, count, psi_ptr, v_ptr, out_ptr):
+    """H psi on device pointers in the pitched layout (ks_hpsi_device)."""
+    _check(lib().ks_hpsi_device(ctypes.c_void_p(stream), int(n), float(h), int(count), ctypes.c_void_p(psi_ptr),
+                                ctypes.c_void_p(v_ptr), ctypes.c_void_p(out_ptr)))

@@ -1,0 +1,144 @@
+/*
+ * ks_cuda.h -- C ABI of the B200 (sm_100a) real-space Kohn-Sham solver.
+ *
+ * This is the drop-in boundary for the reference's GPU solver, the Rust type
+ * `qm_gpu::GpuSolver` (crates/qm-gpu/src/scf.rs:1042-1235, crates/qm-gpu/src/forces.rs:239).
+ * A handle owns one grid, one CUDA stream and every device buffer of the solve; it is
+ * thread-affine like the reference (`Send`, not `Sync`: one handle per worker thread). Every
+ * call is synchronous with respect to the host and returns a status -- the library never traps.
+ *
+ * Array conventions at the boundary: grids are cubic n^3 with spacing h (Bohr), origin
+ * -(n-1)h/2 on every axis, and a host array of a grid field is the reference's `qm::Grid`
+ * layout, f64, idx = i + n*(j + n*k) (crates/qm/src/grid.rs:1-16). Energies in Hartree, forces
+ * in Hartree/Bohr. Nothing here takes a torch type.
+ */
+#ifndef KS_CUDA_H
+#define KS_CUDA_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* qm::Nucleus (crates/qm/src/nuclear.rs:88-92): position in Bohr and atomic number. */
+typedef struct { double pos[3]; int z; } ks_nucleus;
+
+/* qm::QmError (crates/qm/src/error.rs:4-31) plus the C-side conditions. */
+typedef enum {
+    KS_OK = 0,
+    KS_COINCIDENT_NUCLEI = 1, /* QmError::CoincidentNuclei */
+    KS_NOT_CONVERGED = 2,     /* QmError::ScfNotConverged */
+    KS_STALLED = 3,           /* QmError::ScfStalled */
+    KS_NUMERICAL = 4,         /* QmError::Numerical */
+    KS_DEVICE = 5,            /* QmError::Device (a CUDA error or a kernel wait that gave up) */
+    KS_INVALID = 6,           /* bad argument (the reference panics on these) */
+    KS_ABORTED = 7,           /* should_abort returned nonzero: the iterate is parked as the warm start */
+    KS_NO_STATE = 8           /* forces / state access without a converged state */
+} ks_status;
+
+/* qm::ScfSettings (crates/qm/src/scf.rs:375), Aufbau occupations. */
+typedef struct {
+    double sigma;      /* nuclear smearing width (Bohr); the reference's default is h */
+    double tol;        /* on the density change dRho = integral |rho_out - rho_in| (electrons) */
+    double mixing;     /* DIIS step alpha (0.3) */
+    double eig_tol;    /* LOBPCG residual tolerance (1e-6) */
+    int max_iter;      /* SCF iteration cap (200) */
+    int diis_history;  /* Pulay history (6) */
+    int stall_window;  /* stall stop W (50; 0 = off) */
+} ks_settings;
+
+/* Solver construction options (no reference counterpart: B200 choices). */
+typedef struct {
+    int gram_mode;     /* LOBPCG Gram: 0 = FP32 CUDA cores ("plain FP32"), 1 = tensor cores (3xTF32, "mixed") */
+    int n_extra;       /* extra LOBPCG bands per occupied spin channel (buffer columns, not occupied) */
+    int init_mode;     /* cold orbitals: 0 = the reference's initial_orbitals (crates/qm/src/scf.rs:636-644), 1 = uniform(-1,1) */
+    int reserved;
+} ks_options;
+
+/* qm::Energy (crates/qm/src/scf.rs:533) */
+typedef struct { double kinetic, external_, hartree, xc, nuclear, internal, ts, total; } ks_energy;
+
+/* qm::ScfStats (crates/qm/src/scf.rs:558-574), Aufbau subset. */
+typedef struct {
+    int iterations;
+    double delta_rho;
+    ks_energy energy;
+    double boundary_density;
+    double max_eigen_residual;
+    double poisson_residual;
+    int poisson_iterations;
+    double electrons[2];
+    double tol_used;
+    int n_warnings;
+} ks_stats;
+
+/* qm_gpu::SolveProfile (crates/qm-gpu/src/scf.rs:448-514), subset. */
+typedef struct {
+    int steps, readbacks, eigen_iterations, poisson_iterations, eigen_calls, diis_resets;
+    double wall_s, start_s, poisson_s, eigen_s;
+} ks_profile;
+
+/* Polled before every SCF step (GpuSolver::solve_with, crates/qm-gpu/src/scf.rs:1208): nonzero abandons the solve. */
+typedef int (*ks_abort_fn)(void* user);
+
+/* GpuSolver::new (crates/qm-gpu/src/scf.rs:1083): a solver for the cubic grid n^3, spacing h, on the
+   current CUDA device. opts may be NULL (defaults: plain FP32 Gram, no extra bands, reference guess).
+   Returns NULL on failure (ks_last_error(NULL) holds the message). */
+void* ks_solver_create(int n, double h, const ks_options* opts);
+void ks_solver_destroy(void* solver);
+
+/* GpuSolver::solve / solve_with (crates/qm-gpu/src/scf.rs:1195-1235): n_up / n_dn electrons per spin,
+   warm != 0 reuses the last converged state when its counts match. abort may be NULL. */
+ks_status ks_solve(void* solver, const ks_nucleus* nuclei, int n_nuclei, int n_up, int n_dn, const ks_settings* settings,
+                   int warm, ks_abort_fn abort_fn, void* user, ks_stats* out);
+
+/* GpuSolver::forces (crates/qm-gpu/src/forces.rs:239): Hellmann-Feynman force on each nucleus
+   (out3n[3*i + axis]) from the converged state, plus the point nuclear repulsion. */
+ks_status ks_forces(void* solver, const ks_nucleus* nuclei, int n_nuclei, double sigma, double* out3n);
+
+/* The message of the last failure on this handle (or of ks_solver_create when solver is NULL). */
+const char* ks_last_error(const void* solver);
+
+/* State access (GpuSolver::state / ks_state, crates/qm-gpu/src/scf.rs:1172, :1713-1775). */
+ks_status ks_state_counts(const void* solver, int* n_up, int* n_dn);
+ks_status ks_state_evals(const void* solver, double* up, double* dn);
+ks_status ks_state_density(const void* solver, double* rho_up, double* rho_dn);   /* n^3 each */
+ks_status ks_state_potentials(const void* solver, double* v_nuc, double* v_h);     /* n^3 each */
+ks_status ks_state_orbitals(const void* solver, int spin, double* out);            /* count * n^3 */
+ks_status ks_profile_get(const void* solver, ks_profile* out);                     /* GpuSolver::profile */
+
+/* ---- grid-kernel entry points (host f64 in / out; the kernels run on the solver's device in f32) ----
+   One parity hook per hot-path kernel; each mirrors the reference kernel named beside it. */
+/* hamiltonian (crates/qm-gpu/src/shaders/stencil.wgsl:77-90): out_v = -1/2 lap psi_v + V psi_v for count vectors */
+ks_status ks_apply_hamiltonian(int n, double h, int count, const double* psi, const double* v, double* out);
+/* laplacian (stencil.wgsl:67-75) */
+ks_status ks_apply_laplacian(int n, double h, const double* f, double* out);
+/* precond_init + jacobi_step x3 (shaders/eigen.wgsl:25-34, stencil.wgsl:94-106): w = T r at shift lambda */
+ks_status ks_apply_precond(int n, double h, const double* v, double lambda, const double* r, double* w);
+/* xc_lsda (shaders/xc.wgsl:137-152): e = n eps_xc, v_up, v_dn for len points */
+ks_status ks_xc_lsda(size_t len, const double* up, const double* dn, double* e, double* vu, double* vd);
+/* nuclear_potential (shaders/nuclear.wgsl:124-139) */
+ks_status ks_nuclear_potential(int n, double h, const ks_nucleus* nuclei, int n_nuclei, double sigma, double* out);
+/* GpuPoisson::solve (crates/qm-gpu/src/poisson.rs:284-342): MG-PCG with l<=6 multipole ghosts.
+   v is the initial guess and the output; returns the true relative residual and the iteration count. */
+ks_status ks_poisson_solve(int n, double h, const double* rho, double* v, double tol, int max_iter, double* residual,
+                           int* iterations);
+/* Reducer::gram / block_dots (crates/qm-gpu/src/reduce.rs:340-420): G = S^T [S | T], m and mt fields, gram_mode as
+   in ks_options; out row-major m x (m + mt). */
+ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gram_mode, double* out);
+/* lobpcg (crates/qm-gpu/src/eigen.rs:685-1000) on H = -1/2 lap + V: k vectors x (guess and result), evals out. */
+ks_status ks_lobpcg(int n, double h, const double* v, int k, double* x, double* evals, double tol, int max_iter,
+                    int gram_mode, double* max_residual, int* iterations);
+/* multipole moments Q_lm = sum rho R_lm dV (crates/qm-gpu/src/poisson.rs:237-244) */
+ks_status ks_multipole_moments(int n, double h, const double* rho, double* q49);
+
+/* ---- device-pointer entry points for callers that keep fields on the GPU (bench, integrations) ----
+   Fields are in the pitched layout: element (i, j, k) at (k*n + j)*P + i, P = ks_field_pitch(n),
+   F = n*n*P floats per field, blocks of fields contiguous with stride F; pad columns hold 0. */
+int ks_field_pitch(int n);
+/* out_v = -1/2 lap psi_v + V psi_v, v = 0..count-1, enqueued on `stream` (a cudaStream_t, NULL = legacy). */
+ks_status ks_hpsi_device(void* stream, int n, double h, int count, const float* psi, const float* v, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
