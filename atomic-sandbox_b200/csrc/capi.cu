@@ -333,7 +333,8 @@ ks_status ks_multipole_moments(int n, double h, const double* rho, double* q49) 
 }
 
 ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gram_mode, double* out) {
-    if (n < 1 || m < 1 || mt < 0 || !s || (mt > 0 && !t) || !out || gram_mode != 0) return fail(nullptr, KS_INVALID, "invalid arguments");
+    if (n < 1 || m < 1 || mt < 0 || !s || (mt > 0 && !t) || !out || gram_mode < 0 || gram_mode > 1 || (gram_mode == 1 && mt < 1))
+        return fail(nullptr, KS_INVALID, "invalid arguments");
     return guarded(nullptr, [&] {
         Solver so(n, 1.0, SolverOptions());
         Scratch sc(n, 1.0);
@@ -342,6 +343,7 @@ ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gr
         T.create(so.layout(), std::max(mt, 1));
         sc.upload_fields(s, m, S);
         if (mt > 0) sc.upload_fields(t, mt, T);
+        so.reducer().gram_mode = gram_mode;
         so.reducer().gram(m, S.at(0), mt, T.at(0), 0);
         const double* g = so.reducer().read(m * (m + mt));
         std::memcpy(out, g, sizeof(double) * m * (m + mt));
@@ -351,9 +353,11 @@ ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gr
 
 ks_status ks_lobpcg(int n, double h, const double* v, int k, double* x, double* evals, double tol, int max_iter, int gram_mode,
                     double* max_residual, int* iterations) {
-    if (!valid_grid(n, h) || !v || k < 1 || !x || !evals || gram_mode != 0) return fail(nullptr, KS_INVALID, "invalid arguments");
+    if (!valid_grid(n, h) || !v || k < 1 || !x || !evals || gram_mode < 0 || gram_mode > 1) return fail(nullptr, KS_INVALID, "invalid arguments");
     return guarded(nullptr, [&] {
-        Solver so(n, h, SolverOptions());
+        SolverOptions o;
+        o.gram_mode = gram_mode;
+        Solver so(n, h, o);
         const Layout& L = so.layout();
         Scratch sc(n, h);
         Channel ch;
@@ -373,6 +377,13 @@ ks_status ks_lobpcg(int n, double h, const double* v, int k, double* x, double* 
 }
 
 int ks_field_pitch(int n) { return Layout::make(n, 1.0).P; }
+
+long long ks_launch_count(void) { return ks::launch_count(); }
+
+void* ks_solver_stream(void* solver) {
+    auto* h = static_cast<Handle*>(solver);
+    return h ? static_cast<void*>(h->solver->stream()) : nullptr;
+}
 
 ks_status ks_hpsi_device(void* stream, int n, double h, int count, const float* psi, const float* v, float* out) {
     if (!valid_grid(n, h) || count < 1 || !psi || !v || !out) return fail(nullptr, KS_INVALID, "invalid arguments");

@@ -54,7 +54,10 @@ inline void check_cuda(cudaError_t e, const char* what, const char* file, int li
     }
 }
 #define KS_CUDA(call) ::ks::check_cuda((call), #call, __FILE__, __LINE__)
-#define KS_LAUNCH_CHECK() ::ks::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+// Every kernel launch of the library goes through this check, which also counts it
+// (ks_launch_count: the number of this library's kernels launched by the process).
+void count_launch();
+#define KS_LAUNCH_CHECK() (::ks::count_launch(), ::ks::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 

@@ -17,17 +17,27 @@ namespace {
 
 constexpr int TPB = 256;
 
-__global__ void finish_kernel(const double* __restrict__ partials, int blocks, int nvals, double scale, double* __restrict__ out) {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per value: lane l sums the partials of CTAs l, l+32, ... (Neumaier), then the lanes are
+// combined by a fixed shuffle tree -- the same order on every run. With trows > 0 the value v =
+// r*tcols + c is written transposed, to out[c*trows + r].
+__global__ void finish_kernel(const double* __restrict__ partials, int blocks, int nvals, double scale, double* __restrict__ out,
+                              int trows, int tcols) {
+    const int v = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     if (v >= nvals) return;
     double sum = 0.0, comp = 0.0;
-    for (int b = 0; b < blocks; ++b) {
+    for (int b = lane; b < blocks; b += 32) {
         double x = partials[(size_t)b * nvals + v];
         double t = sum + x;
         if (fabs(sum) >= fabs(x)) comp += (sum - t) + x; else comp += (x - t) + sum;
         sum = t;
     }
-    out[v] = (sum + comp) * scale;
+    double total = warp_sum(sum + comp);
+    if (lane == 0) {
+        int o = v;
+        if (trows > 0) o = (v % tcols) * trows + v / tcols;
+        out[o] = total * scale;
+    }
 }
 
 __global__ void finish_max_kernel(const double* __restrict__ partials, int blocks, double* __restrict__ out) {
@@ -207,7 +217,12 @@ int reduce_blocks(long long F) {
 }
 
 void launch_finish(const double* partials, int blocks, int nvals, double scale, double* out, cudaStream_t s) {
-    finish_kernel<<<ceil_div(nvals, 128), 128, 0, s>>>(partials, blocks, nvals, scale, out);
+    finish_kernel<<<ceil_div((long long)nvals * 32, 256), 256, 0, s>>>(partials, blocks, nvals, scale, out, 0, 0);
+    KS_LAUNCH_CHECK();
+}
+
+void launch_finish_transposed(const double* partials, int blocks, int rows, int cols, double scale, double* out, cudaStream_t s) {
+    finish_kernel<<<ceil_div((long long)rows * cols * 32, 256), 256, 0, s>>>(partials, blocks, rows * cols, scale, out, rows, cols);
     KS_LAUNCH_CHECK();
 }
 

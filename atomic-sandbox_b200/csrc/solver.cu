@@ -15,6 +15,7 @@
 // channel at once, and the SCF's charge renormalisation is a device-side scale.
 #include "solver.h"
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -34,6 +35,10 @@ int sm_count() {
     }
     return count;
 }
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 int* device_error_flag() {
     static int* flags[64] = {nullptr};
@@ -260,6 +265,16 @@ void Reducer::dots(const std::vector<std::pair<const float*, const float*>>& pai
 }
 
 void Reducer::gram(int m, const float* S, int mt, const float* T, int off, double scale) {
+    if (gram_mode == 1) {
+        // tensor cores: partials of D = [S | T]^T S, finished transposed into G = S^T [S | T]
+        if (m > 64 || ((m + 7) & ~7) + mt > 128) throw std::invalid_argument("tensor-core Gram: block too large (m <= 64, round8(m) + mt <= 128)");
+        const int blocks = gram_tc_blocks();
+        const size_t need = (size_t)blocks * m * (m + mt);
+        if (need * sizeof(double) > partials_.bytes) partials_.alloc(need * sizeof(double));
+        launch_gram_tc(L_.F, m, S, mt, T, partials_.d(), s_);
+        launch_finish_transposed(partials_.d(), blocks, m + mt, m, scale, res_.d() + off, s_);
+        return;
+    }
     const size_t need = (size_t)gram_blocks_ * m * (m + mt);
     if (need * sizeof(double) > partials_.bytes) partials_.alloc(need * sizeof(double));
     launch_gram(L_.F, m, S, mt, T, partials_.d(), gram_blocks_, s_);
@@ -493,7 +508,7 @@ void Solver::ensure_channel(int spin, int k) {
 }
 
 void Solver::gram_checked(int m, const float* S, int mt, const float* T) {
-    if (opt_.gram_mode != 0) throw std::invalid_argument("gram_mode 1 (tensor cores) is not built in this library");
+    red_.gram_mode = opt_.gram_mode;
     red_.gram(m, S, mt, T, 0, L_.h * L_.h * L_.h);  // the L2 product <a, b> = h^3 sum a b
 }
 

@@ -53,6 +53,7 @@ public:
     // copies res[0..count) to the host and synchronises; raises DeviceError on a failed kernel wait
     const double* read(int count);
     int readbacks = 0;
+    int gram_mode = 0;  // 0: CUDA-core f32 Gram, 1: tensor-core 3xTF32 Gram
     double* host() const { return host_; }
     static constexpr int RES_CAP = 1 << 16;
 
@@ -158,6 +159,8 @@ private:
     bool have_warm_ = false;
     double floor_;
 };
+
+long long launch_count();
 
 // Residual floor model of an f32-stored eigenvector (crates/qm-gpu/src/eigen.rs:313-318).
 double residual_floor_estimate(double h);

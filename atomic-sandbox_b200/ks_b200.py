@@ -100,7 +100,7 @@ EXPORTED = [
     "ks_solver_create", "ks_solver_destroy", "ks_solve", "ks_forces", "ks_last_error", "ks_state_counts", "ks_state_evals",
     "ks_state_density", "ks_state_potentials", "ks_state_orbitals", "ks_profile_get", "ks_apply_hamiltonian",
     "ks_apply_laplacian", "ks_apply_precond", "ks_xc_lsda", "ks_nuclear_potential", "ks_poisson_solve", "ks_gram", "ks_lobpcg",
-    "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device",
+    "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
 ]
 
 
@@ -146,6 +146,10 @@ def lib():
                                 dp, ip]
         L.ks_multipole_moments.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
         L.ks_field_pitch.argtypes = [ctypes.c_int]
+        L.ks_launch_count.restype = ctypes.c_longlong
+        L.ks_launch_count.argtypes = []
+        L.ks_solver_stream.restype = ctypes.c_void_p
+        L.ks_solver_stream.argtypes = [ctypes.c_void_p]
         L.ks_hpsi_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p]
         _lib = L
@@ -300,6 +304,10 @@ class GpuSolver:
         _check(lib().ks_state_orbitals(self._h, int(spin), _p(out)), self._h)
         return out[: k * self.n ** 3].reshape(k, self.n ** 3)
 
+    def stream(self):
+        """The cudaStream_t (as an int) every kernel of this solver runs on."""
+        return lib().ks_solver_stream(self._h)
+
     def profile(self):
         p = _Profile()
         _check(lib().ks_profile_get(self._h, ctypes.byref(p)), self._h)
@@ -374,6 +382,11 @@ def lobpcg(n, h, v, x0, tol=1e-5, max_iter=500, gram_mode=0):
 
 def field_pitch(n):
     return lib().ks_field_pitch(int(n))
+
+
+def launch_count():
+    """Kernels of this library launched so far by the process."""
+    return lib().ks_launch_count()
 
 
 def hpsi_device(stream, n, h, count, psi_ptr, v_ptr, out_ptr):

@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark: time for water on a 95^3 grid to converge (dRho < 1e-6), B200, through the C ABI.
+
+Workload (the north-star configuration): O at the origin, H at (+-1.43, 1.11, 0) Bohr (O-H 1.81 Bohr,
+104.5 deg), cubic 95^3 grid at h = 0.25 Bohr, Gaussian nuclear smearing sigma = 0.5 Bohr, LSDA
+(Slater + PW92), 5 occupied + 3 extra bands per spin (LOBPCG block 8), orbitals initialised
+uniform(-1, 1) from a fixed seed, Aufbau occupations, DIIS history 6, alpha = 0.3, tol 1e-6 on
+dRho = int |rho_out - rho_in|. Synthetic input (no dataset): the geometry above.
+
+One "step" = one cold SCF solve plus the forces. Timing: W warm-up solves, then K timed solves,
+each bracketed by CUDA events on the solver's own stream, L2 flushed (256 MiB write) before each;
+a barrier + synchronize on both sides of the timed region; the max over ranks. `e2e` is the wall
+time of the user-facing calls (ks_solve + ks_forces + ks_state_density: nuclei in from host memory,
+energy, forces and both spin densities out to host memory).
+
+Forms: "plain FP32" = the LOBPCG Gram on CUDA cores, "mixed" = the Gram on the tensor cores
+(3xTF32); FP64 stays in the Rayleigh-Ritz, DIIS and every reduction finish in both.
+
+--impl reference times the reference's CPU algorithm (the f64 C++ restatement under oracle/, all
+host threads) on a bounded sample of the same workload and scales it to one SCF; rank 0 only.
+Multi-GPU: the SCF of one molecule does not shard, so N GPUs run N independent replicas
+(weak scaling, no collective); the reported time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "atomic-sandbox_b200"))
+
+N, H, SIGMA = 95, 0.25, 0.5
+NUCLEI = [(0.0, 0.0, 0.0, 8), (1.43, 1.11, 0.0, 1), (-1.43, 1.11, 0.0, 1)]
+N_UP = N_DN = 5
+N_EXTRA = 3
+METRIC = "water 95^3 SCF time-to-converge (dRho < 1e-6), B200"
+CONFIG = {"workload": "H2O cold SCF + forces, 95^3 grid, h=0.25 Bohr, sigma=0.5 Bohr, LSDA, 5 occupied + 3 extra bands/spin, "
+                      "uniform(-1,1) orbitals, Aufbau, DIIS 6, tol 1e-6",
+          "grid": N, "h_bohr": H, "sigma_bohr": SIGMA, "bands_per_spin": N_UP + N_EXTRA, "l2": "flushed (256 MiB write) before each step"}
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        cmd = ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(threads, sample_scale=1.0):
+    """The CPU baseline: the oracle (f64 C++ restatement of the reference's CPU solver) timed on a
+    bounded sample of this workload -- LOBPCG iterations (k = 5 per spin, Jacobi smoother) and
+    Jacobi-CG Poisson iterations at 95^3 -- scaled to one SCF by the work counts of a full oracle
+    SCF of the same workload (tests/golden/oracle_h2o95.json). Returns (seconds per SCF, details)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import ks_oracle as O
+    O.set_threads(threads)
+    rec_path = os.path.join(ROOT, "tests", "golden", "oracle_h2o95.json")
+    counts = None
+    if os.path.exists(rec_path):
+        with open(rec_path) as f:
+            counts = json.load(f)["stats"]
+    v = O.nuclear_potential(N, H, NUCLEI, SIGMA)
+    rho = O.deposit_charge(N, H, NUCLEI, 1.0) * (10.0 / 10.0)
+    cg_its = max(4, int(20 * sample_scale))
+    t0 = time.perf_counter()
+    O.poisson_solve(N, H, rho, tol=1e-30, max_iter=cg_its)
+    t_cg = (time.perf_counter() - t0) / cg_its
+    x0 = O.initial_orbitals(N, H, NUCLEI, 5, 1)
+    lob_its = max(1, int(2 * sample_scale))
+    t0 = time.perf_counter()
+    O.lobpcg(N, H, v, x0, tol=1e-30, max_iter=lob_its, precond_lambda=-1.0)
+    t_lob = (time.perf_counter() - t0) / (lob_its + 1)  # the final residual evaluation costs about one more iteration's H x
+    if counts:
+        eig_its, cg_total, steps = counts["eigen_iterations_total"], counts["poisson_iterations_total"], counts["iterations"]
+        source = "counts of a full oracle SCF of this workload (tests/golden/oracle_h2o95.json)"
+    else:
+        eig_its, cg_total, steps = 400, 3000, 17
+        source = "counts assumed (no full oracle record present)"
+    value = eig_its * t_lob + cg_total * t_cg
+    sample = (f"oracle f64 (C++ restatement of crates/qm), H2O 95^3: {lob_its} LOBPCG iterations (k=5) at {t_lob:.3f} s/it and "
+              f"{cg_its} Jacobi-CG iterations at {t_cg:.3f} s/it, scaled by {eig_its} LOBPCG + {cg_total} CG iterations per SCF ({source})")
+    return value, {"t_lobpcg_it_s": t_lob, "t_cg_it_s": t_cg, "sample": sample}
+
+
+def bench_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(threads, sample_scale=0.25)
+    vals = []
+    t_start = time.perf_counter()
+    last = None
+    for _ in range(args.steps):
+        v, last = cpu_sample(threads)
+        vals.append(v)
+    value = statistics.mean(vals)
+    line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (fixed geometry)", "config": CONFIG, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": last["sample"]},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t_start}
+    print(json.dumps(line), flush=True)
+
+
+def hpsi_roofline(torch, ks, peak, source):
+    """H psi on a 64-vector block of 95^3 fields (0.44 GB, 3.5x L2): CUDA events on the launching
+    stream around 20 back-to-back launches after 3 warm-ups; 12 algorithmic bytes per point and
+    vector (psi read, V read, H psi written)."""
+    count = 64
+    P = ks.field_pitch(N)
+    F = N * N * P
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev).manual_seed(7)
+    psi = torch.zeros(count, N, N, P, device=dev)
+    psi[..., :N] = torch.rand(count, N, N, N, device=dev, generator=g) - 0.5
+    v = torch.zeros(N, N, P, device=dev)
+    v[..., :N] = torch.rand(N, N, N, device=dev, generator=g)
+    out = torch.empty_like(psi)
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        ks.hpsi_device(stream.cuda_stream, N, H, count, psi.data_ptr(), v.data_ptr(), out.data_ptr())
+    reps = 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        ks.hpsi_device(stream.cuda_stream, N, H, count, psi.data_ptr(), v.data_ptr(), out.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1000.0 / reps
+    algo = 12.0 * N ** 3 * count
+    achieved = algo / t / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "stencil_hpsi_95.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            p = json.load(f)
+        if p.get("count") and p.get("dram_bytes_per_launch"):
+            traffic = p["dram_bytes_per_launch"] * count / p["count"]
+    del psi, v, out
+    return {"bound": "hbm", "kernel": "stencil_kernel (H psi, 64 x 95^3 block)", "achieved": achieved, "peak": peak,
+            "peak_source": source, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "algorithmic_bytes_per_launch": algo, "launch_ms": t * 1000.0}
+
+
+def bench_ours(args):
+    import torch
+    import ks_b200 as ks
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    peak, peak_source = measured_peaks()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    system = ks.System(NUCLEI, N_UP, N_DN)
+    settings = ks.ScfSettings(sigma=SIGMA, tol=1e-6)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def run_form(gram_mode):
+        try:
+            solver = ks.GpuSolver(N, H, gram_mode=gram_mode, n_extra=N_EXTRA, init_mode=1)
+        except ks.QmError:
+            return None
+        sstream = torch.cuda.ExternalStream(solver.stream(), device=dev)
+        try:
+            for _ in range(args.warmup):
+                solver.solve(system, settings)
+                solver.forces(NUCLEI, SIGMA)
+        except ValueError:
+            solver.close()
+            return None
+        times, walls, stats, forces = [], [], None, None
+        barrier()
+        launches0 = ks.launch_count()
+        with Clocks(uuid) as clk:
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                t0 = time.perf_counter()
+                e0.record(sstream)
+                stats = solver.solve(system, settings)
+                forces = solver.forces(NUCLEI, SIGMA)
+                e1.record(sstream)
+                rho = solver.density()
+                walls.append(time.perf_counter() - t0)
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1) / 1000.0)
+        launches = (ks.launch_count() - launches0) / max(args.steps, 1)
+        barrier()
+        prof = solver.profile()
+        solver.close()
+        return {"times": times, "walls": walls, "stats": stats, "forces": forces.tolist(), "clocks": clk.summary(), "profile": prof,
+                "rho_bytes": 2 * rho[0].size * 8, "launches": launches}
+
+    plain = run_form(0)
+    mixed = run_form(1)
+    best = mixed if mixed is not None else plain
+    t_local = statistics.mean(best["times"])
+    e2e_local = statistics.mean(best["walls"])
+    if world > 1:
+        t = torch.tensor([t_local, e2e_local], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_max, e2e_max = float(t[0]), float(t[1])
+    else:
+        t_max, e2e_max = t_local, e2e_local
+    roof = hpsi_roofline(torch, ks, peak, peak_source) if rank == 0 else None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, det = cpu_sample(os.cpu_count() or 1)
+        cpu = {"value": v, "unit": "s", "cores": os.cpu_count() or 1, "kind": "port", "sample": det["sample"]}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    oracle_e = None
+    rec_path = os.path.join(ROOT, "tests", "golden", "oracle_h2o95.json")
+    if os.path.exists(rec_path):
+        with open(rec_path) as f:
+            oracle_e = json.load(f)["stats"]["total"]
+    st = best["stats"]
+    line = {
+        "metric": METRIC, "value": t_max, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * t_max, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (fixed geometry)", "config": dict(CONFIG, parallelism=f"replicas x{world}"),
+        "forms": {"plain_fp32_s": statistics.mean(plain["times"]) if plain else None,
+                  "mixed_s": statistics.mean(mixed["times"]) if mixed else None,
+                  "mixed_speedup": (statistics.mean(plain["times"]) / statistics.mean(mixed["times"])) if (plain and mixed) else None,
+                  "reported_form": "mixed" if mixed is not None else "plain_fp32"},
+        "accuracy": {"energy_ha": st["energy"]["total"], "scf_steps": st["iterations"], "delta_rho": st["delta_rho"],
+                     "oracle_fp64_energy_ha": oracle_e, "abs_dE_vs_fp64": abs(st["energy"]["total"] - oracle_e) if oracle_e else None},
+        "profile": best["profile"],
+        "e2e": {"value": e2e_max, "unit": "s", "h2d_bytes_per_step": 32 * len(NUCLEI), "d2h_bytes_per_step": best["rho_bytes"] + 24 * len(NUCLEI)},
+        "gpu_launches": best["launches"],
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": best["clocks"],
+        "solves_per_s": world / t_max,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_ours(args)
+
+
+if __name__ == "__main__":
+    main()

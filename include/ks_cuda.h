@@ -135,6 +135,10 @@ ks_status ks_multipole_moments(int n, double h, const double* rho, double* q49);
    Fields are in the pitched layout: element (i, j, k) at (k*n + j)*P + i, P = ks_field_pitch(n),
    F = n*n*P floats per field, blocks of fields contiguous with stride F; pad columns hold 0. */
 int ks_field_pitch(int n);
+/* The cudaStream_t every kernel of this solver runs on (for callers that time or order work on it). */
+void* ks_solver_stream(void* solver);
+/* How many of this library's kernels the process has launched so far (instrumentation). */
+long long ks_launch_count(void);
 /* out_v = -1/2 lap psi_v + V psi_v, v = 0..count-1, enqueued on `stream` (a cudaStream_t, NULL = legacy). */
 ks_status ks_hpsi_device(void* stream, int n, double h, int count, const float* psi, const float* v, float* out);
 

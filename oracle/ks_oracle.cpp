@@ -790,6 +790,7 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
         int pit = poisson.solve(rho_in, v_h, ptol, PMAX, pr);
         pois_res = std::fmax(pois_res, pr);
         pois_it = std::max(pois_it, pit);
+        st->poisson_iterations_total += pit;
         lsda(N, in_up.data(), in_dn.data(), exc.data(), xu.data(), xd.data());
         for (size_t i = 0; i < N; ++i) { vu[i] = v_nuc[i] + v_h[i] + xu[i]; vd[i] = v_nuc[i] + v_h[i] + xd[i]; }
         for (int spin = 0; spin < 2; ++spin) {
@@ -803,6 +804,7 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
             int it = lobpcg(g, v.data(), orb, ev, &pc, s->eig_tol, 200, mr);
             if (it < 0) { st->status = 4; return nullptr; }
             eig_res = std::fmax(eig_res, mr);
+            st->eigen_iterations_total += it;
         }
         out_up.assign(N, 0.0);
         out_dn.assign(N, 0.0);
@@ -841,6 +843,7 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
     int pit = poisson.solve(rho, v_h, ptol, PMAX, pr);
     pois_res = std::fmax(pois_res, pr);
     pois_it = std::max(pois_it, pit);
+    st->poisson_iterations_total += pit;
     Vec t(N);
     double kinetic_e = 0.0;
     for (int spin = 0; spin < 2; ++spin)

@@ -33,6 +33,7 @@ typedef struct {
     int poisson_iterations;
     double electrons[2];
     int status;          /* 0 ok, 1 not converged, 2 stalled, 3 coincident nuclei */
+    int eigen_iterations_total, poisson_iterations_total;  /* work counters over the whole solve */
 } ora_stats;
 
 /* thread count for the parallel loops (stencils, pointwise); sums stay sequential */

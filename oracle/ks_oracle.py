@@ -31,7 +31,8 @@ class Stats(ctypes.Structure):
                 ("xc", ctypes.c_double), ("nuclear", ctypes.c_double), ("total", ctypes.c_double),
                 ("boundary_density", ctypes.c_double), ("max_eigen_residual", ctypes.c_double),
                 ("poisson_residual", ctypes.c_double), ("poisson_iterations", ctypes.c_int),
-                ("electrons", ctypes.c_double * 2), ("status", ctypes.c_int)]
+                ("electrons", ctypes.c_double * 2), ("status", ctypes.c_int),
+                ("eigen_iterations_total", ctypes.c_int), ("poisson_iterations_total", ctypes.c_int)]
 
 
 def build():

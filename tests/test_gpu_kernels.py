@@ -161,3 +161,29 @@ def test_lobpcg_oscillator_matches_oracle(ks, oracle):
     assert np.abs(np.sort(ev) - np.sort(evo)).max() < 1e-5, (ev, evo)
     gm = xs @ xs.T * h ** 3
     assert np.abs(gm / np.sqrt(np.outer(gm.diagonal(), gm.diagonal())) - np.eye(4)).max() < 1e-5
+
+
+@pytest.mark.parametrize("m,mt", [(8, 8), (24, 24), (10, 15), (60, 60)])
+def test_tensor_core_gram_matches_numpy(ks, m, mt):
+    """The 3xTF32 tcgen05 Gram (the "mixed" form): the same pairs as the CUDA-core Gram to ~1e-6
+    relative, including blocks whose row counts are not multiples of 8 and the largest block (60)."""
+    n = 33 if m < 60 else 21
+    rng = np.random.default_rng(m + mt)
+    s = f32(rng.standard_normal((m, n ** 3)))
+    t = f32(rng.standard_normal((mt, n ** 3)))
+    g = ks.gram(n, s, t, gram_mode=1)
+    want = s @ np.concatenate([s, t]).T
+    scale = np.sqrt(np.outer((s * s).sum(1), np.concatenate([(s * s).sum(1), (t * t).sum(1)])))
+    err = np.abs(g - want).max() / scale.max()
+    assert err < 2e-6, err
+
+
+def test_lobpcg_tensor_core_gram_matches_oracle(ks, oracle):
+    n, h = 33, 0.25
+    x, y, z = oracle.grid_points(n, h)
+    v = f32(0.5 * (x * x + y * y + z * z))
+    rng = np.random.default_rng(5)
+    guess = (rng.uniform(-0.5, 0.5, (4, n ** 3)) * np.exp(-(x * x + y * y + z * z) / 8.0))
+    ev, xs, it, mr = ks.lobpcg(n, h, v, guess, tol=2e-5, max_iter=400, gram_mode=1)
+    evo, _, _, _ = oracle.lobpcg(n, h, v, guess, tol=1e-8, max_iter=500, precond_lambda=1.5)
+    assert np.abs(np.sort(ev) - np.sort(evo)).max() < 1e-5, (ev, evo)

@@ -87,3 +87,15 @@ def test_not_converged_within_the_cap(ks):
     with ks.GpuSolver(33, 0.25) as so:
         with pytest.raises(ks.ScfNotConverged):
             so.solve(sys_, ks.ScfSettings(max_iter=2))
+
+
+@pytest.mark.parametrize("name", ["H2", "LiH"])
+def test_scf_mixed_precision_matches_reference_pins_33(ks, name):
+    """The mixed form (tensor-core 3xTF32 Gram) meets the same bars as plain FP32."""
+    spec = GOLDEN["pins_33"][name]
+    sys_ = _system(ks, spec)
+    with ks.GpuSolver(33, 0.25, gram_mode=1) as so:
+        st = so.solve(sys_, ks.ScfSettings(sigma=0.25, tol=1e-6))
+        f = so.forces(sys_.nuclei, 0.25)
+    assert abs(st["energy"]["total"] - spec["energy"]) < 1e-5, st
+    assert abs(f[0, 0] - spec["force_x0"]) < 1e-4, f
