@@ -30,6 +30,7 @@ constexpr int KT = 32;                       // points per stage (one 128-byte s
 constexpr int ROWS = 128;                    // MMA M: rows of [S | T] padded
 constexpr int TILE_BYTES = ROWS * KT * 4;    // 16 KB
 constexpr int THREADS = 320;
+constexpr int NBUF_MAX = 4;                  // hi*hi accumulator buffers in flight (TMEM permitting)
 constexpr long long WAIT_LIMIT = 1LL << 24;
 
 __device__ __forceinline__ unsigned su32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -81,6 +82,11 @@ __device__ __forceinline__ void mma_tf32(unsigned d_tmem, unsigned long long a, 
         "l"(a), "l"(b), "r"(idesc), "r"(acc)
         : "memory");
 }
+__device__ __forceinline__ void ld8(unsigned* r, unsigned taddr) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+}
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar)) : "memory");
 }
@@ -92,6 +98,7 @@ struct Params {
     int* err;
 };
 
+template <int NMAX>
 __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_t,
                                                              Params p, double* __restrict__ partials) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -99,12 +106,13 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
     unsigned char* base = smem_raw + ((1024 - (su32(smem_raw) & 1023)) & 1023);
     float* hi = reinterpret_cast<float*>(base);
     float* lo = reinterpret_cast<float*>(base + STAGES * TILE_BYTES);
-    __shared__ __align__(8) uint64_t full[STAGES], conv[STAGES], empty[STAGES], acc_full[2], acc_empty[2];
+    __shared__ __align__(8) uint64_t full[STAGES], conv[STAGES], empty[STAGES], acc_full[NBUF_MAX], acc_empty[NBUF_MAX];
     __shared__ unsigned tmem_base;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m8 = p.N;                 // T rows start at a 1024-byte-aligned row (m rounded up to 8)
     const int rows = m8 + p.mt;         // rows of the A tile that hold data
+    const int nbuf = min(NBUF_MAX, (512 - p.N) / (2 * p.N));  // TMEM: slot C + nbuf x (A, B)
     // this CTA's contiguous range of 32-point stages
     const int per = (p.stages_total + gridDim.x - 1) / gridDim.x;
     const int s0 = blockIdx.x * per;
@@ -117,7 +125,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
             mbar_init(&conv[i], 4);
             mbar_init(&empty[i], 1);
         }
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < NBUF_MAX; ++i) {
             mbar_init(&acc_full[i], 1);
             mbar_init(&acc_empty[i], 4);
         }
@@ -172,70 +180,86 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
             if (lane == 0) mbar_arrive(&conv[s]);
         }
     } else if (warp == 9) {
-        // ---- MMA issuer. Stage i accumulates into TMEM buffer b = i & 1 (columns 256 b ...), three
-        // slots of N columns: A = hi*hi of k-steps 0-1, B = hi*hi of k-steps 2-3, C = hi*lo + lo*hi of
-        // all four. The tensor core's f32 accumulation truncates, so no large slot takes more than one
-        // accumulating add; the epilogue drains every stage.
+        // ---- MMA issuer. TMEM columns [0, N) hold slot C, the hi*lo + lo*hi cross terms of the whole
+        // range (2^-11 of the main terms, so its own truncation is negligible); stage i writes the
+        // hi*hi products into buffer b = i % nbuf, two slots of N columns (A: k-steps 0-1, B: 2-3):
+        // the tensor core's f32 accumulation rounds toward zero, so no large slot takes more than one
+        // accumulating add, and the epilogue drains each buffer as soon as its stage is done.
         if (lane == 0) {
             const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(p.N >> 3) << 17) | ((unsigned)(ROWS >> 4) << 24);
+            const unsigned dC = tmem;
             for (int i = 0; i < nst; ++i) {
-                const int b = i & 1, s = i % STAGES;
-                if (i >= 2 && !mbar_wait(&acc_empty[b], ((i / 2) - 1) & 1, p.err)) break;
+                const int b = i % nbuf, s = i % STAGES;
+                if (i >= nbuf && !mbar_wait(&acc_empty[b], ((i / nbuf) - 1) & 1, p.err)) break;
                 if (!mbar_wait(&conv[s], (i / STAGES) & 1, p.err)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const unsigned dA = tmem + (unsigned)(b * 256), dB = dA + (unsigned)p.N, dC = dA + 2u * (unsigned)p.N;
+                const unsigned dA = tmem + (unsigned)(p.N + b * 2 * p.N), dB = dA + (unsigned)p.N;
                 const unsigned ah = su32(hi + s * (TILE_BYTES / 4)), al = su32(lo + s * (TILE_BYTES / 4));
 #pragma unroll
                 for (int kk = 0; kk < KT / 8; ++kk) {
                     const unsigned long long dh = smem_desc(ah + kk * 32), dl = smem_desc(al + kk * 32);
                     mma_tf32(kk < 2 ? dA : dB, dh, dh, idesc, (kk & 1) ? 1u : 0u);
-                    mma_tf32(dC, dh, dl, idesc, kk > 0 ? 1u : 0u);
+                    mma_tf32(dC, dh, dl, idesc, (i > 0 || kk > 0) ? 1u : 0u);
                     mma_tf32(dC, dl, dh, idesc, 1u);
                 }
                 mma_commit(&empty[s]);     // the stage's tiles are free once these MMAs have read them
-                mma_commit(&acc_full[b]);  // and its three slots are ready to drain
+                mma_commit(&acc_full[b]);  // and its two slots are ready to drain
             }
         }
     } else {
-        // ---- epilogue: warps 0..3 own TMEM lanes 32w..32w+31 (row = lane index); per stage the
-        // three slots are summed in f32 (round-to-nearest) and added to f64 totals
+        // ---- epilogue: warps 0..3 own TMEM lanes 32w..32w+31 (row = lane index); per stage the two
+        // hi*hi slots are summed in f32 (round-to-nearest) and added to f64 totals; slot C once at the end
         const int row = warp * 32 + lane;
-        double acc[64];
+        double acc[NMAX];
 #pragma unroll
-        for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+        for (int j = 0; j < NMAX; ++j) acc[j] = 0.0;
+        const unsigned lane_base = tmem + ((unsigned)(warp * 32) << 16);
+        int done = 0;
         for (int i = 0; i < nst; ++i) {
-            const int b = i & 1;
-            if (!mbar_wait(&acc_full[b], (i / 2) & 1, p.err)) break;
+            const int b = i % nbuf;
+            if (!mbar_wait(&acc_full[b], (i / nbuf) & 1, p.err)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(b * 256);
+            const unsigned ta = lane_base + (unsigned)(p.N + b * 2 * p.N), tb = ta + (unsigned)p.N;
 #pragma unroll
-            for (int j0 = 0; j0 < 64; j0 += 8) {
-                if (j0 < p.N) {
-                    unsigned ra[8], rb[8], rc[8];
-                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                                 : "=r"(ra[0]), "=r"(ra[1]), "=r"(ra[2]), "=r"(ra[3]), "=r"(ra[4]), "=r"(ra[5]), "=r"(ra[6]), "=r"(ra[7])
-                                 : "r"(taddr + (unsigned)j0));
-                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                                 : "=r"(rb[0]), "=r"(rb[1]), "=r"(rb[2]), "=r"(rb[3]), "=r"(rb[4]), "=r"(rb[5]), "=r"(rb[6]), "=r"(rb[7])
-                                 : "r"(taddr + (unsigned)(p.N + j0)));
-                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                                 : "=r"(rc[0]), "=r"(rc[1]), "=r"(rc[2]), "=r"(rc[3]), "=r"(rc[4]), "=r"(rc[5]), "=r"(rc[6]), "=r"(rc[7])
-                                 : "r"(taddr + (unsigned)(2 * p.N + j0)));
+            for (int g = 0; g < NMAX; g += 16) {
+                if (g < p.N) {
+                    unsigned ra[16], rb[16];
+                    ld8(ra, ta + g);
+                    ld8(rb, tb + g);
+                    if (g + 8 < p.N) {
+                        ld8(ra + 8, ta + g + 8);
+                        ld8(rb + 8, tb + g + 8);
+                    }
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        acc[j0 + q] += (double)((__uint_as_float(ra[q]) + __uint_as_float(rb[q])) + __uint_as_float(rc[q]));
+                    for (int q = 0; q < 16; ++q)
+                        if (g + q < p.N) acc[g + q] += (double)(__uint_as_float(ra[q]) + __uint_as_float(rb[q]));
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[b]);
+            done = i + 1;
+        }
+        if (done == nst && nst > 0) {
+#pragma unroll
+            for (int g = 0; g < NMAX; g += 8) {
+                if (g < p.N) {
+                    unsigned rc[8];
+                    ld8(rc, lane_base + g);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) acc[g + q] += (double)__uint_as_float(rc[q]);
+                }
+            }
         }
         // output row: S rows [0, m) and T rows [m8, m8 + mt) -> [0, m + mt)
         const int orow = row < p.m ? row : (row >= m8 && row < rows ? row - m8 + p.m : -1);
         if (orow >= 0) {
             double* out = partials + (size_t)blockIdx.x * (p.m + p.mt) * p.m + (size_t)orow * p.m;
-            for (int j = 0; j < p.m; ++j) out[j] = acc[j];
+#pragma unroll
+            for (int j = 0; j < NMAX; ++j)
+                if (j < p.m) out[j] = acc[j];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -288,10 +312,12 @@ void launch_gram_tc(long long F, int m, const float* S, int mt, const float* T, 
     const int smem = 2 * STAGES * TILE_BYTES + 1024;
     static bool attr = false;
     if (!attr) {
-        KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr = true;
     }
-    gram_tc_kernel<<<gram_tc_blocks(), THREADS, smem, s>>>(ms, mtm, p, partials);
+    if (p.N <= 32) gram_tc_kernel<32><<<gram_tc_blocks(), THREADS, smem, s>>>(ms, mtm, p, partials);
+    else gram_tc_kernel<64><<<gram_tc_blocks(), THREADS, smem, s>>>(ms, mtm, p, partials);
     KS_LAUNCH_CHECK();
 }
 

@@ -8,14 +8,14 @@
 // exact in real arithmetic because c_0 = -2 sum c_m, and exact per difference in f32 for smooth f.
 //
 // B200 design ("2.5-D" tiling): a CTA owns a 32 x 16 (x, y) tile of one field and marches a
-// z-chunk. Each z-plane of the tile plus its 4-point xy halo (40 x 24 floats) is staged in
-// shared memory by one TMA load (cp.async.bulk.tensor.4d); the tensor map's extent is n on
-// every axis, so the halo beyond the box arrives as the hardware's zero fill -- the Dirichlet
-// boundary costs no branches and no ghost storage. An 8-deep ring of planes keeps four planes
-// of prefetch in flight. Each thread computes two adjacent y-rows at one x and keeps the nine
-// z-values of its two columns in registers (a rolling queue), so per output it reads 8 x- and
-// 5 y-neighbours from shared memory and nothing else. Stores and the V / R reads are plain
-// coalesced 128-byte warp accesses.
+// z-chunk. Each z-plane of the tile plus its 4-point xy halo (40 x 24 floats) is staged in shared
+// memory by one TMA load (cp.async.bulk.tensor.4d); the tensor map's extent is n on every axis, so
+// the halo beyond the box arrives as the hardware's zero fill -- the Dirichlet boundary costs no
+// branches and no ghost storage. An 8-deep ring of planes keeps four planes of prefetch in flight.
+// Each of the 128 threads computes a 2 x 2 block of outputs (two x-neighbours in two adjacent
+// rows) with Blackwell's packed f32x2 arithmetic, keeps the nine z-values of its columns in a
+// register queue that the 9-way unrolled z-loop rotates by renaming (no moves), and reads 4.5
+// shared-memory words per output. Stores and the V / R reads are coalesced 8-byte accesses.
 #include <cudaTypedefs.h>
 #include "kernels.cuh"
 #include "reduce_util.cuh"
@@ -24,13 +24,15 @@ namespace ks {
 
 namespace {
 
+typedef unsigned long long u64;
+
 constexpr int BX = 32, BY = 16;
-constexpr int HXW = BX + 8, HYW = BY + 8;       // staged plane with halo: 40 x 24
-constexpr int NS = 8;                            // ring depth (planes)
-constexpr int PLANE_FLOATS = HXW * HYW;          // 960
+constexpr int HXW = BX + 8, HYW = BY + 8;          // staged plane with halo: 40 x 24
+constexpr int NS = 8;                               // ring depth (planes)
+constexpr int PLANE_FLOATS = HXW * HYW;             // 960
 constexpr unsigned PLANE_BYTES = PLANE_FLOATS * 4;  // 3840 = 30 * 128
-constexpr int THREADS = 256;                     // 32 (x) * 8 (pairs of y rows)
-constexpr long long WAIT_LIMIT = 1LL << 22;      // bounded mbarrier waits (~seconds)
+constexpr int THREADS = 128;                        // 16 x-pairs * 8 y-pairs
+constexpr long long WAIT_LIMIT = 1LL << 22;         // bounded mbarrier waits (~seconds)
 
 constexpr float C1 = 1.6f, C2 = -0.2f, C3 = 0.025396825396825397f, C4 = -0.0017857142857142857f;
 
@@ -38,7 +40,6 @@ struct Params {
     int n, P;
     long long F;
     int tiles_x, tiles_y, zc;
-    int mode;
     float scale, omega, diag_t;
     const float* V;
     const float* R;
@@ -86,119 +87,197 @@ __device__ __forceinline__ void tma_load_plane(float* dst, const CUtensorMap* ma
         : "memory");
 }
 
-// sum_m c_m * (m-th second differences over the three axes), smallest coefficients first
-__device__ __forceinline__ float lap_unscaled(const float* c, int ci, const float* q, float f0) {
-    float d[5];
+// ---- packed f32x2 arithmetic (sm_100): one instruction for both x-neighbours of a thread
+__device__ __forceinline__ u64 add2(u64 a, u64 b) { u64 d; asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
+__device__ __forceinline__ u64 sub2(u64 a, u64 b) { u64 d; asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
+__device__ __forceinline__ u64 mul2(u64 a, u64 b) { u64 d; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
+    u64 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ u64 pack(float lo, float hi) {
+    u64 d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ float lo_of(u64 v) { return __uint_as_float((unsigned)v); }
+__device__ __forceinline__ float hi_of(u64 v) { return __uint_as_float((unsigned)(v >> 32)); }
+// (hi of a, lo of b): the pair one float to the right of a
+__device__ __forceinline__ u64 straddle(u64 a, u64 b) { return pack(hi_of(a), lo_of(b)); }
+__device__ __forceinline__ u64 lds2(const float* p) { return *reinterpret_cast<const u64*>(p); }
+
+// Second differences of one row's two x-outputs at the centre plane c (ci = the thread's even x
+// in the staged plane), with the row's z-queue q (plane z+d at q[(J + 4 + d) % 9]):
+// sum_m c_m [dx_m + dy_m + dz_m], smallest coefficients first -- the scalar kernel's order.
+template <int J>
+__device__ __forceinline__ u64 lap_row(const float* c, int ci, const u64 (&q)[9]) {
+    const u64 f0 = q[(J + 4) % 9];
+    const u64 xm4 = lds2(c + ci - 4), xm2 = lds2(c + ci - 2), xp2 = lds2(c + ci + 2), xp4 = lds2(c + ci + 4);
+    const u64 xp[5] = {0, straddle(f0, xp2), xp2, straddle(xp2, xp4), xp4};
+    const u64 xm[5] = {0, straddle(xm2, f0), xm2, straddle(xm4, xm2), xm4};
+    u64 d[5];
 #pragma unroll
     for (int m = 1; m <= 4; ++m) {
-        float dx = (c[ci + m] - f0) + (c[ci - m] - f0);
-        float dy = (c[ci + m * HXW] - f0) + (c[ci - m * HXW] - f0);
-        float dz = (q[4 + m] - f0) + (q[4 - m] - f0);
-        d[m] = (dx + dy) + dz;
+        const u64 dx = add2(sub2(xp[m], f0), sub2(xm[m], f0));
+        const u64 dy = add2(sub2(lds2(c + ci + m * HXW), f0), sub2(lds2(c + ci - m * HXW), f0));
+        const u64 dz = add2(sub2(q[(J + 4 + m) % 9], f0), sub2(q[(J + 13 - m) % 9], f0));
+        d[m] = add2(add2(dx, dy), dz);
     }
-    float acc = C4 * d[4];
-    acc = fmaf(C3, d[3], acc);
-    acc = fmaf(C2, d[2], acc);
-    acc = fmaf(C1, d[1], acc);
+    u64 acc = mul2(pack(C4, C4), d[4]);
+    acc = fma2(pack(C3, C3), d[3], acc);
+    acc = fma2(pack(C2, C2), d[2], acc);
+    acc = fma2(pack(C1, C1), d[1], acc);
     return acc;
 }
 
+struct Tile {
+    int z0, nplanes, vec;
+    int gx, gy, ciA;
+    long long vbase;
+    bool okA, okB, ok2;  // rows A / B in range (and gx < n), gx + 1 < n
+};
+
+// One z-step (output plane z0 + s) with the queue rotation J = s % 9 fixed at compile time.
+template <int MODE, bool DOT, int J>
+__device__ __forceinline__ void step(const Params& p, const Tile& t, float* ring, uint64_t* bar, u64 (&qa)[9], u64 (&qb)[9], int s,
+                                     float lam, float* __restrict__ out, double& dot, const CUtensorMap* tmap, int x0, int y0) {
+    const int qn = s + 8;
+    mbar_wait(&bar[qn % NS], (unsigned)((qn / NS) & 1), p.err);
+    const float* pn = ring + (qn % NS) * PLANE_FLOATS;
+    qa[(J + 8) % 9] = lds2(pn + t.ciA);
+    qb[(J + 8) % 9] = lds2(pn + t.ciA + HXW);
+    const float* c = ring + ((s + 4) % NS) * PLANE_FLOATS;
+    const u64 sc = pack(p.scale, p.scale);
+    const u64 la = mul2(lap_row<J>(c, t.ciA, qa), sc);
+    const u64 lb = mul2(lap_row<J>(c, t.ciA + HXW, qb), sc);
+    const u64 fa = qa[(J + 4) % 9], fb = qb[(J + 4) % 9];
+    const long long rowA = ((long long)(t.z0 + s) * p.n + t.gy) * p.P + t.gx;
+    const long long rowB = rowA + p.P;
+    u64 oa = la, ob = lb;
+    if (MODE != ST_LAPLACIAN) {
+        const u64 va = t.okA ? *reinterpret_cast<const u64*>(p.V + rowA) : 0ull;
+        const u64 vb = t.okB ? *reinterpret_cast<const u64*>(p.V + rowB) : 0ull;
+        const u64 ha = fma2(va, fa, la), hb = fma2(vb, fb, lb);
+        if (MODE == ST_HAMILTONIAN) {
+            oa = ha;
+            ob = hb;
+        } else {
+            const u64 ra = t.okA ? *reinterpret_cast<const u64*>(p.R + t.vbase + rowA) : 0ull;
+            const u64 rb = t.okB ? *reinterpret_cast<const u64*>(p.R + t.vbase + rowB) : 0ull;
+            const u64 nl = pack(-lam, -lam);
+            // w + (omega / max(diag_t + V - lambda, 0.1)) (r - (H w - lambda w)), as the scalar sweep
+            const u64 ua = sub2(ra, fma2(nl, fa, ha)), ub = sub2(rb, fma2(nl, fb, hb));
+            const float ia0 = p.omega * (1.0f / fmaxf(p.diag_t + lo_of(va) - lam, 0.1f));
+            const float ia1 = p.omega * (1.0f / fmaxf(p.diag_t + hi_of(va) - lam, 0.1f));
+            const float ib0 = p.omega * (1.0f / fmaxf(p.diag_t + lo_of(vb) - lam, 0.1f));
+            const float ib1 = p.omega * (1.0f / fmaxf(p.diag_t + hi_of(vb) - lam, 0.1f));
+            oa = fma2(pack(ia0, ia1), ua, fa);
+            ob = fma2(pack(ib0, ib1), ub, fb);
+        }
+    }
+    if (t.okA) {
+        if (t.ok2) *reinterpret_cast<u64*>(out + t.vbase + rowA) = oa;
+        else out[t.vbase + rowA] = lo_of(oa);
+    }
+    if (t.okB) {
+        if (t.ok2) *reinterpret_cast<u64*>(out + t.vbase + rowB) = ob;
+        else out[t.vbase + rowB] = lo_of(ob);
+    }
+    if (DOT) {
+        if (t.okA) {
+            dot += (double)lo_of(fa) * (double)lo_of(oa);
+            if (t.ok2) dot += (double)hi_of(fa) * (double)hi_of(oa);
+        }
+        if (t.okB) {
+            dot += (double)lo_of(fb) * (double)lo_of(ob);
+            if (t.ok2) dot += (double)hi_of(fb) * (double)hi_of(ob);
+        }
+    }
+    __syncthreads();  // the centre plane's buffer is free
+    if (threadIdx.x == 0 && s + 12 < t.nplanes) {
+        const int q = s + 12, b = q % NS;
+        mbar_expect_tx(&bar[b], PLANE_BYTES);
+        tma_load_plane(ring + b * PLANE_FLOATS, tmap, x0 - 4, y0 - 4, t.z0 - 4 + q, p.vec0 + t.vec, &bar[b]);
+    }
+}
+
+template <int MODE, bool DOT>
 __global__ void __launch_bounds__(THREADS) stencil_kernel(const __grid_constant__ CUtensorMap tmap, Params p, float* __restrict__ out) {
     extern __shared__ __align__(1024) float ring[];  // NS planes of 40 x 24
     __shared__ __align__(8) uint64_t bar[NS];
 
-    const int vec = blockIdx.y;
-    int t = blockIdx.x;
-    const int tile_x = t % p.tiles_x;
-    t /= p.tiles_x;
-    const int tile_y = t % p.tiles_y;
-    const int chunk = t / p.tiles_y;
+    Tile t;
+    t.vec = blockIdx.y;
+    int b = blockIdx.x;
+    const int tile_x = b % p.tiles_x;
+    b /= p.tiles_x;
+    const int tile_y = b % p.tiles_y;
+    const int chunk = b / p.tiles_y;
     const int x0 = tile_x * BX, y0 = tile_y * BY;
-    const int z0 = chunk * p.zc;
-    const int z1 = min(z0 + p.zc, p.n);
-    const int nz = z1 - z0;
-    const int nplanes = nz + 8;  // relative plane q <-> z = z0 - 4 + q
-
-    const int lx = threadIdx.x & 31;
-    const int ly = (threadIdx.x >> 5) * 2;  // rows ly and ly + 1 of the tile
-    const int gx = x0 + lx;
-    const int gy = y0 + ly;
-    const bool okx = gx < p.n;
-    const bool okA = okx && gy < p.n;
-    const bool okB = okx && gy + 1 < p.n;
-    const int ciA = (ly + 4) * HXW + (lx + 4);
-    const int ciB = ciA + HXW;
+    t.z0 = chunk * p.zc;
+    const int nz = min(t.z0 + p.zc, p.n) - t.z0;
+    t.nplanes = nz + 8;  // relative plane q <-> z = z0 - 4 + q
+    const int lx = (threadIdx.x & 15) * 2;   // even x of the thread's pair
+    const int ly = (threadIdx.x >> 4) * 2;   // rows ly and ly + 1
+    t.gx = x0 + lx;
+    t.gy = y0 + ly;
+    const bool okx = t.gx < p.n;
+    t.ok2 = t.gx + 1 < p.n;
+    t.okA = okx && t.gy < p.n;
+    t.okB = okx && t.gy + 1 < p.n;
+    t.ciA = (ly + 4) * HXW + (lx + 4);
+    t.vbase = (long long)t.vec * p.F;
 
     if (threadIdx.x == 0) {
-        for (int b = 0; b < NS; ++b) mbar_init(&bar[b], 1);
+        for (int i = 0; i < NS; ++i) mbar_init(&bar[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     auto issue = [&](int q) {
-        const int b = q % NS;
-        mbar_expect_tx(&bar[b], PLANE_BYTES);
-        tma_load_plane(ring + b * PLANE_FLOATS, &tmap, x0 - 4, y0 - 4, z0 - 4 + q, p.vec0 + vec, &bar[b]);
+        const int bb = q % NS;
+        mbar_expect_tx(&bar[bb], PLANE_BYTES);
+        tma_load_plane(ring + bb * PLANE_FLOATS, &tmap, x0 - 4, y0 - 4, t.z0 - 4 + q, p.vec0 + t.vec, &bar[bb]);
     };
     if (threadIdx.x == 0)
         for (int q = 0; q < NS; ++q) issue(q);
 
-    float qa[9], qb[9];
+    u64 qa[9], qb[9];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         mbar_wait(&bar[q], 0, p.err);
         const float* pl = ring + q * PLANE_FLOATS;
-        qa[q] = pl[ciA];
-        qb[q] = pl[ciB];
+        qa[q] = lds2(pl + t.ciA);
+        qb[q] = lds2(pl + t.ciA + HXW);
     }
     __syncthreads();  // planes 0..3 are consumed: their buffers take planes 8..11
     if (threadIdx.x == 0)
-        for (int q = NS; q < min(NS + 4, nplanes); ++q) issue(q);
+        for (int q = NS; q < min(NS + 4, t.nplanes); ++q) issue(q);
 
-    const long long vbase = (long long)vec * p.F;
-    const float lam = (p.mode == ST_JACOBI) ? (float)p.lambda[vec] : 0.0f;
+    const float lam = (MODE == ST_JACOBI) ? (float)p.lambda[t.vec] : 0.0f;
     double dot = 0.0;
-    for (int s = 0; s < nz; ++s) {
-        const int qn = s + 8;
-        mbar_wait(&bar[qn % NS], (unsigned)((qn / NS) & 1), p.err);
-        const float* pn = ring + (qn % NS) * PLANE_FLOATS;
-        qa[8] = pn[ciA];
-        qb[8] = pn[ciB];
-        const float* c = ring + ((s + 4) % NS) * PLANE_FLOATS;
-        const int z = z0 + s;
-        const long long rowA = ((long long)z * p.n + gy) * p.P + gx;
-        const long long rowB = rowA + p.P;
-        float la = lap_unscaled(c, ciA, qa, qa[4]) * p.scale;
-        float lb = lap_unscaled(c, ciB, qb, qb[4]) * p.scale;
-        float oa = la, ob = lb;
-        if (p.mode != ST_LAPLACIAN) {
-            const float va = okA ? p.V[rowA] : 0.0f;
-            const float vb = okB ? p.V[rowB] : 0.0f;
-            const float ha = fmaf(va, qa[4], la);
-            const float hb = fmaf(vb, qb[4], lb);
-            if (p.mode == ST_HAMILTONIAN) {
-                oa = ha;
-                ob = hb;
-            } else {
-                const float ra = okA ? p.R[vbase + rowA] : 0.0f;
-                const float rb = okB ? p.R[vbase + rowB] : 0.0f;
-                const float ia = 1.0f / fmaxf(p.diag_t + va - lam, 0.1f);
-                const float ib = 1.0f / fmaxf(p.diag_t + vb - lam, 0.1f);
-                oa = qa[4] + p.omega * ia * (ra - (ha - lam * qa[4]));
-                ob = qb[4] + p.omega * ib * (rb - (hb - lam * qb[4]));
-            }
-        }
-        if (okA) out[vbase + rowA] = oa;
-        if (okB) out[vbase + rowB] = ob;
-        if (p.dot_partials) {
-            if (okA) dot += (double)qa[4] * (double)oa;
-            if (okB) dot += (double)qb[4] * (double)ob;
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) { qa[q] = qa[q + 1]; qb[q] = qb[q + 1]; }
-        __syncthreads();  // the centre plane's buffer is free
-        if (threadIdx.x == 0 && s + 12 < nplanes) issue(s + 12);
+    int s = 0;
+    for (; s + 9 <= nz; s += 9) {
+        step<MODE, DOT, 0>(p, t, ring, bar, qa, qb, s + 0, lam, out, dot, &tmap, x0, y0);
+        step<MODE, DOT, 1>(p, t, ring, bar, qa, qb, s + 1, lam, out, dot, &tmap, x0, y0);
+        step<MODE, DOT, 2>(p, t, ring, bar, qa, qb, s + 2, lam, out, dot, &tmap, x0, y0);
+        step<MODE, DOT, 3>(p, t, ring, bar, qa, qb, s + 3, lam, out, dot, &tmap, x0, y0);
+        step<MODE, DOT, 4>(p, t, ring, bar, qa, qb, s + 4, lam, out, dot, &tmap, x0, y0);
+        step<MODE, DOT, 5>(p, t, ring, bar, qa, qb, s + 5, lam, out, dot, &tmap, x0, y0);
+        step<MODE, DOT, 6>(p, t, ring, bar, qa, qb, s + 6, lam, out, dot, &tmap, x0, y0);
+        step<MODE, DOT, 7>(p, t, ring, bar, qa, qb, s + 7, lam, out, dot, &tmap, x0, y0);
+        step<MODE, DOT, 8>(p, t, ring, bar, qa, qb, s + 8, lam, out, dot, &tmap, x0, y0);
     }
-    if (p.dot_partials) {
+    // the tail: s % 9 == 0 here, so the rotation continues at J = 0
+    if (s < nz) step<MODE, DOT, 0>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
+    if (s < nz) step<MODE, DOT, 1>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
+    if (s < nz) step<MODE, DOT, 2>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
+    if (s < nz) step<MODE, DOT, 3>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
+    if (s < nz) step<MODE, DOT, 4>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
+    if (s < nz) step<MODE, DOT, 5>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
+    if (s < nz) step<MODE, DOT, 6>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
+    if (s < nz) step<MODE, DOT, 7>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
+    if (DOT) {
         double sum = block_sum(dot);
         if (threadIdx.x == 0) p.dot_partials[blockIdx.x + (size_t)gridDim.x * blockIdx.y] = sum;
     }
@@ -223,12 +302,25 @@ Shape shape_for(const Layout& L, int count) {
     sh.tiles_x = ceil_div(L.n, BX);
     sh.tiles_y = ceil_div(L.n, BY);
     const long long per_chunk = (long long)sh.tiles_x * sh.tiles_y * count;
-    const long long target = 2LL * sm_count();
+    const long long target = 4LL * sm_count();
     int chunks = (int)((target + per_chunk - 1) / per_chunk);
     chunks = std::max(1, std::min(chunks, ceil_div(L.n, 8)));
     sh.zc = ceil_div(L.n, chunks);
     sh.chunks = ceil_div(L.n, sh.zc);
     return sh;
+}
+
+template <int MODE, bool DOT>
+void launch_mode(const Shape& sh, int count, const CUtensorMap& tmap, const Params& p, float* out, cudaStream_t s) {
+    static bool attr_set = false;
+    const int smem = NS * PLANE_BYTES;
+    if (!attr_set) {
+        KS_CUDA(cudaFuncSetAttribute(stencil_kernel<MODE, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr_set = true;
+    }
+    dim3 grid(sh.tiles_x * sh.tiles_y * sh.chunks, count);
+    stencil_kernel<MODE, DOT><<<grid, THREADS, smem, s>>>(tmap, p, out);
+    KS_LAUNCH_CHECK();
 }
 
 }  // namespace
@@ -251,12 +343,6 @@ int stencil_ctas(const Layout& L, int count) {
 
 int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const StencilArgs& a, float* out, cudaStream_t s) {
     if (count <= 0) return 0;
-    static bool attr_set = false;
-    const int smem = NS * PLANE_BYTES;
-    if (!attr_set) {
-        KS_CUDA(cudaFuncSetAttribute(stencil_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr_set = true;
-    }
     Shape sh = shape_for(L, count);
     Params p;
     p.n = L.n;
@@ -265,7 +351,6 @@ int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const St
     p.tiles_x = sh.tiles_x;
     p.tiles_y = sh.tiles_y;
     p.zc = sh.zc;
-    p.mode = a.mode;
     p.scale = a.scale;
     p.omega = a.omega;
     p.diag_t = a.diag_t;
@@ -275,10 +360,22 @@ int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const St
     p.dot_partials = a.dot_partials;
     p.err = device_error_flag();
     p.vec0 = a.vec0;
-    dim3 grid(sh.tiles_x * sh.tiles_y * sh.chunks, count);
-    stencil_kernel<<<grid, THREADS, smem, s>>>(tmap, p, out);
-    KS_LAUNCH_CHECK();
-    return (int)(grid.x * grid.y);
+    const bool dot = a.dot_partials != nullptr;
+    switch (a.mode) {
+        case ST_LAPLACIAN:
+            if (dot) launch_mode<ST_LAPLACIAN, true>(sh, count, tmap, p, out, s);
+            else launch_mode<ST_LAPLACIAN, false>(sh, count, tmap, p, out, s);
+            break;
+        case ST_HAMILTONIAN:
+            if (dot) launch_mode<ST_HAMILTONIAN, true>(sh, count, tmap, p, out, s);
+            else launch_mode<ST_HAMILTONIAN, false>(sh, count, tmap, p, out, s);
+            break;
+        default:
+            if (dot) throw std::invalid_argument("stencil: dot partials are for the Laplacian and H only");
+            launch_mode<ST_JACOBI, false>(sh, count, tmap, p, out, s);
+            break;
+    }
+    return sh.tiles_x * sh.tiles_y * sh.chunks * count;
 }
 
 }  // namespace ks

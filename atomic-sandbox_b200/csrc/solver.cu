@@ -285,7 +285,9 @@ const double* Reducer::read(int count) {
     if (count > RES_CAP) throw std::invalid_argument("reducer: result overflow");
     if (count > 0) KS_CUDA(cudaMemcpyAsync(host_, res_.d(), (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, s_));
     KS_CUDA(cudaMemcpyAsync(host_flag_, device_error_flag(), sizeof(int), cudaMemcpyDeviceToHost, s_));
+    auto t0 = std::chrono::steady_clock::now();
     KS_CUDA(cudaStreamSynchronize(s_));
+    wait_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     ++readbacks;
     if (*host_flag_) {
         KS_CUDA(cudaMemsetAsync(device_error_flag(), 0, sizeof(int), s_));
@@ -672,6 +674,7 @@ EigenStats Solver::lobpcg(Channel& ch, const float* V, double tol, double guess_
             break;
         }
         ++iterations;
+        auto t_dense = clk::now();
         // 4. Rayleigh-Ritz with the conditioning guard; fallback: drop P and redo on [X, W]
         std::vector<double> th, C;
         double alpha = rayleigh_ritz(m, A, B, k, th, C);
@@ -712,6 +715,7 @@ EigenStats Solver::lobpcg(Channel& ch, const float* V, double tol, double guess_
         prev_theta = theta;
         have_prev = true;
         theta = th;
+        dense_s_ += secs(t_dense);
         upload(theta, lambda, &coef);
         const int next = ch.cur ^ 1;
         launch_block_lincomb(L_.F, m, S.at(0), 2 * k, coef_d, ch.A[next].at(0), k, k, s_);
@@ -730,6 +734,8 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
     std::memset(out, 0, sizeof(*out));
     profile = ks_profile{};
     const int rb0 = red_.readbacks;
+    const double wait0 = red_.wait_s;
+    dense_s_ = 0.0;
     if (nn < 0 || n_up < 0 || n_dn < 0 || (nn > 0 && !nuc)) { error = "invalid arguments"; return KS_INVALID; }
     if (nn > 32) { error = "at most 32 nuclei"; return KS_INVALID; }
     // E_nn (crates/qm/src/nuclear.rs:277-289)
@@ -825,6 +831,8 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 KS_CUDA(cudaStreamSynchronize(s_));
                 profile.steps = iterations;
                 profile.readbacks = red_.readbacks - rb0;
+                profile.host_dense_s = dense_s_;
+                profile.sync_wait_s = red_.wait_s - wait0;
                 profile.wall_s = secs(t0);
                 error = "abandoned before SCF step " + std::to_string(iterations + 1);
                 return KS_ABORTED;
@@ -960,12 +968,16 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         if (stalled) {
             error = "SCF stalled: best dRho " + std::to_string(best) + " not improved 2x in " + std::to_string(s.stall_window) + " iterations";
             profile.readbacks = red_.readbacks - rb0;
+            profile.host_dense_s = dense_s_;
+            profile.sync_wait_s = red_.wait_s - wait0;
             profile.wall_s = secs(t0);
             return KS_STALLED;
         }
         if (!(delta_rho < test_tol)) {
             error = "SCF did not converge after " + std::to_string(iterations) + " iterations (dRho = " + std::to_string(delta_rho) + ")";
             profile.readbacks = red_.readbacks - rb0;
+            profile.host_dense_s = dense_s_;
+            profile.sync_wait_s = red_.wait_s - wait0;
             profile.wall_s = secs(t0);
             return KS_NOT_CONVERGED;
         }
@@ -1021,6 +1033,8 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         converged_ = true;
         have_warm_ = true;
         profile.readbacks = red_.readbacks - rb0;
+        profile.host_dense_s = dense_s_;
+        profile.sync_wait_s = red_.wait_s - wait0;
         profile.wall_s = secs(t0);
         return KS_OK;
     } catch (const NumericalError& e) {

@@ -53,6 +53,7 @@ public:
     // copies res[0..count) to the host and synchronises; raises DeviceError on a failed kernel wait
     const double* read(int count);
     int readbacks = 0;
+    double wait_s = 0;  // host time blocked in read()
     int gram_mode = 0;  // 0: CUDA-core f32 Gram, 1: tensor-core 3xTF32 Gram
     double* host() const { return host_; }
     static constexpr int RES_CAP = 1 << 16;
@@ -157,6 +158,7 @@ private:
     DevBuf nuc_d_;
     bool converged_ = false;
     bool have_warm_ = false;
+    double dense_s_ = 0;  // host time in the Rayleigh-Ritz algebra (profile)
     double floor_;
 };
 

@@ -75,6 +75,8 @@ typedef struct {
 typedef struct {
     int steps, readbacks, eigen_iterations, poisson_iterations, eigen_calls, diis_resets;
     double wall_s, start_s, poisson_s, eigen_s;
+    double host_dense_s;  /* host time in the f64 Rayleigh-Ritz / DIIS algebra */
+    double sync_wait_s;   /* host time blocked on device results (readbacks) */
 } ks_profile;
 
 /* Polled before every SCF step (GpuSolver::solve_with, crates/qm-gpu/src/scf.rs:1208): nonzero abandons the solve. */
