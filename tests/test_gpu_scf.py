@@ -99,3 +99,22 @@ def test_scf_mixed_precision_matches_reference_pins_33(ks, name):
         f = so.forces(sys_.nuclei, 0.25)
     assert abs(st["energy"]["total"] - spec["energy"]) < 1e-5, st
     assert abs(f[0, 0] - spec["force_x0"]) < 1e-4, f
+
+
+H2O95 = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "oracle_h2o95.json")))
+
+
+@pytest.mark.parametrize("gram_mode", [0, 1])
+def test_h2o_95_matches_oracle_record(ks, gram_mode):
+    """The timed workload (H2O, 95^3, h = 0.25, sigma = 0.5, tol 1e-6) against a full oracle SCF of
+    it (tests/golden/oracle_h2o95.json): |dE| < 1e-5 Ha, occupied eigenvalues within 1e-5 Ha and
+    forces within 1e-4 Ha/Bohr, for the all-CUDA-core form and the tensor-core Gram form."""
+    nuc = [(0.0, 0.0, 0.0, 8), (1.43, 1.11, 0.0, 1), (-1.43, 1.11, 0.0, 1)]
+    with ks.GpuSolver(95, 0.25, gram_mode=gram_mode, n_extra=3, init_mode=1) as so:
+        st = so.solve(ks.System(nuc, 5, 5), ks.ScfSettings(sigma=0.5, tol=1e-6))
+        f = so.forces(nuc, 0.5)
+        ev_up, ev_dn = so.evals()
+    assert abs(st["energy"]["total"] - H2O95["stats"]["total"]) < 1e-5, st["energy"]
+    assert np.abs(np.sort(ev_up)[:5] - np.array(H2O95["evals_up"])).max() < 1e-5
+    assert np.abs(np.sort(ev_dn)[:5] - np.array(H2O95["evals_dn"])).max() < 1e-5
+    assert np.abs(f - np.array(H2O95["forces"])).max() < 1e-4
