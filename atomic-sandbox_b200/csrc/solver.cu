@@ -40,6 +40,14 @@ static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
+// Zeroes fresh device memory before any stream uses it. cudaMemset runs on the legacy default stream,
+// which does not order against the solver's non-blocking stream: without the wait, a kernel enqueued
+// on that stream right afterwards (ones_ = 1, a first iterate) can run first and be wiped.
+void zero_device(void* p, size_t bytes) {
+    KS_CUDA(cudaMemset(p, 0, bytes));
+    KS_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
+}
+
 int* device_error_flag() {
     static int* flags[64] = {nullptr};
     int dev = 0;
@@ -47,7 +55,7 @@ int* device_error_flag() {
     if (dev < 0 || dev >= 64) throw DeviceError("device index out of range");
     if (!flags[dev]) {
         KS_CUDA(cudaMalloc(&flags[dev], sizeof(int)));
-        KS_CUDA(cudaMemset(flags[dev], 0, sizeof(int)));
+        zero_device(flags[dev], sizeof(int));
     }
     return flags[dev];
 }
@@ -233,7 +241,7 @@ void Block::create(const Layout& L, int c) {
     count = c;
     F = L.F;
     buf.alloc((size_t)std::max(c, 1) * L.F * sizeof(float));
-    KS_CUDA(cudaMemset(buf.p, 0, buf.bytes));
+    zero_device(buf.p, buf.bytes);
     make_field_tmap(&tmap, L, buf.f(), std::max(c, 1));
 }
 
@@ -304,7 +312,7 @@ void Poisson::init(const Layout& L, cudaStream_t s, Reducer* red) {
     r_.create(L, 1); p_.create(L, 1); ap_.create(L, 1); b_.create(L, 1); z_.create(L, 1); res0_.create(L, 1); tmp0_.create(L, 1);
     ghost_.alloc(24 * (size_t)L.n * L.n * sizeof(double));
     scal_.alloc(8 * sizeof(double));
-    KS_CUDA(cudaMemset(scal_.p, 0, 8 * sizeof(double)));
+    zero_device(scal_.p, 8 * sizeof(double));
     q_.alloc(49 * sizeof(double));
     // hierarchy (crates/qm-gpu/src/multigrid.rs:105-118): odd-index coarsening down to n <= 2
     MgLevel l0{L.n, L.P, L.F, L.h, 0.f, 0.f};
@@ -329,8 +337,8 @@ void Poisson::init(const Layout& L, cudaStream_t s, Reducer* red) {
         size_t bytes = (size_t)lvdesc_[l].F * sizeof(float);
         levels_[l].lv = lvdesc_[l];
         levels_[l].x.alloc(bytes); levels_[l].b.alloc(bytes); levels_[l].res.alloc(bytes); levels_[l].tmp.alloc(bytes);
-        KS_CUDA(cudaMemset(levels_[l].x.p, 0, bytes)); KS_CUDA(cudaMemset(levels_[l].b.p, 0, bytes));
-        KS_CUDA(cudaMemset(levels_[l].res.p, 0, bytes)); KS_CUDA(cudaMemset(levels_[l].tmp.p, 0, bytes));
+        zero_device(levels_[l].x.p, bytes); zero_device(levels_[l].b.p, bytes);
+        zero_device(levels_[l].res.p, bytes); zero_device(levels_[l].tmp.p, bytes);
     }
     fused_from_ = (int)lvdesc_.size() - 1;
     for (size_t l = 0; l < lvdesc_.size(); ++l)
