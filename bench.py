@@ -165,8 +165,9 @@ def bench_reference(args):
 
 def hpsi_roofline(torch, ks, peak, source):
     """H psi on a 64-vector block of 95^3 fields (0.44 GB, 3.5x L2): CUDA events on the launching
-    stream around 20 back-to-back launches after 3 warm-ups; 12 algorithmic bytes per point and
-    vector (psi read, V read, H psi written)."""
+    stream around 20 back-to-back launches after 3 warm-ups. Algorithmic bytes per launch: psi read
+    and H psi written once per point and vector, V read once per point (it is shared by the block):
+    (8 k + 4) N^3 for k vectors."""
     count = 64
     P = ks.field_pitch(N)
     F = N * N * P
@@ -189,7 +190,7 @@ def hpsi_roofline(torch, ks, peak, source):
     e1.record(stream)
     torch.cuda.synchronize()
     t = e0.elapsed_time(e1) / 1000.0 / reps
-    algo = 12.0 * N ** 3 * count
+    algo = (8.0 * count + 4.0) * N ** 3
     achieved = algo / t / 1e9
     traffic = None
     prof = os.path.join(ROOT, "profiles", "stencil_hpsi_95.json")
