@@ -1,5 +1,6 @@
 // capi.cu -- the extern "C" boundary (include/ks_cuda.h). Every entry point catches every
 // exception and turns it into a status; nothing here traps or aborts the host process.
+#include <atomic>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -60,6 +61,27 @@ struct Scratch {
 };
 
 bool valid_grid(int n, double h) { return n >= 5 && n <= 1024 && h > 0 && std::isfinite(h); }
+
+// Scratch of ks_gram_device_noalloc: per-CTA Gram partials, 2^19 doubles (4 MiB), written in full by every
+// launch. Its address is looked up once per device (with that device current) and cached.
+constexpr size_t NOALLOC_PARTIALS = size_t(1) << 19;
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_PARTIALS];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::atomic<double*> g_noalloc_addr[NOALLOC_MAX_DEVICES];
+
+double* noalloc_partials() {
+    int dev = 0;
+    KS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) throw std::invalid_argument("ks_gram_device_noalloc: device index above 63");
+    double* p = g_noalloc_addr[dev].load(std::memory_order_acquire);
+    if (!p) {
+        void* a = nullptr;
+        KS_CUDA(cudaGetSymbolAddress(&a, g_noalloc_partials));
+        p = static_cast<double*>(a);
+        g_noalloc_addr[dev].store(p, std::memory_order_release);
+    }
+    return p;
+}
 
 }  // namespace
 
@@ -404,6 +426,24 @@ ks_status ks_hpsi_device(void* stream, int n, double h, int count, const float* 
         a.scale = (float)(-0.5 / (h * h));
         a.V = v;
         launch_stencil(L, map, count, a, out, static_cast<cudaStream_t>(stream));
+        return KS_OK;
+    });
+}
+
+ks_status ks_gram_device_noalloc(void* stream, int n, int m, const float* s, int mt, const float* t, double* out) {
+    if (n < 5 || n > 1024 || m < 1 || mt < 0 || !s || (mt > 0 && !t) || !out) return fail(nullptr, KS_INVALID, "invalid arguments");
+    return guarded(nullptr, [&] {
+        // the same grid as the solver's CUDA-core Gram (Reducer::init), hence the same partials and result
+        const int blocks = 2 * sm_count();
+        const size_t need = (size_t)blocks * m * (m + mt);
+        if (need > NOALLOC_PARTIALS)
+            throw std::invalid_argument("ks_gram_device_noalloc: 2 * SMs * m * (m + mt) = " + std::to_string(need) +
+                                        " partials exceed the static scratch of 524288 doubles (4 MiB)");
+        double* partials = noalloc_partials();
+        const Layout L = Layout::make(n, 1.0);
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        launch_gram(L.F, m, s, mt, mt > 0 ? t : s, partials, blocks, st);
+        launch_finish(partials, blocks, m * (m + mt), 1.0, out, st);
         return KS_OK;
     });
 }

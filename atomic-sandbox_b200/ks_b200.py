@@ -101,6 +101,7 @@ EXPORTED = [
     "ks_state_density", "ks_state_potentials", "ks_state_orbitals", "ks_profile_get", "ks_apply_hamiltonian",
     "ks_apply_laplacian", "ks_apply_precond", "ks_xc_lsda", "ks_nuclear_potential", "ks_poisson_solve", "ks_gram", "ks_lobpcg",
     "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
+    "ks_gram_device_noalloc",
 ]
 
 
@@ -152,6 +153,8 @@ def lib():
         L.ks_solver_stream.argtypes = [ctypes.c_void_p]
         L.ks_hpsi_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p]
+        L.ks_gram_device_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -387,6 +390,14 @@ def field_pitch(n):
 def launch_count():
     """Kernels of this library launched so far by the process."""
     return lib().ks_launch_count()
+
+
+def gram_device_noalloc(stream, n, m, s_ptr, mt, t_ptr, out_ptr):
+    """G = S^T [S | T] (CUDA-core form) on device pointers, enqueued on `stream`, allocating no device
+    memory: the partial sums live in the library's 4 MiB static scratch, so m * (m + mt) is limited to
+    2^19 / (2 * SMs) and calls on one device must not overlap (ks_gram_device_noalloc)."""
+    _check(lib().ks_gram_device_noalloc(ctypes.c_void_p(stream), int(n), int(m), ctypes.c_void_p(s_ptr), int(mt),
+                                        ctypes.c_void_p(t_ptr), ctypes.c_void_p(out_ptr)))
 
 
 def hpsi_device(stream, n, h, count, psi_ptr, v_ptr, out_ptr):

@@ -144,6 +144,21 @@ long long ks_launch_count(void);
 /* out_v = -1/2 lap psi_v + V psi_v, v = 0..count-1, enqueued on `stream` (a cudaStream_t, NULL = legacy). */
 ks_status ks_hpsi_device(void* stream, int n, double h, int count, const float* psi, const float* v, float* out);
 
+/* G = S^T [S | T] with the CUDA-core Gram (the gram_mode 0 form of ks_gram, bit-for-bit the same result) for
+   callers that must not allocate device memory: a host framework whose caching allocator owns the GPU's memory
+   (a stray cudaMalloc can fail for lack of memory or fragment its pool), and latency-critical stream pipelines
+   (cudaFree synchronises the whole device). No counterpart in the reference: its Gram always runs inside a
+   solver that owns its buffers.
+   s: m fields, t: mt fields (NULL when mt = 0), pitched layout on the current device; out: m x (m + mt) doubles on
+   the device, row-major. Enqueued on `stream` (a cudaStream_t, NULL = legacy); nothing is read back.
+   Allocates nothing: the per-CTA partial sums live in a 4 MiB static device array (2^19 doubles) that every
+   launch overwrites in full, so nothing needs to start at zero. Limit: 2 * SMs * m * (m + mt) <= 2^19, i.e.
+   m * (m + mt) <= 1771 on a 148-SM B200; larger blocks return KS_INVALID with a message and launch nothing.
+   The first call on each device looks the array up (cudaGetSymbolAddress, with that device current); make that
+   first call before any stream capture begins. Calls on one device share the array: calls that overlap in time
+   (other streams, other host threads) race, so order them on one stream. */
+ks_status ks_gram_device_noalloc(void* stream, int n, int m, const float* s, int mt, const float* t, double* out);
+
 #ifdef __cplusplus
 }
 #endif
