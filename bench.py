@@ -163,12 +163,11 @@ def bench_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def hpsi_roofline(torch, ks, peak, source):
+def hpsi_roofline(torch, ks, peak, source, count=64):
     """H psi on a 64-vector block of 95^3 fields (0.44 GB, 3.5x L2): CUDA events on the launching
     stream around 20 back-to-back launches after 3 warm-ups. Algorithmic bytes per launch: psi read
     and H psi written once per point and vector, V read once per point (it is shared by the block):
     (8 k + 4) N^3 for k vectors."""
-    count = 64
     P = ks.field_pitch(N)
     F = N * N * P
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -193,14 +192,16 @@ def hpsi_roofline(torch, ks, peak, source):
     algo = (8.0 * count + 4.0) * N ** 3
     achieved = algo / t / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "stencil_hpsi_95.json")
+    prof = os.path.join(ROOT, "profiles", "stencil_hpsi_95.md")
     if os.path.exists(prof):
+        import re
         with open(prof) as f:
-            p = json.load(f)
-        if p.get("count") and p.get("dram_bytes_per_launch"):
-            traffic = p["dram_bytes_per_launch"] * count / p["count"]
+            text = f.read()
+        mb, mc = re.search(r"dram_bytes_per_launch: (\d+)", text), re.search(r"count: (\d+)", text)
+        if mb and mc:
+            traffic = int(mb.group(1)) * count / int(mc.group(1))
     del psi, v, out
-    return {"bound": "hbm", "kernel": "stencil_kernel (H psi, 64 x 95^3 block)", "achieved": achieved, "peak": peak,
+    return {"bound": "hbm", "kernel": f"stencil_kernel (H psi, {count} x 95^3 block)", "achieved": achieved, "peak": peak,
             "peak_source": source, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
             "algorithmic_bytes_per_launch": algo, "launch_ms": t * 1000.0}
 
@@ -268,8 +269,8 @@ def bench_ours(args):
         return {"times": times, "walls": walls, "stats": stats, "forces": forces.tolist(), "clocks": clk.summary(), "profile": prof,
                 "rho_bytes": 2 * rho[0].size * 8, "launches": launches}
 
-    plain = run_form(0)
-    mixed = run_form(1)
+    plain = run_form(0) if args.form in ("both", "plain") else None
+    mixed = run_form(1) if args.form in ("both", "mixed") else None
     best = mixed if mixed is not None else plain
     t_local = statistics.mean(best["times"])
     e2e_local = statistics.mean(best["walls"])
@@ -316,6 +317,26 @@ def bench_ours(args):
     print(json.dumps(line), flush=True)
 
 
+def kernel_only(args):
+    """One hot kernel in isolation, for profiling: --kernel hpsi (H psi on a --count block of 95^3
+    fields, timed as in the roofline) or --kernel gram (the LOBPCG Gram G = S^T [S | T] at 95^3 with
+    m = mt = 24, through ks_gram; --form plain runs the CUDA-core form)."""
+    import torch
+    import ks_b200 as ks
+    peak, source = measured_peaks()
+    if args.kernel == "hpsi":
+        print(json.dumps(hpsi_roofline(torch, ks, peak, source, count=args.count)), flush=True)
+        return
+    import numpy as np
+    rng = np.random.default_rng(5)
+    s = rng.standard_normal((24, N ** 3))
+    t = rng.standard_normal((24, N ** 3))
+    gm = 0 if args.form == "plain" else 1
+    for _ in range(4):
+        g = ks.gram(N, s, t, gram_mode=gm)
+    print(json.dumps({"kernel": "gram", "gram_mode": gm, "n": N, "m": 24, "mt": 24, "g00": float(g[0, 0])}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -323,8 +344,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--form", default="both", choices=["both", "plain", "mixed"], help="which SCF forms to time")
+    ap.add_argument("--kernel", choices=["hpsi", "gram"], help="time one hot kernel only (profiling)")
+    ap.add_argument("--count", type=int, default=64, help="vectors per H psi launch with --kernel hpsi")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernel:
+        kernel_only(args)
+    elif args.impl == "reference":
         bench_reference(args)
     else:
         bench_ours(args)
