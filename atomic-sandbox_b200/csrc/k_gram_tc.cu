@@ -7,17 +7,28 @@
 // Precision ("3xTF32"): every f32 input x is split in shared memory into hi = x with the low 13
 // mantissa bits cleared (exactly a TF32 value) and lo = x - hi (exact in f32); each K-step issues
 // hi*hi + hi*lo + lo*hi on kind::tf32, so products carry ~22 significant bits (the dropped lo*lo
-// term is ~2^-22 relative). The tensor core's f32 accumulation rounds toward zero, so the hi*hi sums
-// are kept in two slots per stage (at most one accumulating add each) and the stage is drained to
-// f64 in registers; the small cross terms share a third slot.
+// term is ~2^-22 relative). The tensor core's f32 accumulation rounds toward zero, so a stage's
+// hi*hi sum (4 K-steps) gets its own TMEM slot and is drained right after the stage into f32 sums
+// (round-to-nearest) that move into f64 every FLUSH stages; the small cross terms share one slot
+// for the whole range.
 //
-// Per CTA (10 warps): warp 8 lane 0 is the TMA producer (one 128B-swizzled box of the S rows and
-// one of the T rows per 32-point stage, 4-stage ring); warps 4..7 split each stage into hi/lo; warp
-// 9 lane 0 issues the tcgen05.mma chain into one of two TMEM buffers (128 lanes x 3 slots of N
-// columns, N = m rounded up to 8) and commits to mbarriers; warps 0..3 (TMEM lane quadrants 0..3)
-// drain a finished buffer with tcgen05.ld into f64 sums, one row per thread. The B operand is
-// the A tile itself (its first N rows), so S is loaded once. The T rows start at row N = m rounded
-// up to 8, so every TMA destination is 1024-byte aligned. Every wait is bounded.
+// Per CTA (14 warps): warp 12 lane 0 is the TMA producer (one 128B-swizzled box of the S rows and
+// one of the T rows per 32-point stage); warps 8..11 split each stage into hi/lo in place; warp 13
+// lane 0 issues the tcgen05.mma chain into TMEM slots of N columns (N = m rounded up to 8) and
+// commits to mbarriers; warps 0..7 drain finished slots with tcgen05.ld (warp w: TMEM lane quadrant
+// w % 4, column half w / 4), one row per thread. The B operand is the A tile itself (its first N
+// rows), so S is loaded once. The T rows start at row N, so every TMA destination is 1024-byte
+// aligned.
+//
+// The ring is what sets the speed: a stage's round trip (TMA, split, MMA, commit) takes a few
+// microseconds, so ~16 stages must be in flight per SM to stream at HBM rate. The tiles are
+// therefore compact -- a stage holds only the rows with data (round8(N + mt) rows of 128 B, 6 KB
+// at m = mt = 24) -- although the M = 128 MMA reads 128 rows: the rows past the data are whatever
+// follows in shared memory (the next stages' tiles, or a zeroed tail), and they only produce rows
+// of D the epilogue never reads (each row of D depends on its own row of A). Per-stage scalar work
+// is kept small (running ring indices, descriptors advanced by addition): one issuing thread and
+// the drains, not the tensor core, bound the stage rate. Every wait is bounded.
+#include <algorithm>
 #include <cudaTypedefs.h>
 #include "kernels.cuh"
 
@@ -25,12 +36,13 @@ namespace ks {
 
 namespace {
 
-constexpr int STAGES = 4;
+constexpr int RMAX = 16;                     // ring depth cap
 constexpr int KT = 32;                       // points per stage (one 128-byte swizzle row)
 constexpr int ROWS = 128;                    // MMA M: rows of [S | T] padded
 constexpr int TILE_BYTES = ROWS * KT * 4;    // 16 KB
-constexpr int THREADS = 320;
-constexpr int NBUF_MAX = 4;                  // hi*hi accumulator buffers in flight (TMEM permitting)
+constexpr int THREADS = 448;                 // 8 epilogue, 4 split, 1 TMA, 1 MMA warps
+constexpr int FLUSH = 8;                     // stages summed in f32 before an f64 add
+constexpr int NBUF_MAX = 8;                  // hi*hi accumulator buffers in flight (TMEM permitting)
 constexpr long long WAIT_LIMIT = 1LL << 24;
 
 __device__ __forceinline__ unsigned su32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -95,6 +107,8 @@ struct Params {
     long long F;  // points per field (multiple of 4)
     int m, mt, N;
     int stages_total;
+    int R;        // ring depth
+    int tbytes;   // bytes per compact tile: round8(N + mt) rows of 128 B (a multiple of 1024)
     int* err;
 };
 
@@ -102,17 +116,19 @@ template <int NMAX>
 __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_t,
                                                              Params p, double* __restrict__ partials) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // 1024-aligned tile ring: hi tiles then lo tiles
+    // 1024-aligned compact rings: R hi tiles, R lo tiles, then a zero tail so that an M = 128 read
+    // from the last lo tile stays inside the allocation
     unsigned char* base = smem_raw + ((1024 - (su32(smem_raw) & 1023)) & 1023);
-    float* hi = reinterpret_cast<float*>(base);
-    float* lo = reinterpret_cast<float*>(base + STAGES * TILE_BYTES);
-    __shared__ __align__(8) uint64_t full[STAGES], conv[STAGES], empty[STAGES], acc_full[NBUF_MAX], acc_empty[NBUF_MAX];
+    const int R = p.R;
+    unsigned char* hi = base;
+    unsigned char* lo = base + (size_t)R * p.tbytes;
+    __shared__ __align__(8) uint64_t full[RMAX], conv[RMAX], empty[RMAX], acc_full[NBUF_MAX], acc_empty[NBUF_MAX];
     __shared__ unsigned tmem_base;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m8 = p.N;                 // T rows start at a 1024-byte-aligned row (m rounded up to 8)
     const int rows = m8 + p.mt;         // rows of the A tile that hold data
-    const int nbuf = min(NBUF_MAX, (512 - p.N) / (2 * p.N));  // TMEM: slot C + nbuf x (A, B)
+    const int nbuf = min(NBUF_MAX, (512 - p.N) / p.N);  // TMEM: slot C + nbuf hi*hi slots
     // this CTA's contiguous range of 32-point stages
     const int per = (p.stages_total + gridDim.x - 1) / gridDim.x;
     const int s0 = blockIdx.x * per;
@@ -120,20 +136,20 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
     const int nst = max(0, s1 - s0);
 
     if (threadIdx.x == 0) {
-        for (int i = 0; i < STAGES; ++i) {
+        for (int i = 0; i < R; ++i) {
             mbar_init(&full[i], 1);
             mbar_init(&conv[i], 4);
             mbar_init(&empty[i], 1);
         }
         for (int i = 0; i < NBUF_MAX; ++i) {
             mbar_init(&acc_full[i], 1);
-            mbar_init(&acc_empty[i], 4);
+            mbar_init(&acc_empty[i], 8);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // rows >= mc of every hi/lo tile stay zero (the MMA reads all 128 rows)
-    for (int i = threadIdx.x; i < 2 * STAGES * TILE_BYTES / 16; i += blockDim.x)
-        reinterpret_cast<float4*>(base)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    // zero the rings and the tail once (the pad rows between S and T are never loaded)
+    const int clear16 = (2 * R * p.tbytes + (TILE_BYTES - p.tbytes)) / 16;
+    for (int i = threadIdx.x; i < clear16; i += blockDim.x) reinterpret_cast<float4*>(base)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(su32(&tmem_base)) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
@@ -144,122 +160,146 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const unsigned tmem = tmem_base;
 
-    if (warp == 8) {
+    if (warp == 12) {
         // ---- TMA producer
         if (lane == 0) {
             const unsigned bytes = (unsigned)((p.m + p.mt) * KT * 4);
+            int s = 0;
+            unsigned ph = 0;
             for (int i = 0; i < nst; ++i) {
-                const int s = i % STAGES;
-                if (i >= STAGES && !mbar_wait(&empty[s], ((i / STAGES) - 1) & 1, p.err)) break;
+                if (i >= R && !mbar_wait(&empty[s], ph ^ 1u, p.err)) break;
                 mbar_expect_tx(&full[s], bytes);
                 const int x = (s0 + i) * KT;
-                tma_2d(hi + s * (TILE_BYTES / 4), &tm_s, x, 0, &full[s]);
-                tma_2d(hi + s * (TILE_BYTES / 4) + m8 * KT, &tm_t, x, 0, &full[s]);
+                unsigned char* dst = hi + (size_t)s * p.tbytes;
+                tma_2d(dst, &tm_s, x, 0, &full[s]);
+                tma_2d(dst + m8 * KT * 4, &tm_t, x, 0, &full[s]);
+                if (++s == R) { s = 0; ph ^= 1u; }
             }
         }
-    } else if (warp >= 4 && warp < 8) {
-        // ---- hi/lo split of rows [0, rows) of each stage
-        const int t = threadIdx.x - 128;
-        const int n4 = rows * KT / 4;
+    } else if (warp >= 8 && warp < 12) {
+        // ---- hi/lo split of rows [0, rows) of each stage, in place (hi) and into the lo ring
+        const int t = threadIdx.x - 256;
+        const int n4 = rows * KT / 4;  // <= 1024: at most 8 float4 per thread
+        int s = 0;
+        unsigned ph = 0;
         for (int i = 0; i < nst; ++i) {
-            const int s = i % STAGES;
-            if (!mbar_wait(&full[s], (i / STAGES) & 1, p.err)) break;
-            float4* h4 = reinterpret_cast<float4*>(hi + s * (TILE_BYTES / 4));
-            float4* l4 = reinterpret_cast<float4*>(lo + s * (TILE_BYTES / 4));
-            for (int e = t; e < n4; e += 128) {
-                float4 x = h4[e], a, b;
-                a.x = __uint_as_float(__float_as_uint(x.x) & 0xFFFFE000u); b.x = x.x - a.x;
-                a.y = __uint_as_float(__float_as_uint(x.y) & 0xFFFFE000u); b.y = x.y - a.y;
-                a.z = __uint_as_float(__float_as_uint(x.z) & 0xFFFFE000u); b.z = x.z - a.z;
-                a.w = __uint_as_float(__float_as_uint(x.w) & 0xFFFFE000u); b.w = x.w - a.w;
-                h4[e] = a;
-                l4[e] = b;
+            if (!mbar_wait(&full[s], ph, p.err)) break;
+            float4* h4 = reinterpret_cast<float4*>(hi + (size_t)s * p.tbytes);
+            float4* l4 = reinterpret_cast<float4*>(lo + (size_t)s * p.tbytes);
+            float4 x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (t + 128 * u < n4) x[u] = h4[t + 128 * u];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (t + 128 * u < n4) {
+                    float4 a, b;
+                    a.x = __uint_as_float(__float_as_uint(x[u].x) & 0xFFFFE000u); b.x = x[u].x - a.x;
+                    a.y = __uint_as_float(__float_as_uint(x[u].y) & 0xFFFFE000u); b.y = x[u].y - a.y;
+                    a.z = __uint_as_float(__float_as_uint(x[u].z) & 0xFFFFE000u); b.z = x[u].z - a.z;
+                    a.w = __uint_as_float(__float_as_uint(x[u].w) & 0xFFFFE000u); b.w = x[u].w - a.w;
+                    h4[t + 128 * u] = a;
+                    l4[t + 128 * u] = b;
+                }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&conv[s]);
+            if (++s == R) { s = 0; ph ^= 1u; }
         }
-    } else if (warp == 9) {
+    } else if (warp == 13) {
         // ---- MMA issuer. TMEM columns [0, N) hold slot C, the hi*lo + lo*hi cross terms of the whole
-        // range (2^-11 of the main terms, so its own truncation is negligible); stage i writes the
-        // hi*hi products into buffer b = i % nbuf, two slots of N columns (A: k-steps 0-1, B: 2-3):
-        // the tensor core's f32 accumulation rounds toward zero, so no large slot takes more than one
-        // accumulating add, and the epilogue drains each buffer as soon as its stage is done.
+        // range (2^-11 of the main terms, so its own truncation is negligible); stage i writes its
+        // hi*hi products (4 K-steps, 3 accumulating adds) into buffer b = i % nbuf, N columns, which
+        // the epilogue drains as soon as the stage is done: the tensor core's f32 accumulation rounds
+        // toward zero, so no hi*hi sum runs longer than one stage. Descriptors advance by the tile
+        // size (ring) and 32 B per K-step (the address field counts 16-byte units).
         if (lane == 0) {
             const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(p.N >> 3) << 17) | ((unsigned)(ROWS >> 4) << 24);
             const unsigned dC = tmem;
+            const unsigned long long dh0 = smem_desc(su32(hi)), dl0 = smem_desc(su32(lo));
+            const unsigned long long step = (unsigned long long)(p.tbytes >> 4);
+            int s = 0, b = 0;
+            unsigned ph = 0, bph = 0;
             for (int i = 0; i < nst; ++i) {
-                const int b = i % nbuf, s = i % STAGES;
-                if (i >= nbuf && !mbar_wait(&acc_empty[b], ((i / nbuf) - 1) & 1, p.err)) break;
-                if (!mbar_wait(&conv[s], (i / STAGES) & 1, p.err)) break;
+                if (i >= nbuf && !mbar_wait(&acc_empty[b], bph ^ 1u, p.err)) break;
+                if (!mbar_wait(&conv[s], ph, p.err)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const unsigned dA = tmem + (unsigned)(p.N + b * 2 * p.N), dB = dA + (unsigned)p.N;
-                const unsigned ah = su32(hi + s * (TILE_BYTES / 4)), al = su32(lo + s * (TILE_BYTES / 4));
+                const unsigned d = tmem + (unsigned)(p.N + b * p.N);
+                const unsigned long long h0 = dh0 + (unsigned long long)s * step, l0 = dl0 + (unsigned long long)s * step;
+                mma_tf32(d, h0, h0, idesc, 0u);
+                mma_tf32(dC, h0, l0, idesc, i > 0 ? 1u : 0u);
+                mma_tf32(dC, l0, h0, idesc, 1u);
 #pragma unroll
-                for (int kk = 0; kk < KT / 8; ++kk) {
-                    const unsigned long long dh = smem_desc(ah + kk * 32), dl = smem_desc(al + kk * 32);
-                    mma_tf32(kk < 2 ? dA : dB, dh, dh, idesc, (kk & 1) ? 1u : 0u);
-                    mma_tf32(dC, dh, dl, idesc, (i > 0 || kk > 0) ? 1u : 0u);
-                    mma_tf32(dC, dl, dh, idesc, 1u);
+                for (int kk = 1; kk < KT / 8; ++kk) {
+                    const unsigned long long hk = h0 + 2 * kk, lk = l0 + 2 * kk;
+                    mma_tf32(d, hk, hk, idesc, 1u);
+                    mma_tf32(dC, hk, lk, idesc, 1u);
+                    mma_tf32(dC, lk, hk, idesc, 1u);
                 }
                 mma_commit(&empty[s]);     // the stage's tiles are free once these MMAs have read them
-                mma_commit(&acc_full[b]);  // and its two slots are ready to drain
+                mma_commit(&acc_full[b]);  // and its hi*hi slot is ready to drain
+                if (++s == R) { s = 0; ph ^= 1u; }
+                if (++b == nbuf) { b = 0; bph ^= 1u; }
             }
         }
     } else {
-        // ---- epilogue: warps 0..3 own TMEM lanes 32w..32w+31 (row = lane index); per stage the two
-        // hi*hi slots are summed in f32 (round-to-nearest) and added to f64 totals; slot C once at the end
-        const int row = warp * 32 + lane;
-        double acc[NMAX];
+        // ---- epilogue: warps 0..7; warp w reads TMEM lanes 32(w%4)..+31 (row = lane index) and the
+        // column half w/4. Each stage's hi*hi slot is added to f32 sums (round-to-nearest), which go
+        // into f64 totals every FLUSH stages; slot C is added once at the end.
+        constexpr int HALF = NMAX / 2;
+        const int quad = warp & 3, c0 = (warp >> 2) * HALF;
+        const int row = quad * 32 + lane;
+        const int ncols = max(0, min(HALF, p.N - c0));  // multiple of 8
+        float fs[HALF];
+        double acc[HALF];
 #pragma unroll
-        for (int j = 0; j < NMAX; ++j) acc[j] = 0.0;
-        const unsigned lane_base = tmem + ((unsigned)(warp * 32) << 16);
-        int done = 0;
+        for (int j = 0; j < HALF; ++j) { fs[j] = 0.f; acc[j] = 0.0; }
+        const unsigned lane_base = tmem + ((unsigned)(quad * 32) << 16) + (unsigned)c0;
+        int done = 0, b = 0, since = 0;
+        unsigned bph = 0;
         for (int i = 0; i < nst; ++i) {
-            const int b = i % nbuf;
-            if (!mbar_wait(&acc_full[b], (i / nbuf) & 1, p.err)) break;
+            if (!mbar_wait(&acc_full[b], bph, p.err)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const unsigned ta = lane_base + (unsigned)(p.N + b * 2 * p.N), tb = ta + (unsigned)p.N;
+            const unsigned ta = lane_base + (unsigned)(p.N + b * p.N);
+            unsigned r[HALF];
 #pragma unroll
-            for (int g = 0; g < NMAX; g += 16) {
-                if (g < p.N) {
-                    unsigned ra[16], rb[16];
-                    ld8(ra, ta + g);
-                    ld8(rb, tb + g);
-                    if (g + 8 < p.N) {
-                        ld8(ra + 8, ta + g + 8);
-                        ld8(rb + 8, tb + g + 8);
-                    }
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                    for (int q = 0; q < 16; ++q)
-                        if (g + q < p.N) acc[g + q] += (double)(__uint_as_float(ra[q]) + __uint_as_float(rb[q]));
-                }
-            }
+            for (int g = 0; g < HALF; g += 8)
+                if (g < ncols) ld8(r + g, ta + g);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[b]);
+#pragma unroll
+            for (int j = 0; j < HALF; ++j)
+                if (j < ncols) fs[j] += __uint_as_float(r[j]);
+            if (++since == FLUSH) {
+#pragma unroll
+                for (int j = 0; j < HALF; ++j) { acc[j] += (double)fs[j]; fs[j] = 0.f; }
+                since = 0;
+            }
+            if (++b == nbuf) { b = 0; bph ^= 1u; }
             done = i + 1;
         }
-        if (done == nst && nst > 0) {
 #pragma unroll
-            for (int g = 0; g < NMAX; g += 8) {
-                if (g < p.N) {
-                    unsigned rc[8];
-                    ld8(rc, lane_base + g);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        for (int j = 0; j < HALF; ++j) acc[j] += (double)fs[j];
+        if (done == nst && nst > 0 && ncols > 0) {
+            unsigned rc[HALF];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) acc[g + q] += (double)__uint_as_float(rc[q]);
-                }
-            }
+            for (int g = 0; g < HALF; g += 8)
+                if (g < ncols) ld8(rc + g, lane_base + g);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < HALF; ++j)
+                if (j < ncols) acc[j] += (double)__uint_as_float(rc[j]);
         }
         // output row: S rows [0, m) and T rows [m8, m8 + mt) -> [0, m + mt)
         const int orow = row < p.m ? row : (row >= m8 && row < rows ? row - m8 + p.m : -1);
         if (orow >= 0) {
             double* out = partials + (size_t)blockIdx.x * (p.m + p.mt) * p.m + (size_t)orow * p.m;
 #pragma unroll
-            for (int j = 0; j < NMAX; ++j)
-                if (j < p.m) out[j] = acc[j];
+            for (int j = 0; j < HALF; ++j)
+                if (c0 + j < p.m) out[c0 + j] = acc[j];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -308,12 +348,19 @@ void launch_gram_tc(long long F, int m, const float* S, int mt, const float* T, 
     p.mt = mt;
     p.N = (m + 7) & ~7;
     p.stages_total = (int)((F + KT - 1) / KT);
+    p.tbytes = (p.N + ((mt + 7) & ~7)) * KT * 4;
+    // dynamic shared memory: two compact rings, the zero tail, 1 KB of alignment slack; the static
+    // barriers take the last KB of the 227 KB a CTA may use
+    constexpr int SMEM_BUDGET = 227 * 1024 - 1024;
+    const int fixed = (TILE_BYTES - p.tbytes) + 1024;
+    p.R = std::min(RMAX, (SMEM_BUDGET - fixed) / (2 * p.tbytes));
+    if (p.R < 2) throw std::invalid_argument("gram_tc: tile ring does not fit");
     p.err = device_error_flag();
-    const int smem = 2 * STAGES * TILE_BYTES + 1024;
+    const int smem = fixed + 2 * p.R * p.tbytes;
     static bool attr = false;
     if (!attr) {
-        KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BUDGET));
+        KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BUDGET));
         attr = true;
     }
     if (p.N <= 32) gram_tc_kernel<32><<<gram_tc_blocks(), THREADS, smem, s>>>(ms, mtm, p, partials);

@@ -16,6 +16,7 @@
 // rows) with Blackwell's packed f32x2 arithmetic, keeps the nine z-values of its columns in a
 // register queue that the 9-way unrolled z-loop rotates by renaming (no moves), and reads 4.5
 // shared-memory words per output. Stores and the V / R reads are coalesced 8-byte accesses.
+#include <algorithm>
 #include <cudaTypedefs.h>
 #include "kernels.cuh"
 #include "reduce_util.cuh"
@@ -203,7 +204,7 @@ __device__ __forceinline__ void step(const Params& p, const Tile& t, float* ring
 }
 
 template <int MODE, bool DOT>
-__global__ void __launch_bounds__(THREADS) stencil_kernel(const __grid_constant__ CUtensorMap tmap, Params p, float* __restrict__ out) {
+__global__ void __launch_bounds__(THREADS, 4) stencil_kernel(const __grid_constant__ CUtensorMap tmap, Params p, float* __restrict__ out) {
     extern __shared__ __align__(1024) float ring[];  // NS planes of 40 x 24
     __shared__ __align__(8) uint64_t bar[NS];
 
@@ -297,16 +298,29 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 struct Shape { int tiles_x, tiles_y, chunks, zc; };
 
+// The grid: (x, y) tiles x vectors x z-chunks. A CTA's time is about (its planes + prologue) steps
+// whatever else runs (the kernel is latency-bound at 4 CTAs per SM), and the launch takes
+// ceil(CTAs / resident slots) such rounds, so the chunk count minimises waves x (zc + 8 halo planes
+// + ~4 prologue steps). At 95^3 this gives 4 chunks of 24 planes for 8 vectors (576 CTAs, one
+// wave) instead of a wave and a fifth, and one chunk for 64 vectors.
 Shape shape_for(const Layout& L, int count) {
     Shape sh;
     sh.tiles_x = ceil_div(L.n, BX);
     sh.tiles_y = ceil_div(L.n, BY);
     const long long per_chunk = (long long)sh.tiles_x * sh.tiles_y * count;
-    const long long target = 4LL * sm_count();
-    int chunks = (int)((target + per_chunk - 1) / per_chunk);
-    chunks = std::max(1, std::min(chunks, ceil_div(L.n, 8)));
-    sh.zc = ceil_div(L.n, chunks);
-    sh.chunks = ceil_div(L.n, sh.zc);
+    const long long slots = 4LL * sm_count();
+    long long best = -1;
+    for (int c = 1; c <= std::max(1, L.n / 8); ++c) {
+        const int zc = ceil_div(L.n, c);
+        const int cc = ceil_div(L.n, zc);
+        const long long waves = (cc * per_chunk + slots - 1) / slots;
+        const long long cost = waves * (zc + 12);
+        if (best < 0 || cost < best) {
+            best = cost;
+            sh.zc = zc;
+            sh.chunks = cc;
+        }
+    }
     return sh;
 }
 
