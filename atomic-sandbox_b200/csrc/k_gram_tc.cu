@@ -40,7 +40,7 @@ constexpr int RMAX = 16;                     // ring depth cap
 constexpr int KT = 32;                       // points per stage (one 128-byte swizzle row)
 constexpr int ROWS = 128;                    // MMA M: rows of [S | T] padded
 constexpr int TILE_BYTES = ROWS * KT * 4;    // 16 KB
-constexpr int THREADS = 448;                 // 8 epilogue, 4 split, 1 TMA, 1 MMA warps
+constexpr int THREADS = 480;                 // 8 epilogue, 4 split, 1 TMA, 2 MMA warps
 constexpr int FLUSH = 8;                     // stages summed in f32 before an f64 add
 constexpr int NBUF_MAX = 8;                  // hi*hi accumulator buffers in flight (TMEM permitting)
 constexpr long long WAIT_LIMIT = 1LL << 24;
@@ -105,10 +105,15 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 
 struct Params {
     long long F;  // points per field (multiple of 4)
-    int m, mt, N;
+    int m, mt;
+    int P;        // 32-point slabs per stage (2 when m and mt fit 32-row blocks, else 1)
+    int SB;       // row stride of the S blocks of a stage's slabs
+    int TR0, TB;  // first T row, row stride of the T blocks
+    int N;        // MMA N: rows of the tile used as the B operand
+    int rows;     // rows the split converts
     int stages_total;
     int R;        // ring depth
-    int tbytes;   // bytes per compact tile: round8(N + mt) rows of 128 B (a multiple of 1024)
+    int tbytes;   // bytes per tile (a multiple of 1024)
     int* err;
 };
 
@@ -116,20 +121,18 @@ template <int NMAX>
 __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_constant__ CUtensorMap tm_s, const __grid_constant__ CUtensorMap tm_t,
                                                              Params p, double* __restrict__ partials) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // 1024-aligned compact rings: R hi tiles, R lo tiles, then a zero tail so that an M = 128 read
-    // from the last lo tile stays inside the allocation
+    // 1024-aligned rings: R hi tiles, R lo tiles, then a zero tail so that an M = 128 read from the
+    // last lo tile stays inside the allocation
     unsigned char* base = smem_raw + ((1024 - (su32(smem_raw) & 1023)) & 1023);
     const int R = p.R;
     unsigned char* hi = base;
     unsigned char* lo = base + (size_t)R * p.tbytes;
-    __shared__ __align__(8) uint64_t full[RMAX], conv[RMAX], empty[RMAX], acc_full[NBUF_MAX], acc_empty[NBUF_MAX];
+    __shared__ __align__(8) uint64_t full[RMAX], conv[RMAX], empty[RMAX], acc_full[NBUF_MAX], acc_empty[NBUF_MAX], cdone;
     __shared__ unsigned tmem_base;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m8 = p.N;                 // T rows start at a 1024-byte-aligned row (m rounded up to 8)
-    const int rows = m8 + p.mt;         // rows of the A tile that hold data
-    const int nbuf = min(NBUF_MAX, (512 - p.N) / p.N);  // TMEM: slot C + nbuf hi*hi slots
-    // this CTA's contiguous range of 32-point stages
+    const int nbuf = min(NBUF_MAX, (512 - p.N) / p.N);  // TMEM: slot C + nbuf hi*hi slots of N columns
+    // this CTA's contiguous range of stages (P slabs of 32 points each)
     const int per = (p.stages_total + gridDim.x - 1) / gridDim.x;
     const int s0 = blockIdx.x * per;
     const int s1 = min(p.stages_total, s0 + per);
@@ -139,15 +142,16 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
         for (int i = 0; i < R; ++i) {
             mbar_init(&full[i], 1);
             mbar_init(&conv[i], 4);
-            mbar_init(&empty[i], 1);
+            mbar_init(&empty[i], 2);  // both MMA issuers release a tile
         }
         for (int i = 0; i < NBUF_MAX; ++i) {
             mbar_init(&acc_full[i], 1);
             mbar_init(&acc_empty[i], 8);
         }
+        mbar_init(&cdone, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // zero the rings and the tail once (the pad rows between S and T are never loaded)
+    // zero the rings and the tail once (rows that are never loaded stay zero)
     const int clear16 = (2 * R * p.tbytes + (TILE_BYTES - p.tbytes)) / 16;
     for (int i = threadIdx.x; i < clear16; i += blockDim.x) reinterpret_cast<float4*>(base)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (warp == 0) {
@@ -161,25 +165,27 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
     const unsigned tmem = tmem_base;
 
     if (warp == 12) {
-        // ---- TMA producer
+        // ---- TMA producer: slab q of a stage puts its S rows at row q*SB, its T rows at TR0 + q*TB
         if (lane == 0) {
-            const unsigned bytes = (unsigned)((p.m + p.mt) * KT * 4);
+            const unsigned bytes = (unsigned)(p.P * (p.m + p.mt) * KT * 4);
             int s = 0;
             unsigned ph = 0;
             for (int i = 0; i < nst; ++i) {
                 if (i >= R && !mbar_wait(&empty[s], ph ^ 1u, p.err)) break;
                 mbar_expect_tx(&full[s], bytes);
-                const int x = (s0 + i) * KT;
                 unsigned char* dst = hi + (size_t)s * p.tbytes;
-                tma_2d(dst, &tm_s, x, 0, &full[s]);
-                tma_2d(dst + m8 * KT * 4, &tm_t, x, 0, &full[s]);
+                for (int q = 0; q < p.P; ++q) {
+                    const int x = ((s0 + i) * p.P + q) * KT;
+                    tma_2d(dst + q * p.SB * KT * 4, &tm_s, x, 0, &full[s]);
+                    tma_2d(dst + (p.TR0 + q * p.TB) * KT * 4, &tm_t, x, 0, &full[s]);
+                }
                 if (++s == R) { s = 0; ph ^= 1u; }
             }
         }
     } else if (warp >= 8 && warp < 12) {
         // ---- hi/lo split of rows [0, rows) of each stage, in place (hi) and into the lo ring
         const int t = threadIdx.x - 256;
-        const int n4 = rows * KT / 4;  // <= 1024: at most 8 float4 per thread
+        const int n4 = p.rows * KT / 4;  // <= 1024: at most 8 float4 per thread
         int s = 0;
         unsigned ph = 0;
         for (int i = 0; i < nst; ++i) {
@@ -207,55 +213,81 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
             if (lane == 0) mbar_arrive(&conv[s]);
             if (++s == R) { s = 0; ph ^= 1u; }
         }
-    } else if (warp == 13) {
-        // ---- MMA issuer. TMEM columns [0, N) hold slot C, the hi*lo + lo*hi cross terms of the whole
-        // range (2^-11 of the main terms, so its own truncation is negligible); stage i writes its
-        // hi*hi products (4 K-steps, 3 accumulating adds) into buffer b = i % nbuf, N columns, which
-        // the epilogue drains as soon as the stage is done: the tensor core's f32 accumulation rounds
-        // toward zero, so no hi*hi sum runs longer than one stage. Descriptors advance by the tile
-        // size (ring) and 32 B per K-step (the address field counts 16-byte units).
+    } else if (warp == 13 || warp == 14) {
+        // ---- MMA issuers (one thread each, so their issue latencies overlap). Warp 13 puts a stage's
+        // hi*hi products (4 K-steps, 3 accumulating adds) into buffer b = i % nbuf of N columns,
+        // which the epilogue drains as soon as the stage is done: the tensor core's f32 accumulation
+        // rounds toward zero, so no hi*hi sum runs longer than one stage. Warp 14 accumulates the
+        // hi*lo + lo*hi cross terms of the whole range in slot C (columns [0, N); 2^-11 of the main
+        // terms, so its own truncation is negligible). Descriptors advance by the tile size (ring)
+        // and 32 B per K-step (the address field counts 16-byte units).
         if (lane == 0) {
             const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(p.N >> 3) << 17) | ((unsigned)(ROWS >> 4) << 24);
-            const unsigned dC = tmem;
             const unsigned long long dh0 = smem_desc(su32(hi)), dl0 = smem_desc(su32(lo));
             const unsigned long long step = (unsigned long long)(p.tbytes >> 4);
             int s = 0, b = 0;
             unsigned ph = 0, bph = 0;
-            for (int i = 0; i < nst; ++i) {
-                if (i >= nbuf && !mbar_wait(&acc_empty[b], bph ^ 1u, p.err)) break;
-                if (!mbar_wait(&conv[s], ph, p.err)) break;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const unsigned d = tmem + (unsigned)(p.N + b * p.N);
-                const unsigned long long h0 = dh0 + (unsigned long long)s * step, l0 = dl0 + (unsigned long long)s * step;
-                mma_tf32(d, h0, h0, idesc, 0u);
-                mma_tf32(dC, h0, l0, idesc, i > 0 ? 1u : 0u);
-                mma_tf32(dC, l0, h0, idesc, 1u);
+            if (warp == 13) {
+                for (int i = 0; i < nst; ++i) {
+                    if (i >= nbuf && !mbar_wait(&acc_empty[b], bph ^ 1u, p.err)) break;
+                    if (!mbar_wait(&conv[s], ph, p.err)) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const unsigned d = tmem + (unsigned)(p.N + b * p.N);
+                    const unsigned long long h0 = dh0 + (unsigned long long)s * step;
+                    mma_tf32(d, h0, h0, idesc, 0u);
 #pragma unroll
-                for (int kk = 1; kk < KT / 8; ++kk) {
-                    const unsigned long long hk = h0 + 2 * kk, lk = l0 + 2 * kk;
-                    mma_tf32(d, hk, hk, idesc, 1u);
-                    mma_tf32(dC, hk, lk, idesc, 1u);
-                    mma_tf32(dC, lk, hk, idesc, 1u);
+                    for (int kk = 1; kk < KT / 8; ++kk) mma_tf32(d, h0 + 2 * kk, h0 + 2 * kk, idesc, 1u);
+                    mma_commit(&empty[s]);     // this issuer is done with the stage's tiles
+                    mma_commit(&acc_full[b]);  // and the hi*hi slot is ready to drain
+                    if (++s == R) { s = 0; ph ^= 1u; }
+                    if (++b == nbuf) { b = 0; bph ^= 1u; }
                 }
-                mma_commit(&empty[s]);     // the stage's tiles are free once these MMAs have read them
-                mma_commit(&acc_full[b]);  // and its hi*hi slot is ready to drain
-                if (++s == R) { s = 0; ph ^= 1u; }
-                if (++b == nbuf) { b = 0; bph ^= 1u; }
+            } else {
+                const unsigned dC = tmem;
+                int i = 0;
+                for (; i < nst; ++i) {
+                    if (!mbar_wait(&conv[s], ph, p.err)) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const unsigned long long h0 = dh0 + (unsigned long long)s * step, l0 = dl0 + (unsigned long long)s * step;
+                    mma_tf32(dC, h0, l0, idesc, i > 0 ? 1u : 0u);
+                    mma_tf32(dC, l0, h0, idesc, 1u);
+#pragma unroll
+                    for (int kk = 1; kk < KT / 8; ++kk) {
+                        mma_tf32(dC, h0 + 2 * kk, l0 + 2 * kk, idesc, 1u);
+                        mma_tf32(dC, l0 + 2 * kk, h0 + 2 * kk, idesc, 1u);
+                    }
+                    mma_commit(&empty[s]);
+                    if (++s == R) { s = 0; ph ^= 1u; }
+                }
+                if (i == nst) mma_commit(&cdone);  // slot C is final once these MMAs complete
             }
         }
     } else {
         // ---- epilogue: warps 0..7; warp w reads TMEM lanes 32(w%4)..+31 (row = lane index) and the
-        // column half w/4. Each stage's hi*hi slot is added to f32 sums (round-to-nearest), which go
-        // into f64 totals every FLUSH stages; slot C is added once at the end.
+        // column half w/4 of its rows' own N-column block. Each stage's hi*hi slot is added to f32
+        // sums (round-to-nearest), which go into f64 totals every FLUSH stages; slot C is added once
+        // at the end. With two slabs per stage, lane quadrants 0..3 hold S of slab 0, S of slab 1,
+        // T of slab 0, T of slab 1, and slab q's columns start at 32q.
         constexpr int HALF = NMAX / 2;
         const int quad = warp & 3, c0 = (warp >> 2) * HALF;
-        const int row = quad * 32 + lane;
-        const int ncols = max(0, min(HALF, p.N - c0));  // multiple of 8
+        const int mc = (p.m + 7) & ~7;  // columns of D that hold data
+        int orow, colbase, slab;
+        if (p.P == 2) {
+            slab = quad & 1;
+            colbase = 32 * slab;
+            orow = (quad < 2) ? (lane < p.m ? lane : -1) : (lane < p.mt ? p.m + lane : -1);
+        } else {
+            const int r = quad * 32 + lane;
+            slab = 0;
+            colbase = 0;
+            orow = r < p.m ? r : (r >= p.TR0 && r < p.TR0 + p.mt ? r - p.TR0 + p.m : -1);
+        }
+        const int ncols = max(0, min(HALF, mc - c0));  // multiple of 8, the same for the whole warp
         float fs[HALF];
         double acc[HALF];
 #pragma unroll
         for (int j = 0; j < HALF; ++j) { fs[j] = 0.f; acc[j] = 0.0; }
-        const unsigned lane_base = tmem + ((unsigned)(quad * 32) << 16) + (unsigned)c0;
+        const unsigned lane_base = tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(colbase + c0);
         int done = 0, b = 0, since = 0;
         unsigned bph = 0;
         for (int i = 0; i < nst; ++i) {
@@ -283,7 +315,8 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
         }
 #pragma unroll
         for (int j = 0; j < HALF; ++j) acc[j] += (double)fs[j];
-        if (done == nst && nst > 0 && ncols > 0) {
+        if (done == nst && nst > 0 && ncols > 0 && mbar_wait(&cdone, 0u, p.err)) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             unsigned rc[HALF];
 #pragma unroll
             for (int g = 0; g < HALF; g += 8)
@@ -293,10 +326,8 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
             for (int j = 0; j < HALF; ++j)
                 if (j < ncols) acc[j] += (double)__uint_as_float(rc[j]);
         }
-        // output row: S rows [0, m) and T rows [m8, m8 + mt) -> [0, m + mt)
-        const int orow = row < p.m ? row : (row >= m8 && row < rows ? row - m8 + p.m : -1);
         if (orow >= 0) {
-            double* out = partials + (size_t)blockIdx.x * (p.m + p.mt) * p.m + (size_t)orow * p.m;
+            double* out = partials + ((size_t)blockIdx.x * p.P + slab) * (p.m + p.mt) * p.m + (size_t)orow * p.m;
 #pragma unroll
             for (int j = 0; j < HALF; ++j)
                 if (c0 + j < p.m) out[c0 + j] = acc[j];
@@ -333,9 +364,15 @@ void make_rows_map(CUtensorMap* map, const float* base, long long F, int rows) {
 
 }  // namespace
 
-int gram_tc_blocks() { return sm_count(); }
+// Two 32-point slabs per stage when S and T fit 32-row blocks (m, mt <= 32): the 128-row A tile holds
+// S(slab 0), S(slab 1), T(slab 0), T(slab 1) at rows 0, 32, 64, 96, and B is its first 64 rows, so one
+// MMA serves both slabs (the cross-slab blocks of D are never read) and each slab writes its own
+// partials. Otherwise one slab per stage: S at row 0, T at row round8(m).
+static int slabs_for(int m, int mt) { return (((m + 7) & ~7) <= 32 && ((mt + 7) & ~7) <= 32) ? 2 : 1; }
 
-// partials: [gram_tc_blocks()][(m + mt) x m] of D = [S | T]^T S
+int gram_tc_blocks(int m, int mt) { return sm_count() * slabs_for(m, mt); }
+
+// partials: [gram_tc_blocks(m, mt)][(m + mt) x m] of D = [S | T]^T S
 void launch_gram_tc(long long F, int m, const float* S, int mt, const float* T, double* partials, cudaStream_t s) {
     if (m < 1 || mt < 1 || ((m + 7) & ~7) + mt > ROWS || m > 64) throw std::invalid_argument("gram_tc: need m <= 64 and round8(m) + mt <= 128");
     if (F % 4 != 0) throw std::invalid_argument("gram_tc: F must be a multiple of 4");
@@ -346,11 +383,19 @@ void launch_gram_tc(long long F, int m, const float* S, int mt, const float* T, 
     p.F = F;
     p.m = m;
     p.mt = mt;
-    p.N = (m + 7) & ~7;
-    p.stages_total = (int)((F + KT - 1) / KT);
-    p.tbytes = (p.N + ((mt + 7) & ~7)) * KT * 4;
-    // dynamic shared memory: two compact rings, the zero tail, 1 KB of alignment slack; the static
-    // barriers take the last KB of the 227 KB a CTA may use
+    p.P = slabs_for(m, mt);
+    const int m8 = (m + 7) & ~7, mt8 = (mt + 7) & ~7;
+    if (p.P == 2) {
+        p.SB = 32; p.TR0 = 64; p.TB = 32; p.N = 64; p.rows = 96 + mt8;
+        p.tbytes = TILE_BYTES;
+    } else {
+        p.SB = 0; p.TR0 = m8; p.TB = 0; p.N = m8; p.rows = m8 + mt8;
+        p.tbytes = p.rows * KT * 4;
+    }
+    const long long slab_pts = (long long)KT * p.P;
+    p.stages_total = (int)((F + slab_pts - 1) / slab_pts);
+    // dynamic shared memory: two rings, the zero tail, 1 KB of alignment slack; the static barriers
+    // take the last KB of the 227 KB a CTA may use
     constexpr int SMEM_BUDGET = 227 * 1024 - 1024;
     const int fixed = (TILE_BYTES - p.tbytes) + 1024;
     p.R = std::min(RMAX, (SMEM_BUDGET - fixed) / (2 * p.tbytes));
@@ -363,8 +408,8 @@ void launch_gram_tc(long long F, int m, const float* S, int mt, const float* T, 
         KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BUDGET));
         attr = true;
     }
-    if (p.N <= 32) gram_tc_kernel<32><<<gram_tc_blocks(), THREADS, smem, s>>>(ms, mtm, p, partials);
-    else gram_tc_kernel<64><<<gram_tc_blocks(), THREADS, smem, s>>>(ms, mtm, p, partials);
+    if (m8 <= 32) gram_tc_kernel<32><<<sm_count(), THREADS, smem, s>>>(ms, mtm, p, partials);
+    else gram_tc_kernel<64><<<sm_count(), THREADS, smem, s>>>(ms, mtm, p, partials);
     KS_LAUNCH_CHECK();
 }
 

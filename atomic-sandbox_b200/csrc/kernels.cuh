@@ -82,9 +82,9 @@ int stencil_ctas(const Layout& L, int count);
 void launch_finish(const double* partials, int blocks, int nvals, double scale, double* out, cudaStream_t s);
 // the same for a rows x cols matrix of values, written transposed (out[c*rows + r])
 void launch_finish_transposed(const double* partials, int blocks, int rows, int cols, double scale, double* out, cudaStream_t s);
-// G = S^T [S | T] on the tensor cores (k_gram_tc.cu): partials [gram_tc_blocks()][(m + mt) x m] of the
+// G = S^T [S | T] on the tensor cores (k_gram_tc.cu): partials [gram_tc_blocks(m, mt)][(m + mt) x m] of the
 // transpose D = [S | T]^T S; m <= 64, round8(m) + mt <= 128.
-int gram_tc_blocks();
+int gram_tc_blocks(int m, int mt);
 void launch_gram_tc(long long F, int m, const float* S, int mt, const float* T, double* partials, cudaStream_t s);
 int reduce_blocks(long long F);
 // out-of-place dot products: partials [blocks][npairs] of sum a_p*b_p over F floats.

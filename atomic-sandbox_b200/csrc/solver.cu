@@ -276,7 +276,7 @@ void Reducer::gram(int m, const float* S, int mt, const float* T, int off, doubl
     if (gram_mode == 1) {
         // tensor cores: partials of D = [S | T]^T S, finished transposed into G = S^T [S | T]
         if (m > 64 || ((m + 7) & ~7) + mt > 128) throw std::invalid_argument("tensor-core Gram: block too large (m <= 64, round8(m) + mt <= 128)");
-        const int blocks = gram_tc_blocks();
+        const int blocks = gram_tc_blocks(m, mt);
         const size_t need = (size_t)blocks * m * (m + mt);
         if (need * sizeof(double) > partials_.bytes) partials_.alloc(need * sizeof(double));
         launch_gram_tc(L_.F, m, S, mt, T, partials_.d(), s_);
