@@ -388,8 +388,8 @@ ks_status ks_lobpcg(int n, double h, const double* v, int k, double* x, double* 
         vv.create(L, 1);
         sc.upload_fields(v, 1, vv);
         sc.upload_fields(x, k, ch.A[0]);
-        EigenStats es = so.lobpcg(ch, vv.at(0), tol, tol, max_iter, k);
-        KS_CUDA(cudaStreamSynchronize(so.stream()));
+        EigenStats es = so.lobpcg(ch, so.lane(0), vv.at(0), tol, tol, max_iter, k);
+        KS_CUDA(cudaStreamSynchronize(so.lane(0).s));
         sc.download_fields(ch.X(), k, x);
         for (int i = 0; i < k; ++i) evals[i] = ch.evals[i];
         if (max_residual) *max_residual = es.max_residual;

@@ -4,21 +4,23 @@
 // crates/qm-gpu/src/reduce.rs:340-420 computes the same pairs with CUDA-core f32 partials). The
 // reduction dimension K is the grid itself (~10^6 points), split across one persistent CTA per SM.
 //
-// Precision ("3xTF32"): every f32 input x is split in shared memory into hi = x with the low 13
-// mantissa bits cleared (exactly a TF32 value) and lo = x - hi (exact in f32); each K-step issues
-// hi*hi + hi*lo + lo*hi on kind::tf32, so products carry ~22 significant bits (the dropped lo*lo
-// term is ~2^-22 relative). The tensor core's f32 accumulation rounds toward zero, so a stage's
+// Precision ("3xTF32"): every f32 input x is split into hi = x with the low 13 mantissa bits
+// cleared (exactly a TF32 value) and lo = x - hi (exact in f32); each K-step issues hi*hi + hi*lo +
+// lo*hi on kind::tf32, so products carry ~22 significant bits (the dropped lo*lo term is ~2^-22
+// relative). kind::tf32 reads only the top 19 bits of each 32-bit operand, so the loaded tile
+// itself serves as hi (the test suite checks the result against f64); only lo is written, into a
+// second tile. The tensor core's f32 accumulation rounds toward zero, so a stage's
 // hi*hi sum (4 K-steps) gets its own TMEM slot and is drained right after the stage into f32 sums
 // (round-to-nearest) that move into f64 every FLUSH stages; the small cross terms share one slot
 // for the whole range.
 //
-// Per CTA (14 warps): warp 12 lane 0 is the TMA producer (one 128B-swizzled box of the S rows and
-// one of the T rows per 32-point stage); warps 8..11 split each stage into hi/lo in place; warp 13
-// lane 0 issues the tcgen05.mma chain into TMEM slots of N columns (N = m rounded up to 8) and
-// commits to mbarriers; warps 0..7 drain finished slots with tcgen05.ld (warp w: TMEM lane quadrant
-// w % 4, column half w / 4), one row per thread. The B operand is the A tile itself (its first N
-// rows), so S is loaded once. The T rows start at row N, so every TMA destination is 1024-byte
-// aligned.
+// Per CTA (15 warps): warp 12 lane 0 is the TMA producer (one 128B-swizzled box of the S rows and
+// one of the T rows per 32-point slab); warps 8..11 form lo;
+// warp 13 lane 0 issues the hi*hi MMAs and warp 14 lane 0 the cross-term MMAs (the issue latency of
+// one thread, not the tensor core, is the limit), each committing to mbarriers; warps 0..7 drain
+// finished slots with tcgen05.ld (warp w: TMEM lane quadrant w % 4, column half w / 4), one row per
+// thread. The B operand is the A tile itself (its first N rows), so S is loaded once; every TMA
+// destination row is a multiple of 8, so 1024-byte aligned.
 //
 // The ring is what sets the speed: a stage's round trip (TMA, split, MMA, commit) takes a few
 // microseconds, so ~16 stages must be in flight per SM to stream at HBM rate. The tiles are
@@ -183,14 +185,14 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
             }
         }
     } else if (warp >= 8 && warp < 12) {
-        // ---- hi/lo split of rows [0, rows) of each stage, in place (hi) and into the lo ring
+        // ---- lo = x - hi of rows [0, rows) of each stage into the lo ring (the loaded tile is hi)
         const int t = threadIdx.x - 256;
         const int n4 = p.rows * KT / 4;  // <= 1024: at most 8 float4 per thread
         int s = 0;
         unsigned ph = 0;
         for (int i = 0; i < nst; ++i) {
             if (!mbar_wait(&full[s], ph, p.err)) break;
-            float4* h4 = reinterpret_cast<float4*>(hi + (size_t)s * p.tbytes);
+            const float4* h4 = reinterpret_cast<const float4*>(hi + (size_t)s * p.tbytes);
             float4* l4 = reinterpret_cast<float4*>(lo + (size_t)s * p.tbytes);
             float4 x[8];
 #pragma unroll
@@ -199,12 +201,11 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 if (t + 128 * u < n4) {
-                    float4 a, b;
-                    a.x = __uint_as_float(__float_as_uint(x[u].x) & 0xFFFFE000u); b.x = x[u].x - a.x;
-                    a.y = __uint_as_float(__float_as_uint(x[u].y) & 0xFFFFE000u); b.y = x[u].y - a.y;
-                    a.z = __uint_as_float(__float_as_uint(x[u].z) & 0xFFFFE000u); b.z = x[u].z - a.z;
-                    a.w = __uint_as_float(__float_as_uint(x[u].w) & 0xFFFFE000u); b.w = x[u].w - a.w;
-                    h4[t + 128 * u] = a;
+                    float4 b;
+                    b.x = x[u].x - __uint_as_float(__float_as_uint(x[u].x) & 0xFFFFE000u);
+                    b.y = x[u].y - __uint_as_float(__float_as_uint(x[u].y) & 0xFFFFE000u);
+                    b.z = x[u].z - __uint_as_float(__float_as_uint(x[u].z) & 0xFFFFE000u);
+                    b.w = x[u].w - __uint_as_float(__float_as_uint(x[u].w) & 0xFFFFE000u);
                     l4[t + 128 * u] = b;
                 }
             }
@@ -340,14 +341,14 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
+    // resolved once (thread-safe static initialisation)
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         cudaDriverEntryPointQueryResult q;
         void* ptr = nullptr;
         KS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q));
         if (q != cudaDriverEntryPointSuccess || !ptr) throw DeviceError("cuTensorMapEncodeTiled is not available");
-        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
-    }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    }();
     return fn;
 }
 
@@ -402,12 +403,12 @@ void launch_gram_tc(long long F, int m, const float* S, int mt, const float* T, 
     if (p.R < 2) throw std::invalid_argument("gram_tc: tile ring does not fit");
     p.err = device_error_flag();
     const int smem = fixed + 2 * p.R * p.tbytes;
-    static bool attr = false;
-    if (!attr) {
+    static const bool attr = [] {
         KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BUDGET));
         KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BUDGET));
-        attr = true;
-    }
+        return true;
+    }();
+    (void)attr;
     if (m8 <= 32) gram_tc_kernel<32><<<sm_count(), THREADS, smem, s>>>(ms, mtm, p, partials);
     else gram_tc_kernel<64><<<sm_count(), THREADS, smem, s>>>(ms, mtm, p, partials);
     KS_LAUNCH_CHECK();

@@ -285,14 +285,14 @@ __global__ void __launch_bounds__(THREADS, 4) stencil_kernel(const __grid_consta
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
+    // resolved once (thread-safe static initialisation)
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         cudaDriverEntryPointQueryResult q;
         void* ptr = nullptr;
         KS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q));
         if (q != cudaDriverEntryPointSuccess || !ptr) throw DeviceError("cuTensorMapEncodeTiled is not available");
-        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
-    }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    }();
     return fn;
 }
 
@@ -326,12 +326,12 @@ Shape shape_for(const Layout& L, int count) {
 
 template <int MODE, bool DOT>
 void launch_mode(const Shape& sh, int count, const CUtensorMap& tmap, const Params& p, float* out, cudaStream_t s) {
-    static bool attr_set = false;
     const int smem = NS * PLANE_BYTES;
-    if (!attr_set) {
+    static const bool attr_set = [smem] {
         KS_CUDA(cudaFuncSetAttribute(stencil_kernel<MODE, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr_set = true;
-    }
+        return true;
+    }();
+    (void)attr_set;
     dim3 grid(sh.tiles_x * sh.tiles_y * sh.chunks, count);
     stencil_kernel<MODE, DOT><<<grid, THREADS, smem, s>>>(tmap, p, out);
     KS_LAUNCH_CHECK();

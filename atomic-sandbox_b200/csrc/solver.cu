@@ -13,6 +13,9 @@
 // What changes on the B200: every reduction is finished on the device, the CG scalars never
 // leave it, the preconditioner/H-products/Ritz updates run as block kernels over all vectors of a
 // channel at once, and the SCF's charge renormalisation is a device-side scale.
+#include <exception>
+#include <mutex>
+#include <thread>
 #include "solver.h"
 #include <algorithm>
 #include <atomic>
@@ -25,15 +28,17 @@
 namespace ks {
 
 // ------------------------------------------------------------------ process-wide device facts
+// Both caches are shared by the host threads of concurrent spin channels, hence the lock.
+static std::mutex g_device_facts;
+
 int sm_count() {
-    static int dev_cached = -1, count = 0;
+    static int counts[64] = {0};
     int dev = 0;
     KS_CUDA(cudaGetDevice(&dev));
-    if (dev != dev_cached) {
-        KS_CUDA(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev));
-        dev_cached = dev;
-    }
-    return count;
+    if (dev < 0 || dev >= 64) throw DeviceError("device index out of range");
+    std::lock_guard<std::mutex> lock(g_device_facts);
+    if (!counts[dev]) KS_CUDA(cudaDeviceGetAttribute(&counts[dev], cudaDevAttrMultiProcessorCount, dev));
+    return counts[dev];
 }
 
 static std::atomic<long long> g_launches{0};
@@ -53,6 +58,7 @@ int* device_error_flag() {
     int dev = 0;
     KS_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw DeviceError("device index out of range");
+    std::lock_guard<std::mutex> lock(g_device_facts);
     if (!flags[dev]) {
         KS_CUDA(cudaMalloc(&flags[dev], sizeof(int)));
         zero_device(flags[dev], sizeof(int));
@@ -104,17 +110,6 @@ double secs(clk::time_point a) { return std::chrono::duration<double>(clk::now()
 
 // pinned host staging for coefficient uploads (one per process; every upload is followed by a
 // synchronising readback before the buffer is rewritten)
-double* upload_buffer(size_t doubles) {
-    static double* buf = nullptr;
-    static size_t cap = 0;
-    if (doubles > cap) {
-        if (buf) cudaFreeHost(buf);
-        KS_CUDA(cudaMallocHost(&buf, doubles * sizeof(double)));
-        cap = doubles;
-    }
-    return buf;
-}
-
 // Columns of a Gram matrix within rel^(1/2) of the span of the earlier ones
 // (crates/qm-gpu/src/eigen.rs:491-509).
 std::vector<int> dependent_columns(int m, const std::vector<double>& b, double rel) {
@@ -255,6 +250,31 @@ void Reducer::init(const Layout& L, cudaStream_t s, size_t partial_doubles) {
     res_.alloc(RES_CAP * sizeof(double));
     KS_CUDA(cudaMallocHost(&host_, RES_CAP * sizeof(double)));
     KS_CUDA(cudaMallocHost(&host_flag_, sizeof(int)));
+}
+
+void Lane::init(const Layout& L) {
+    KS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    KS_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    red.init(L, s, 1 << 20);
+}
+
+double* Lane::upload_buffer(size_t doubles) {
+    if (doubles > up_cap) {
+        if (up) cudaFreeHost(up);
+        up = nullptr;
+        KS_CUDA(cudaMallocHost(&up, doubles * sizeof(double)));
+        up_cap = doubles;
+    }
+    return up;
+}
+
+Lane::~Lane() {
+    if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+    if (up) cudaFreeHost(up);
+    if (ev_join) cudaEventDestroy(ev_join);
 }
 
 Reducer::~Reducer() {
@@ -495,7 +515,13 @@ void Channel::create(const Layout& L, int kk) {
 Solver::Solver(int n, double h, const SolverOptions& o) : L_(Layout::make(n, h)), opt_(o) {
     if (n < 5 || !(h > 0)) throw std::invalid_argument("grid: n >= 5 and h > 0 required");
     KS_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    KS_CUDA(cudaGetDevice(&dev_));
+    KS_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
     red_.init(L_, s_, 1 << 20);
+    for (auto& l : lane_) {
+        l.reset(new Lane());
+        l->init(L_);
+    }
     poisson_.init(L_, s_, &red_);
     for (Block* b : {&vnuc_, &vh_, &in_up_, &in_dn_, &out_up_, &out_dn_, &rho_tot_, &v_up_, &v_dn_, &exc_, &ones_}) b->create(L_, 1);
     launch_fill(ones_.at(0), 1.0f, L_.F, s_);
@@ -508,6 +534,7 @@ Solver::~Solver() {
         cudaStreamSynchronize(s_);
         cudaStreamDestroy(s_);
     }
+    if (ev_fork_) cudaEventDestroy(ev_fork_);
 }
 
 void Solver::ensure_channel(int spin, int k) {
@@ -517,15 +544,15 @@ void Solver::ensure_channel(int spin, int k) {
     }
 }
 
-void Solver::gram_checked(int m, const float* S, int mt, const float* T) {
-    red_.gram_mode = opt_.gram_mode;
-    red_.gram(m, S, mt, T, 0, L_.h * L_.h * L_.h);  // the L2 product <a, b> = h^3 sum a b
+void Solver::gram_checked(Reducer& red, int m, const float* S, int mt, const float* T) {
+    red.gram_mode = opt_.gram_mode;
+    red.gram(m, S, mt, T, 0, L_.h * L_.h * L_.h);  // the L2 product <a, b> = h^3 sum a b
 }
 
-EigenStats Solver::lobpcg(Channel& ch, const float* V, double tol, double guess_tol, int max_iter, int checked) {
+EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked) {
     EigenStats es;
     const int k = ch.k;
-    const int rb0 = red_.readbacks;
+    const int rb0 = lane.red.readbacks;
     const double omega = jacobi_omega();
     const double diag_t = -1.5 * COEFF0 / (L_.h * L_.h);
     const float ham_scale = (float)(-0.5 / (L_.h * L_.h));
@@ -538,15 +565,15 @@ EigenStats Solver::lobpcg(Channel& ch, const float* V, double tol, double guess_
         a.scale = ham_scale;
         a.V = V;
         a.vec0 = vec0;
-        launch_stencil(L_, in.tmap, count, a, out, s_);
+        launch_stencil(L_, in.tmap, count, a, out, lane.s);
     };
     // --- guess: one readback of X^T X and <x_i, H x_i>; dependent columns are re-seeded
     std::vector<double> theta(k), lambda(k);
     for (int round = 0;; ++round) {
         if (round >= MAX_RESEED_ROUNDS) throw NumericalError("lobpcg: could not generate independent guess vectors");
         apply_h(ch.A[ch.cur], 0, k, ch.HX.at(0));
-        gram_checked(k, ch.X(), k, ch.HX.at(0));
-        const double* g = red_.read(k * 2 * k);
+        gram_checked(lane.red, k, ch.X(), k, ch.HX.at(0));
+        const double* g = lane.red.read(k * 2 * k);
         std::vector<double> B((size_t)k * k);
         for (int i = 0; i < k; ++i)
             for (int j = 0; j < k; ++j) B[(size_t)i * k + j] = 0.5 * (g[(size_t)i * 2 * k + j] + g[(size_t)j * 2 * k + i]);
@@ -575,19 +602,19 @@ EigenStats Solver::lobpcg(Channel& ch, const float* V, double tol, double guess_
                         double x = L_.origin + i * L_.h, y = L_.origin + j * L_.h, z = L_.origin + kk * L_.h;
                         noise[q++] = (u - 0.5) * std::exp(-(x * x + y * y + z * z) / (2.0 * sigma2));
                     }
-            KS_CUDA(cudaMemcpyAsync(tmp.p, noise.data(), N * sizeof(double), cudaMemcpyHostToDevice, s_));
-            launch_pack(L_, 1, tmp.d(), ch.A[ch.cur].at(slot), s_);
-            KS_CUDA(cudaStreamSynchronize(s_));
+            KS_CUDA(cudaMemcpyAsync(tmp.p, noise.data(), N * sizeof(double), cudaMemcpyHostToDevice, lane.s));
+            launch_pack(L_, 1, tmp.d(), ch.A[ch.cur].at(slot), lane.s);
+            KS_CUDA(cudaStreamSynchronize(lane.s));
         }
     }
     lambda = theta;
     auto upload = [&](const std::vector<double>& th, const std::vector<double>& la, const std::vector<double>* coef) {
         size_t nd = 2 * (size_t)k + (coef ? coef->size() : 0);
-        double* up = upload_buffer(nd);
+        double* up = lane.upload_buffer(nd);
         std::copy(th.begin(), th.end(), up);
         std::copy(la.begin(), la.end(), up + k);
         if (coef) std::copy(coef->begin(), coef->end(), up + 2 * k);
-        KS_CUDA(cudaMemcpyAsync(theta_d, up, nd * sizeof(double), cudaMemcpyHostToDevice, s_));
+        KS_CUDA(cudaMemcpyAsync(theta_d, up, nd * sizeof(double), cudaMemcpyHostToDevice, lane.s));
     };
     upload(theta, lambda, nullptr);
     int np = 0, iterations = 0, best_it = 0;
@@ -598,12 +625,12 @@ EigenStats Solver::lobpcg(Channel& ch, const float* V, double tol, double guess_
     for (;;) {
         Block& S = ch.A[ch.cur];
         // 1. R = HX - theta X with the first Jacobi sweep fused (into Q), then 3 damped sweeps Q -> W -> Q -> W
-        double* norm_partials = red_.partials();
-        const int nb = red_.blocks();
-        launch_residual_precond(L_, k, ch.HX.at(0), ch.X(), theta_d, V, lambda_d, diag_t, ch.T.at(0), ch.Q.at(0), norm_partials, nb, s_);
+        double* norm_partials = lane.red.partials();
+        const int nb = lane.red.blocks();
+        launch_residual_precond(L_, k, ch.HX.at(0), ch.X(), theta_d, V, lambda_d, diag_t, ch.T.at(0), ch.Q.at(0), norm_partials, nb, lane.s);
         const int m = 2 * k + np;
         const int off_norm = m * 2 * m;
-        launch_finish(norm_partials, nb, k, L_.h * L_.h * L_.h, red_.res() + off_norm, s_);
+        launch_finish(norm_partials, nb, k, L_.h * L_.h * L_.h, lane.red.res() + off_norm, lane.s);
         StencilArgs jac;
         jac.mode = ST_JACOBI;
         jac.scale = ham_scale;
@@ -613,16 +640,16 @@ EigenStats Solver::lobpcg(Channel& ch, const float* V, double tol, double guess_
         jac.omega = (float)omega;
         jac.diag_t = (float)diag_t;
         jac.vec0 = 0;
-        launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), s_);       // Q -> W
+        launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), lane.s);       // Q -> W
         jac.vec0 = k;
-        launch_stencil(L_, S.tmap, k, jac, ch.Q.at(0), s_);       // W -> Q
+        launch_stencil(L_, S.tmap, k, jac, ch.Q.at(0), lane.s);       // W -> Q
         jac.vec0 = 0;
-        launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), s_);       // Q -> W
+        launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), lane.s);       // Q -> W
         // 2. HW and HP in one launch (W and P are contiguous after X)
         apply_h(S, k, k + np, ch.T.at(k));
         // 3. the readback: G = S^T [S | T] and |r_i|^2
-        gram_checked(m, S.at(0), m, ch.T.at(0));
-        const double* g = red_.read(off_norm + k);
+        gram_checked(lane.red, m, S.at(0), m, ch.T.at(0));
+        const double* g = lane.red.read(off_norm + k);
         const int mc = 2 * m;
         std::vector<double> A((size_t)m * m), B((size_t)m * m);
         for (int i = 0; i < m; ++i)
@@ -723,16 +750,16 @@ EigenStats Solver::lobpcg(Channel& ch, const float* V, double tol, double guess_
         prev_theta = theta;
         have_prev = true;
         theta = th;
-        dense_s_ += secs(t_dense);
+        lane.dense_s += secs(t_dense);
         upload(theta, lambda, &coef);
         const int next = ch.cur ^ 1;
-        launch_block_lincomb(L_.F, m, S.at(0), 2 * k, coef_d, ch.A[next].at(0), k, k, s_);
+        launch_block_lincomb(L_.F, m, S.at(0), 2 * k, coef_d, ch.A[next].at(0), k, k, lane.s);
         ch.cur = next;
         np = k;
         // 6. HX of the new X
         apply_h(ch.A[ch.cur], 0, k, ch.HX.at(0));
     }
-    es.readbacks = red_.readbacks - rb0;
+    es.readbacks = lane.red.readbacks - rb0;
     return es;
 }
 
@@ -741,9 +768,9 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
     auto t0 = clk::now();
     std::memset(out, 0, sizeof(*out));
     profile = ks_profile{};
-    const int rb0 = red_.readbacks;
-    const double wait0 = red_.wait_s;
-    dense_s_ = 0.0;
+    const int rb0 = readbacks_total();
+    const double wait0 = wait_total();
+    for (auto& l : lane_) l->dense_s = 0.0;
     if (nn < 0 || n_up < 0 || n_dn < 0 || (nn > 0 && !nuc)) { error = "invalid arguments"; return KS_INVALID; }
     if (nn > 32) { error = "at most 32 nuclei"; return KS_INVALID; }
     // E_nn (crates/qm/src/nuclear.rs:277-289)
@@ -838,9 +865,9 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 KS_CUDA(cudaMemcpyAsync(out_dn_.at(0), in_dn_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
                 KS_CUDA(cudaStreamSynchronize(s_));
                 profile.steps = iterations;
-                profile.readbacks = red_.readbacks - rb0;
-                profile.host_dense_s = dense_s_;
-                profile.sync_wait_s = red_.wait_s - wait0;
+                profile.readbacks = readbacks_total() - rb0;
+                profile.host_dense_s = lane_[0]->dense_s + lane_[1]->dense_s;
+                profile.sync_wait_s = wait_total() - wait0;
                 profile.wall_s = secs(t0);
                 error = "abandoned before SCF step " + std::to_string(iterations + 1);
                 return KS_ABORTED;
@@ -871,9 +898,47 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             last_step_res = 0.0;
             last_step_maxiter = false;
             auto te = clk::now();
+            // the two spin channels are independent: each runs on its own lane (stream, reducer) and,
+            // when both are occupied, the down channel on a second host thread, so one channel's
+            // kernels fill the GPU while the other waits on a readback or does its host algebra
+            EigenStats est[2];
+            {
+                KS_CUDA(cudaEventRecord(ev_fork_, s_));
+                for (auto& l : lane_) KS_CUDA(cudaStreamWaitEvent(l->s, ev_fork_, 0));
+                auto run = [&](int sp) {
+                    est[sp] = lobpcg(ch_[sp], *lane_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, EIG_GUESS_FACTOR * step_tol,
+                                     EIGEN_MAX_ITER, nocc[sp]);
+                };
+                std::exception_ptr err_dn;
+                std::thread worker;
+                const bool both = nocc[0] > 0 && nocc[1] > 0;
+                if (both)
+                    worker = std::thread([&] {
+                        try {
+                            KS_CUDA(cudaSetDevice(dev_));
+                            run(1);
+                        } catch (...) {
+                            err_dn = std::current_exception();
+                        }
+                    });
+                std::exception_ptr err_up;
+                try {
+                    if (nocc[0] > 0) run(0);
+                    if (!both && nocc[1] > 0) run(1);
+                } catch (...) {
+                    err_up = std::current_exception();
+                }
+                if (worker.joinable()) worker.join();
+                for (auto& l : lane_) {
+                    KS_CUDA(cudaEventRecord(l->ev_join, l->s));
+                    KS_CUDA(cudaStreamWaitEvent(s_, l->ev_join, 0));
+                }
+                if (err_up) std::rethrow_exception(err_up);
+                if (err_dn) std::rethrow_exception(err_dn);
+            }
             for (int sp = 0; sp < 2; ++sp) {
                 if (nocc[sp] == 0) continue;
-                EigenStats es = lobpcg(ch_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, EIG_GUESS_FACTOR * step_tol, EIGEN_MAX_ITER, nocc[sp]);
+                const EigenStats& es = est[sp];
                 ++profile.eigen_calls;
                 profile.eigen_iterations += es.iterations;
                 eig_its += es.iterations;
@@ -975,17 +1040,17 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         out->tol_used = test_tol;
         if (stalled) {
             error = "SCF stalled: best dRho " + std::to_string(best) + " not improved 2x in " + std::to_string(s.stall_window) + " iterations";
-            profile.readbacks = red_.readbacks - rb0;
-            profile.host_dense_s = dense_s_;
-            profile.sync_wait_s = red_.wait_s - wait0;
+            profile.readbacks = readbacks_total() - rb0;
+            profile.host_dense_s = lane_[0]->dense_s + lane_[1]->dense_s;
+            profile.sync_wait_s = wait_total() - wait0;
             profile.wall_s = secs(t0);
             return KS_STALLED;
         }
         if (!(delta_rho < test_tol)) {
             error = "SCF did not converge after " + std::to_string(iterations) + " iterations (dRho = " + std::to_string(delta_rho) + ")";
-            profile.readbacks = red_.readbacks - rb0;
-            profile.host_dense_s = dense_s_;
-            profile.sync_wait_s = red_.wait_s - wait0;
+            profile.readbacks = readbacks_total() - rb0;
+            profile.host_dense_s = lane_[0]->dense_s + lane_[1]->dense_s;
+            profile.sync_wait_s = wait_total() - wait0;
             profile.wall_s = secs(t0);
             return KS_NOT_CONVERGED;
         }
@@ -1040,9 +1105,9 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         if (last_step_maxiter || !(last_step_res <= LAST_STEP_RESIDUAL_FACTOR * eig_lo)) ++out->n_warnings;
         converged_ = true;
         have_warm_ = true;
-        profile.readbacks = red_.readbacks - rb0;
-        profile.host_dense_s = dense_s_;
-        profile.sync_wait_s = red_.wait_s - wait0;
+        profile.readbacks = readbacks_total() - rb0;
+        profile.host_dense_s = lane_[0]->dense_s + lane_[1]->dense_s;
+        profile.sync_wait_s = wait_total() - wait0;
         profile.wall_s = secs(t0);
         return KS_OK;
     } catch (const NumericalError& e) {

@@ -42,6 +42,9 @@ struct Block {
 // Device reductions with a fixed grid (deterministic), results kept on the device until read.
 class Reducer {
 public:
+    Reducer() = default;
+    Reducer(const Reducer&) = delete;
+    Reducer& operator=(const Reducer&) = delete;
     void init(const Layout& L, cudaStream_t s, size_t partial_doubles);
     // sum_p a_p b_p * scale for every pair, written to res()[off + i]
     void dots(const std::vector<std::pair<const float*, const float*>>& pairs, int off, double scale);
@@ -119,6 +122,23 @@ struct Channel {
     float* X() const { return A[cur].at(0); }
 };
 
+// A spin channel's execution lane: its own stream, reducer (device partials, pinned readback) and
+// pinned upload buffer, so that the two channels' LOBPCG solves can run concurrently.
+struct Lane {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev_join = nullptr;
+    Reducer red;
+    double* up = nullptr;
+    size_t up_cap = 0;
+    double dense_s = 0;  // host time in the Rayleigh-Ritz algebra (profile)
+    Lane() = default;
+    Lane(const Lane&) = delete;
+    Lane& operator=(const Lane&) = delete;
+    void init(const Layout& L);
+    double* upload_buffer(size_t doubles);
+    ~Lane();
+};
+
 struct SolverOptions { int gram_mode = 0; int n_extra = 0; int init_mode = 0; };
 
 class Solver {
@@ -128,7 +148,8 @@ public:
     ks_status solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,
                     void* user, ks_stats* out);
     ks_status forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n);
-    EigenStats lobpcg(Channel& ch, const float* V, double tol, double guess_tol, int max_iter, int checked);
+    EigenStats lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked);
+    Lane& lane(int i) { return *lane_[i]; }
     std::string error;
     const Layout& layout() const { return L_; }
     cudaStream_t stream() const { return s_; }
@@ -144,7 +165,9 @@ public:
 
 private:
     void ensure_channel(int spin, int k);
-    void gram_checked(int m, const float* S, int mt, const float* T);
+    void gram_checked(Reducer& red, int m, const float* S, int mt, const float* T);
+    int readbacks_total() const { return red_.readbacks + lane_[0]->red.readbacks + lane_[1]->red.readbacks; }
+    double wait_total() const { return red_.wait_s + lane_[0]->red.wait_s + lane_[1]->red.wait_s; }
     Layout L_;
     SolverOptions opt_;
     cudaStream_t s_ = nullptr;
@@ -158,7 +181,9 @@ private:
     DevBuf nuc_d_;
     bool converged_ = false;
     bool have_warm_ = false;
-    double dense_s_ = 0;  // host time in the Rayleigh-Ritz algebra (profile)
+    std::unique_ptr<Lane> lane_[2];
+    cudaEvent_t ev_fork_ = nullptr;
+    int dev_ = 0;
     double floor_;
 };
 
