@@ -143,6 +143,16 @@ ks_status ks_forces(void* solver, const ks_nucleus* nuclei, int n_nuclei, double
     });
 }
 
+ks_status ks_vjp(void* solver, const ks_nucleus* nuclei, int n_nuclei, double sigma, double e_bar, double* dE_dR3n, double* dE_dsigma) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h) return fail(h, KS_INVALID, "null solver");
+    return guarded(h, [&] {
+        ks_status st = h->solver->vjp(nuclei, n_nuclei, sigma, e_bar, dE_dR3n, dE_dsigma);
+        if (st != KS_OK) h->error = h->solver->error;
+        return st;
+    });
+}
+
 ks_status ks_state_counts(const void* solver, int* n_up, int* n_dn) {
     auto* h = static_cast<const Handle*>(solver);
     if (!h || !h->solver->has_state()) return KS_NO_STATE;

@@ -5,14 +5,17 @@
 // reduction dimension K is the grid itself (~10^6 points), split across one persistent CTA per SM.
 //
 // Precision ("3xTF32"): every f32 input x is split into hi = x with the low 13 mantissa bits
-// cleared (exactly a TF32 value) and lo = x - hi (exact in f32); each K-step issues hi*hi + hi*lo +
-// lo*hi on kind::tf32, so products carry ~22 significant bits (the dropped lo*lo term is ~2^-22
-// relative). kind::tf32 reads only the top 19 bits of each 32-bit operand, so the loaded tile
-// itself serves as hi (the test suite checks the result against f64); only lo is written, into a
-// second tile. The tensor core's f32 accumulation rounds toward zero, so a stage's
-// hi*hi sum (4 K-steps) gets its own TMEM slot and is drained right after the stage into f32 sums
-// (round-to-nearest) that move into f64 every FLUSH stages; the small cross terms share one slot
-// for the whole range.
+// cleared (exactly a TF32 value) and lo = x - hi rounded to the nearest TF32; each K-step issues
+// hi*hi + hi*lo + lo*hi on kind::tf32, so products carry ~22 significant bits (the dropped lo*lo
+// term is ~2^-22 relative). kind::tf32 reads only the top 19 bits of each 32-bit operand, so the
+// loaded tile itself serves as hi (the test suite checks the result against f64); only lo is
+// written, into a second tile. The tensor core rounds toward zero -- its f32 accumulation and its
+// reading of an operand's low bits -- so lo is rounded explicitly (truncated, it would bias every
+// hi*lo term toward zero: lo has the sign of x) and each stage's hi*hi and cross-term sums get
+// their own TMEM slots, drained right after the stage into f32 sums (round-to-nearest) that move
+// into f64 every FLUSH stages. Measured relative bias of a Gram diagonal on random data: -3.5e-7
+// with truncated lo and a whole-range cross-term slot, -1.3e-7 (one MMA's own 8-product sum) at
+// best.
 //
 // Per CTA (15 warps): warp 12 lane 0 is the TMA producer (one 128B-swizzled box of the S rows and
 // one of the T rows per 32-point slab); warps 8..11 form lo;
@@ -105,6 +108,11 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar)) : "memory");
 }
 
+// x rounded to the nearest TF32 value (ties away from zero): the tensor core itself reads only the top 19
+// bits, which truncates toward zero. lo = x - hi has the sign of x (hi is x truncated), so a truncated lo
+// would bias every hi*lo term toward zero.
+__device__ __forceinline__ float tf32_rn(float x) { return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u); }
+
 struct Params {
     long long F;  // points per field (multiple of 4)
     int m, mt;
@@ -129,11 +137,11 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
     const int R = p.R;
     unsigned char* hi = base;
     unsigned char* lo = base + (size_t)R * p.tbytes;
-    __shared__ __align__(8) uint64_t full[RMAX], conv[RMAX], empty[RMAX], acc_full[NBUF_MAX], acc_empty[NBUF_MAX], cdone;
+    __shared__ __align__(8) uint64_t full[RMAX], conv[RMAX], empty[RMAX], acc_full[NBUF_MAX], acc_empty[NBUF_MAX];
     __shared__ unsigned tmem_base;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nbuf = min(NBUF_MAX, (512 - p.N) / p.N);  // TMEM: slot C + nbuf hi*hi slots of N columns
+    const int nbuf = min(NBUF_MAX, 512 / (2 * p.N));  // TMEM: nbuf buffers of two N-column slots (hi*hi, cross)
     // this CTA's contiguous range of stages (P slabs of 32 points each)
     const int per = (p.stages_total + gridDim.x - 1) / gridDim.x;
     const int s0 = blockIdx.x * per;
@@ -147,10 +155,9 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
             mbar_init(&empty[i], 2);  // both MMA issuers release a tile
         }
         for (int i = 0; i < NBUF_MAX; ++i) {
-            mbar_init(&acc_full[i], 1);
+            mbar_init(&acc_full[i], 2);  // both issuers commit to a buffer
             mbar_init(&acc_empty[i], 8);
         }
-        mbar_init(&cdone, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // zero the rings and the tail once (rows that are never loaded stay zero)
@@ -202,10 +209,10 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
             for (int u = 0; u < 8; ++u) {
                 if (t + 128 * u < n4) {
                     float4 b;
-                    b.x = x[u].x - __uint_as_float(__float_as_uint(x[u].x) & 0xFFFFE000u);
-                    b.y = x[u].y - __uint_as_float(__float_as_uint(x[u].y) & 0xFFFFE000u);
-                    b.z = x[u].z - __uint_as_float(__float_as_uint(x[u].z) & 0xFFFFE000u);
-                    b.w = x[u].w - __uint_as_float(__float_as_uint(x[u].w) & 0xFFFFE000u);
+                    b.x = tf32_rn(x[u].x - __uint_as_float(__float_as_uint(x[u].x) & 0xFFFFE000u));
+                    b.y = tf32_rn(x[u].y - __uint_as_float(__float_as_uint(x[u].y) & 0xFFFFE000u));
+                    b.z = tf32_rn(x[u].z - __uint_as_float(__float_as_uint(x[u].z) & 0xFFFFE000u));
+                    b.w = tf32_rn(x[u].w - __uint_as_float(__float_as_uint(x[u].w) & 0xFFFFE000u));
                     l4[t + 128 * u] = b;
                 }
             }
@@ -215,59 +222,49 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
             if (++s == R) { s = 0; ph ^= 1u; }
         }
     } else if (warp == 13 || warp == 14) {
-        // ---- MMA issuers (one thread each, so their issue latencies overlap). Warp 13 puts a stage's
-        // hi*hi products (4 K-steps, 3 accumulating adds) into buffer b = i % nbuf of N columns,
-        // which the epilogue drains as soon as the stage is done: the tensor core's f32 accumulation
-        // rounds toward zero, so no hi*hi sum runs longer than one stage. Warp 14 accumulates the
-        // hi*lo + lo*hi cross terms of the whole range in slot C (columns [0, N); 2^-11 of the main
-        // terms, so its own truncation is negligible). Descriptors advance by the tile size (ring)
-        // and 32 B per K-step (the address field counts 16-byte units).
+        // ---- MMA issuers (one thread each, so their issue latencies overlap). A stage writes buffer
+        // b = i % nbuf: warp 13 its hi*hi products (4 K-steps) into slot M, warp 14 its hi*lo + lo*hi
+        // cross terms (8 MMAs) into slot X; the epilogue drains both as soon as the stage is done. The
+        // tensor core's f32 accumulation rounds toward zero, so no sum runs longer than one stage (a
+        // whole-range cross-term slot biased the Gram by ~1e-7 relative). Descriptors advance by the
+        // tile size (ring) and 32 B per K-step (the address field counts 16-byte units).
         if (lane == 0) {
             const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(p.N >> 3) << 17) | ((unsigned)(ROWS >> 4) << 24);
             const unsigned long long dh0 = smem_desc(su32(hi)), dl0 = smem_desc(su32(lo));
             const unsigned long long step = (unsigned long long)(p.tbytes >> 4);
+            const bool main_issuer = warp == 13;
             int s = 0, b = 0;
             unsigned ph = 0, bph = 0;
-            if (warp == 13) {
-                for (int i = 0; i < nst; ++i) {
-                    if (i >= nbuf && !mbar_wait(&acc_empty[b], bph ^ 1u, p.err)) break;
-                    if (!mbar_wait(&conv[s], ph, p.err)) break;
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const unsigned d = tmem + (unsigned)(p.N + b * p.N);
-                    const unsigned long long h0 = dh0 + (unsigned long long)s * step;
+            for (int i = 0; i < nst; ++i) {
+                if (i >= nbuf && !mbar_wait(&acc_empty[b], bph ^ 1u, p.err)) break;
+                if (!mbar_wait(&conv[s], ph, p.err)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const unsigned d = tmem + (unsigned)(2 * b * p.N) + (main_issuer ? 0u : (unsigned)p.N);
+                const unsigned long long h0 = dh0 + (unsigned long long)s * step, l0 = dl0 + (unsigned long long)s * step;
+                if (main_issuer) {
                     mma_tf32(d, h0, h0, idesc, 0u);
 #pragma unroll
                     for (int kk = 1; kk < KT / 8; ++kk) mma_tf32(d, h0 + 2 * kk, h0 + 2 * kk, idesc, 1u);
-                    mma_commit(&empty[s]);     // this issuer is done with the stage's tiles
-                    mma_commit(&acc_full[b]);  // and the hi*hi slot is ready to drain
-                    if (++s == R) { s = 0; ph ^= 1u; }
-                    if (++b == nbuf) { b = 0; bph ^= 1u; }
-                }
-            } else {
-                const unsigned dC = tmem;
-                int i = 0;
-                for (; i < nst; ++i) {
-                    if (!mbar_wait(&conv[s], ph, p.err)) break;
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const unsigned long long h0 = dh0 + (unsigned long long)s * step, l0 = dl0 + (unsigned long long)s * step;
-                    mma_tf32(dC, h0, l0, idesc, i > 0 ? 1u : 0u);
-                    mma_tf32(dC, l0, h0, idesc, 1u);
+                } else {
+                    mma_tf32(d, h0, l0, idesc, 0u);
+                    mma_tf32(d, l0, h0, idesc, 1u);
 #pragma unroll
                     for (int kk = 1; kk < KT / 8; ++kk) {
-                        mma_tf32(dC, h0 + 2 * kk, l0 + 2 * kk, idesc, 1u);
-                        mma_tf32(dC, l0 + 2 * kk, h0 + 2 * kk, idesc, 1u);
+                        mma_tf32(d, h0 + 2 * kk, l0 + 2 * kk, idesc, 1u);
+                        mma_tf32(d, l0 + 2 * kk, h0 + 2 * kk, idesc, 1u);
                     }
-                    mma_commit(&empty[s]);
-                    if (++s == R) { s = 0; ph ^= 1u; }
                 }
-                if (i == nst) mma_commit(&cdone);  // slot C is final once these MMAs complete
+                mma_commit(&empty[s]);     // this issuer is done with the stage's tiles
+                mma_commit(&acc_full[b]);  // and its slot of buffer b is ready to drain
+                if (++s == R) { s = 0; ph ^= 1u; }
+                if (++b == nbuf) { b = 0; bph ^= 1u; }
             }
         }
     } else {
         // ---- epilogue: warps 0..7; warp w reads TMEM lanes 32(w%4)..+31 (row = lane index) and the
-        // column half w/4 of its rows' own N-column block. Each stage's hi*hi slot is added to f32
-        // sums (round-to-nearest), which go into f64 totals every FLUSH stages; slot C is added once
-        // at the end. With two slabs per stage, lane quadrants 0..3 hold S of slab 0, S of slab 1,
+        // column half w/4 of its rows' own N-column block. Each stage's two slots (hi*hi and cross
+        // terms) are added to f32 sums (round-to-nearest), which go into f64 totals every FLUSH
+        // stages. With two slabs per stage, lane quadrants 0..3 hold S of slab 0, S of slab 1,
         // T of slab 0, T of slab 1, and slab q's columns start at 32q.
         constexpr int HALF = NMAX / 2;
         const int quad = warp & 3, c0 = (warp >> 2) * HALF;
@@ -294,18 +291,25 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
         for (int i = 0; i < nst; ++i) {
             if (!mbar_wait(&acc_full[b], bph, p.err)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const unsigned ta = lane_base + (unsigned)(p.N + b * p.N);
-            unsigned r[HALF];
+            const unsigned ta = lane_base + (unsigned)(2 * b * p.N);
+            // 16 columns of both slots per tcgen05.ld round (registers: the 64-column form has 32 per thread)
 #pragma unroll
-            for (int g = 0; g < HALF; g += 8)
-                if (g < ncols) ld8(r + g, ta + g);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            for (int g0 = 0; g0 < HALF; g0 += 16) {
+                unsigned r[16], rx[16];
+#pragma unroll
+                for (int g = 0; g < 16; g += 8)
+                    if (g0 + g < ncols) {
+                        ld8(r + g, ta + g0 + g);
+                        ld8(rx + g, ta + p.N + g0 + g);
+                    }
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (g0 + j < ncols) fs[g0 + j] += __uint_as_float(r[j]) + __uint_as_float(rx[j]);
+            }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[b]);
-#pragma unroll
-            for (int j = 0; j < HALF; ++j)
-                if (j < ncols) fs[j] += __uint_as_float(r[j]);
             if (++since == FLUSH) {
 #pragma unroll
                 for (int j = 0; j < HALF; ++j) { acc[j] += (double)fs[j]; fs[j] = 0.f; }
@@ -316,17 +320,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_tc_kernel(const __grid_consta
         }
 #pragma unroll
         for (int j = 0; j < HALF; ++j) acc[j] += (double)fs[j];
-        if (done == nst && nst > 0 && ncols > 0 && mbar_wait(&cdone, 0u, p.err)) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            unsigned rc[HALF];
-#pragma unroll
-            for (int g = 0; g < HALF; g += 8)
-                if (g < ncols) ld8(rc + g, lane_base + g);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int j = 0; j < HALF; ++j)
-                if (j < ncols) acc[j] += (double)__uint_as_float(rc[j]);
-        }
+        (void)done;
         if (orow >= 0) {
             double* out = partials + ((size_t)blockIdx.x * p.P + slab) * (p.m + p.mt) * p.m + (size_t)orow * p.m;
 #pragma unroll

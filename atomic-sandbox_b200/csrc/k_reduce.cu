@@ -208,6 +208,56 @@ __global__ void __launch_bounds__(TPB) forces_kernel(int n, int P, double h, dou
     }
 }
 
+// The adjoint of the Kohn-Sham energy with respect to the nuclear positions and the smearing width.
+// At self-consistency E is stationary in the density, so the response of the Hartree and XC terms
+// (and of the kinetic energy) to a change of V_ext vanishes and the VJP reduces to
+//     dE/dR_I     = integral rho(r) dV_I/dR_I = integral rho Z_I g'(d)/d (r - R_I),   g(d) = erf(d / (sigma sqrt 2)) / d
+//     dE/dsigma   = integral rho(r) sum_I dV_I/dsigma = integral rho sum_I Z_I sqrt(2/pi) exp(-d^2 / (2 sigma^2)) / sigma^2
+// (V_I = -Z_I g(d); crates/qm/src/nuclear.rs:258-272 and crates/qm/src/forces.rs:177-227 for the
+// position term). rho is recomputed here from the occupied orbitals of both spins in f64, not read
+// from a stored density. partials: [blocks][3 nn + 1], dV not applied.
+__global__ void __launch_bounds__(TPB) vjp_kernel(int n, int P, long long F, double h, double origin, const float* __restrict__ up, int nup,
+                                                  const float* __restrict__ dn, int ndn, const Nuc* __restrict__ nuc, int nn, double sigma,
+                                                  double* __restrict__ partials) {
+    double acc[3 * MAX_NUC + 1];
+    for (int q = 0; q < 3 * nn + 1; ++q) acc[q] = 0.0;
+    const long long N = (long long)n * n * n;
+    const double inv2s2 = 1.0 / (2.0 * sigma * sigma);
+    const double csig = 0.79788456080286536 / (sigma * sigma);  // sqrt(2/pi) / sigma^2
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % n);
+        long long rest = p / n;
+        int j = (int)(rest % n), k = (int)(rest / n);
+        const long long e = ((long long)k * n + j) * P + i;
+        double r = 0.0;
+        for (int v = 0; v < nup; ++v) {
+            const double x = (double)up[(long long)v * F + e];
+            r += x * x;
+        }
+        for (int v = 0; v < ndn; ++v) {
+            const double x = (double)dn[(long long)v * F + e];
+            r += x * x;
+        }
+        if (r == 0.0) continue;
+        double x = origin + i * h, y = origin + j * h, z = origin + k * h;
+        for (int a = 0; a < nn; ++a) {
+            double dx = x - nuc[a].x, dy = y - nuc[a].y, dz = z - nuc[a].z;
+            double d2 = dx * dx + dy * dy + dz * dz;
+            acc[3 * nn] += r * nuc[a].Z * csig * exp(-d2 * inv2s2);
+            double d = sqrt(d2);
+            if (d < 1e-8) continue;
+            double w = r * nuc[a].Z * g_prime(d, sigma) / d;
+            acc[3 * a] += w * dx;
+            acc[3 * a + 1] += w * dy;
+            acc[3 * a + 2] += w * dz;
+        }
+    }
+    for (int q = 0; q < 3 * nn + 1; ++q) {
+        double s = block_sum(acc[q]);
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * (3 * nn + 1) + q] = s;
+    }
+}
+
 }  // namespace
 
 int reduce_blocks(long long F) {
@@ -253,6 +303,13 @@ void launch_moments(const Layout& L, const float* rho, double* partials, int blo
 
 void launch_face_max(const Layout& L, const float* f, double* partials, int blocks, cudaStream_t s) {
     face_max_kernel<<<blocks, TPB, 0, s>>>(L.n, L.P, f, partials);
+    KS_LAUNCH_CHECK();
+}
+
+void launch_vjp(const Layout& L, const float* up, int nup, const float* dn, int ndn, const Nuc* nuc, int nn, double sigma,
+                double* partials, int blocks, cudaStream_t s) {
+    if (nn > MAX_NUC) throw std::invalid_argument("vjp: at most 32 nuclei");
+    vjp_kernel<<<blocks, TPB, 0, s>>>(L.n, L.P, L.F, L.h, L.origin, up, nup, dn, ndn, nuc, nn, sigma, partials);
     KS_LAUNCH_CHECK();
 }
 

@@ -13,6 +13,8 @@
 // What changes on the B200: every reduction is finished on the device, the CG scalars never
 // leave it, the preconditioner/H-products/Ritz updates run as block kernels over all vectors of a
 // channel at once, and the SCF's charge renormalisation is a device-side scale.
+#include <cstdio>
+#include <cstdlib>
 #include <exception>
 #include <mutex>
 #include <thread>
@@ -848,6 +850,11 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             for (auto& r : gram) r.erase(r.begin());
         };
 
+        // KS_TRACE=1 in the environment prints one line per SCF step to stderr (the reference's trace switch)
+        static const bool trace = [] {
+            const char* t = std::getenv("KS_TRACE");
+            return t && *t && *t != '0';
+        }();
         int iterations = 0;
         double delta_rho = INFINITY, test_tol = s.tol;
         double q_out[2] = {0, 0};
@@ -873,6 +880,13 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 return KS_ABORTED;
             }
             ++iterations;
+            // a warm guess is accepted within the 1.5x band only in the convergence phase (the previous step's dRho
+            // already below tol); before that only within the step's own tol. This is the reference's rule for its
+            // Fermi-Dirac channels (crates/qm-gpu/src/scf.rs module doc, "The guess band only in the convergence
+            // phase"); its Aufbau path keeps the band on every step, where a head that hovers at the band edge
+            // alternates frozen / re-solved, resets DIIS every other step and can stall at dRho ~1e-4 (10 of 64
+            // jittered batch molecules); with the rule all 64 converge in fewer steps.
+            const double guess_factor = delta_rho < test_tol ? EIG_GUESS_FACTOR : 1.0;
             const double step_tol = delta_rho < test_tol ? eig_lo
                                                          : (std::isfinite(delta_rho) ? std::min(std::max(EIG_TOL_FRACTION * delta_rho, eig_lo),
                                                                                                 std::max(EIG_TOL_MAX, eig_lo))
@@ -906,7 +920,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 KS_CUDA(cudaEventRecord(ev_fork_, s_));
                 for (auto& l : lane_) KS_CUDA(cudaStreamWaitEvent(l->s, ev_fork_, 0));
                 auto run = [&](int sp) {
-                    est[sp] = lobpcg(ch_[sp], *lane_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, EIG_GUESS_FACTOR * step_tol,
+                    est[sp] = lobpcg(ch_[sp], *lane_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, guess_factor * step_tol,
                                      EIGEN_MAX_ITER, nocc[sp]);
                 };
                 std::exception_ptr err_dn;
@@ -979,6 +993,17 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             q_out[1] = h[3];
             std::vector<double> row;
             for (size_t q = 0; q + 1 < pairs.size(); q += 2) row.push_back(h[4 + q] + h[5 + q]);
+            if (trace) {
+                // the reference's SCF trace line (crates/qm-gpu/src/scf.rs:1509-1512), plus the occupied eigenvalues
+                std::fprintf(stderr, "scf step %d: dRho %.3e (up %.2e dn %.2e), DIIS history %zu, eig tol %.2e, eigen last-step residual %.2e, eigen it this step %d, evals",
+                             iterations, delta_rho, h[0], h[2], hist.size(), step_tol, last_step_res, eig_its);
+                for (int sp = 0; sp < 2; ++sp) {
+                    std::fprintf(stderr, " %s", sp ? "| dn" : "up");
+                    for (size_t i = 0; i < ch_[sp].evals.size() && nocc[sp] > 0; ++i)
+                        std::fprintf(stderr, "%s%.6f", (int)i == nocc[sp] ? " / " : " ", ch_[sp].evals[i]);
+                }
+                std::fprintf(stderr, "\n");
+            }
             // stall watch (crates/qm/src/scf.rs:440-480)
             if (delta_rho < best) best = delta_rho;
             if (std::isfinite(delta_rho) && (!std::isfinite(anchor) || delta_rho <= 0.5 * anchor)) { anchor = delta_rho; anchor_at = iterations; }
@@ -1154,6 +1179,45 @@ ks_status Solver::forces(const ks_nucleus* nuc, int nn, double sigma, double* ou
                 double sc = (double)nuc[a].z * (double)nuc[b].z / (d * d * d);
                 for (int c = 0; c < 3; ++c) out3n[3 * a + c] += sc * dv[c];
             }
+        return KS_OK;
+    } catch (const DeviceError& e) {
+        error = e.what();
+        return KS_DEVICE;
+    }
+}
+
+ks_status Solver::vjp(const ks_nucleus* nuc, int nn, double sigma, double e_bar, double* dE_dR3n, double* dE_dsigma) {
+    if (!converged_) { error = "no converged state"; return KS_NO_STATE; }
+    if (nn <= 0 || nn > 32 || !nuc || !dE_dR3n || !dE_dsigma || !(sigma > 0) || !std::isfinite(e_bar)) {
+        error = "invalid arguments";
+        return KS_INVALID;
+    }
+    try {
+        std::vector<Nuc> hn(nn);
+        for (int i = 0; i < nn; ++i) hn[i] = Nuc{nuc[i].pos[0], nuc[i].pos[1], nuc[i].pos[2], (double)nuc[i].z};
+        nuc_d_.alloc(hn.size() * sizeof(Nuc));
+        KS_CUDA(cudaMemcpyAsync(nuc_d_.p, hn.data(), hn.size() * sizeof(Nuc), cudaMemcpyHostToDevice, s_));
+        const int nv = 3 * nn + 1;
+        launch_vjp(L_, nocc_[0] ? ch_[0].X() : nullptr, nocc_[0], nocc_[1] ? ch_[1].X() : nullptr, nocc_[1],
+                   static_cast<const Nuc*>(nuc_d_.p), nn, sigma, red_.partials(), red_.blocks(), s_);
+        launch_finish(red_.partials(), red_.blocks(), nv, L_.h * L_.h * L_.h, red_.res(), s_);
+        const double* g = red_.read(nv);
+        for (int i = 0; i < 3 * nn; ++i) dE_dR3n[i] = g[i];
+        *dE_dsigma = e_bar * g[3 * nn];
+        // point-charge repulsion E_nn = sum Z_a Z_b / |R_a - R_b| (independent of sigma)
+        for (int a = 0; a < nn; ++a)
+            for (int b = 0; b < nn; ++b) {
+                if (a == b) continue;
+                double dv[3] = {nuc[a].pos[0] - nuc[b].pos[0], nuc[a].pos[1] - nuc[b].pos[1], nuc[a].pos[2] - nuc[b].pos[2]};
+                double d = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+                if (d < 1e-8) {
+                    error = "nuclei " + std::to_string(std::min(a, b)) + " and " + std::to_string(std::max(a, b)) + " coincide";
+                    return KS_COINCIDENT_NUCLEI;
+                }
+                double sc = (double)nuc[a].z * (double)nuc[b].z / (d * d * d);
+                for (int c = 0; c < 3; ++c) dE_dR3n[3 * a + c] -= sc * dv[c];
+            }
+        for (int i = 0; i < 3 * nn; ++i) dE_dR3n[i] *= e_bar;
         return KS_OK;
     } catch (const DeviceError& e) {
         error = e.what();

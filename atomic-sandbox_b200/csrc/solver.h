@@ -148,6 +148,7 @@ public:
     ks_status solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,
                     void* user, ks_stats* out);
     ks_status forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n);
+    ks_status vjp(const ks_nucleus* nuc, int nn, double sigma, double e_bar, double* dE_dR3n, double* dE_dsigma);
     EigenStats lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked);
     Lane& lane(int i) { return *lane_[i]; }
     std::string error;

@@ -101,7 +101,7 @@ EXPORTED = [
     "ks_state_density", "ks_state_potentials", "ks_state_orbitals", "ks_profile_get", "ks_apply_hamiltonian",
     "ks_apply_laplacian", "ks_apply_precond", "ks_xc_lsda", "ks_nuclear_potential", "ks_poisson_solve", "ks_gram", "ks_lobpcg",
     "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
-    "ks_gram_device_noalloc",
+    "ks_gram_device_noalloc", "ks_vjp",
 ]
 
 
@@ -130,6 +130,7 @@ def lib():
         L.ks_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(_Settings), ctypes.c_int, ABORT_FN, ctypes.c_void_p, ctypes.POINTER(_Stats)]
         L.ks_forces.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, dp]
+        L.ks_vjp.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp]
         L.ks_state_counts.argtypes = [ctypes.c_void_p, ip, ip]
         L.ks_state_evals.argtypes = [ctypes.c_void_p, dp, dp]
         L.ks_state_density.argtypes = [ctypes.c_void_p, dp, dp]
@@ -278,6 +279,15 @@ class GpuSolver:
         out = np.empty(3 * len(nuclei))
         _check(lib().ks_forces(self._h, nuclei_array(nuclei), len(nuclei), float(self.h if sigma is None else sigma), _p(out)), self._h)
         return out.reshape(-1, 3)
+
+    def vjp(self, nuclei, sigma=None, e_bar=1.0):
+        """Reverse-mode derivative of the converged total energy: (e_bar * dE/dR as (n, 3), e_bar * dE/dsigma)
+        (ks_vjp). dE/dR equals minus forces()."""
+        g = np.empty(3 * len(nuclei))
+        gs = ctypes.c_double()
+        _check(lib().ks_vjp(self._h, nuclei_array(nuclei), len(nuclei), float(self.h if sigma is None else sigma), float(e_bar), _p(g),
+                            ctypes.byref(gs)), self._h)
+        return g.reshape(-1, 3), gs.value
 
     def counts(self):
         a, b = ctypes.c_int(), ctypes.c_int()

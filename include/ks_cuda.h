@@ -97,6 +97,15 @@ ks_status ks_solve(void* solver, const ks_nucleus* nuclei, int n_nuclei, int n_u
    (out3n[3*i + axis]) from the converged state, plus the point nuclear repulsion. */
 ks_status ks_forces(void* solver, const ks_nucleus* nuclei, int n_nuclei, double sigma, double* out3n);
 
+/* Reverse-mode derivative (vector-Jacobian product) of the converged total energy E with respect to the
+   nuclear positions and the smearing width: dE_dR3n[3*i + axis] = e_bar * dE/dR_i, *dE_dsigma = e_bar *
+   dE/dsigma. At self-consistency E is stationary in the density, so the Hartree, XC and kinetic responses
+   vanish and the product is the explicit derivative of the external energy (rho recomputed on the device
+   from the occupied orbitals) plus the point-nuclear repulsion. No reference counterpart (new API); its
+   position part equals -GpuSolver::forces (crates/qm-gpu/src/forces.rs:239). */
+ks_status ks_vjp(void* solver, const ks_nucleus* nuclei, int n_nuclei, double sigma, double e_bar, double* dE_dR3n,
+                 double* dE_dsigma);
+
 /* The message of the last failure on this handle (or of ks_solver_create when solver is NULL). */
 const char* ks_last_error(const void* solver);
 
