@@ -172,6 +172,17 @@ ks_status ks_state_evals(const void* solver, double* up, double* dn) {
     return KS_OK;
 }
 
+ks_status ks_state_occupations(const void* solver, double* up, double* dn) {
+    auto* h = static_cast<const Handle*>(solver);
+    if (!h || !h->solver->has_state()) return KS_NO_STATE;
+    for (int sp = 0; sp < 2; ++sp) {
+        double* dst = sp ? dn : up;
+        const auto& f = h->solver->occupations(sp);
+        for (int i = 0; i < h->solver->count(sp); ++i) dst[i] = f[i];
+    }
+    return KS_OK;
+}
+
 ks_status ks_state_density(const void* solver, double* rho_up, double* rho_dn) {
     auto* h = const_cast<Handle*>(static_cast<const Handle*>(solver));
     if (!h || !h->solver->has_state()) return KS_NO_STATE;

@@ -302,5 +302,76 @@ bool diis_coefficients(int m, const Mat& gram, std::vector<double>& c) {
     return true;
 }
 
+
+namespace {
+// f at x = (e - mu)/kT, never forming e^|x| > 1
+double fd_occupation(double x) {
+    if (x >= 0.0) {
+        const double e = std::exp(-x);
+        return e / (1.0 + e);
+    }
+    return 1.0 / (1.0 + std::exp(x));
+}
+// s(x) = ln(1 + e^-|x|) + |x| / (1 + e^|x|) = -[f ln f + (1 - f) ln(1 - f)], with the 0 ln 0 limits built in
+double fd_entropy(double x) {
+    const double a = std::fabs(x);
+    if (std::isinf(a)) return 0.0;
+    return std::log1p(std::exp(-a)) + a / (1.0 + std::exp(a));
+}
+double compensated(int k, const double* ev, double mu, double kt, bool entropy) {
+    double sum = 0.0, c = 0.0;
+    for (int i = 0; i < k; ++i) {
+        const double x = entropy ? fd_entropy((ev[i] - mu) / kt) : fd_occupation((ev[i] - mu) / kt);
+        const double t = sum + x;
+        c += std::fabs(sum) >= std::fabs(x) ? (sum - t) + x : (x - t) + sum;
+        sum = t;
+    }
+    return sum + c;
+}
+double fd_bisect(const double* ev, int k, double n, double kt, double lo, double hi, bool ge) {
+    for (int h = 0; h < 2048; ++h) {
+        const double mid = 0.5 * lo + 0.5 * hi;
+        if (mid <= lo || mid >= hi) break;
+        const double d = compensated(k, ev, mid, kt, false) - n;
+        if (ge ? d >= 0.0 : d > 0.0) hi = mid;
+        else lo = mid;
+    }
+    return ge ? hi : lo;
+}
+}  // namespace
+
+bool fermi_dirac(const double* ev, int k, int n, double kt, double* f, double& mu, double& entropy) {
+    if (n == 0) {
+        for (int i = 0; i < k; ++i) f[i] = 0.0;
+        mu = NAN;
+        entropy = 0.0;
+        return true;
+    }
+    if (k < n + 1 || !(std::isfinite(kt) && kt > 0.0)) return false;
+    double lo = INFINITY, hi = -INFINITY;
+    for (int i = 0; i < k; ++i) {
+        if (!std::isfinite(ev[i])) return false;
+        lo = std::fmin(lo, ev[i]);
+        hi = std::fmax(hi, ev[i]);
+    }
+    lo -= 50.0 * kt;
+    hi += 50.0 * kt;
+    const double nf = (double)n;
+    if (!(std::isfinite(lo) && std::isfinite(hi) && compensated(k, ev, lo, kt, false) < nf && compensated(k, ev, hi, kt, false) > nf))
+        return false;
+    mu = 0.5 * fd_bisect(ev, k, nf, kt, lo, hi, true) + 0.5 * fd_bisect(ev, k, nf, kt, lo, hi, false);
+    for (int i = 0; i < k; ++i) f[i] = fd_occupation((ev[i] - mu) / kt);
+    entropy = compensated(k, ev, mu, kt, true);
+    return true;
+}
+
+bool fd_witness(const double* ev, int k, int n, double mu, double kt) {
+    if (n == 0) return true;
+    if (k <= n) return false;
+    std::vector<double> s(ev, ev + k);
+    std::sort(s.begin(), s.end());
+    return s.back() >= s[n - 1] + 0.1 && s.back() - mu >= 36.0 * kt;
+}
+
 }  // namespace dense
 }  // namespace ks

@@ -31,5 +31,14 @@ bool lu_solve(int n, Mat a, std::vector<double>& b);
 // solve fails or gives non-finite coefficients.
 bool diis_coefficients(int m, const Mat& gram, std::vector<double>& c);
 
+// Fermi-Dirac occupations of one channel with n electrons over k levels at temperature kt (Ha)
+// (crates/qm/src/occupations.rs fermi_dirac): f in evals' order, mu the midpoint of the plateau
+// found by two tie-directed bisections over [min - 50 kT, max + 50 kT], S = sum s(x) compensated.
+// n = 0 gives every f = 0 and mu = NaN. Returns false on refused inputs (k < n + 1, a non-finite
+// level or kT).
+bool fermi_dirac(const double* evals, int k, int n, double kt, double* f, double& mu, double& entropy);
+// The highest level at least 0.1 Ha above the n-th lowest and 36 kT above mu (occupations.rs witness_reached).
+bool fd_witness(const double* evals, int k, int n, double mu, double kt);
+
 }  // namespace dense
 }  // namespace ks

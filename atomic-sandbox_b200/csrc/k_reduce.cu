@@ -217,7 +217,8 @@ __global__ void __launch_bounds__(TPB) forces_kernel(int n, int P, double h, dou
 // position term). rho is recomputed here from the occupied orbitals of both spins in f64, not read
 // from a stored density. partials: [blocks][3 nn + 1], dV not applied.
 __global__ void __launch_bounds__(TPB) vjp_kernel(int n, int P, long long F, double h, double origin, const float* __restrict__ up, int nup,
-                                                  const float* __restrict__ dn, int ndn, const Nuc* __restrict__ nuc, int nn, double sigma,
+                                                  const double* __restrict__ wu, const float* __restrict__ dn, int ndn,
+                                                  const double* __restrict__ wd, const Nuc* __restrict__ nuc, int nn, double sigma,
                                                   double* __restrict__ partials) {
     double acc[3 * MAX_NUC + 1];
     for (int q = 0; q < 3 * nn + 1; ++q) acc[q] = 0.0;
@@ -232,11 +233,11 @@ __global__ void __launch_bounds__(TPB) vjp_kernel(int n, int P, long long F, dou
         double r = 0.0;
         for (int v = 0; v < nup; ++v) {
             const double x = (double)up[(long long)v * F + e];
-            r += x * x;
+            r += (wu ? wu[v] : 1.0) * x * x;
         }
         for (int v = 0; v < ndn; ++v) {
             const double x = (double)dn[(long long)v * F + e];
-            r += x * x;
+            r += (wd ? wd[v] : 1.0) * x * x;
         }
         if (r == 0.0) continue;
         double x = origin + i * h, y = origin + j * h, z = origin + k * h;
@@ -306,10 +307,10 @@ void launch_face_max(const Layout& L, const float* f, double* partials, int bloc
     KS_LAUNCH_CHECK();
 }
 
-void launch_vjp(const Layout& L, const float* up, int nup, const float* dn, int ndn, const Nuc* nuc, int nn, double sigma,
-                double* partials, int blocks, cudaStream_t s) {
+void launch_vjp(const Layout& L, const float* up, int nup, const double* wu, const float* dn, int ndn, const double* wd, const Nuc* nuc,
+                int nn, double sigma, double* partials, int blocks, cudaStream_t s) {
     if (nn > MAX_NUC) throw std::invalid_argument("vjp: at most 32 nuclei");
-    vjp_kernel<<<blocks, TPB, 0, s>>>(L.n, L.P, L.F, L.h, L.origin, up, nup, dn, ndn, nuc, nn, sigma, partials);
+    vjp_kernel<<<blocks, TPB, 0, s>>>(L.n, L.P, L.F, L.h, L.origin, up, nup, wu, dn, ndn, wd, nuc, nn, sigma, partials);
     KS_LAUNCH_CHECK();
 }
 

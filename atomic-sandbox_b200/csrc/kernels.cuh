@@ -106,9 +106,10 @@ void launch_finish_max(const double* partials, int blocks, double* out, cudaStre
 // Hellmann-Feynman electronic force partials: [blocks][3*nn] of sum rho * (-Z g'(d)/d) * (r - R)
 // (crates/qm/src/forces.rs:205-218)
 // dE/dR_I and dE/dsigma of the converged state (adjoint of the stationary KS energy; rho recomputed
-// from the occupied orbitals): partials [blocks][3 nn + 1] (dE/dR of nucleus a at 3a..3a+2, dE/dsigma last).
-void launch_vjp(const Layout& L, const float* up, int nup, const float* dn, int ndn, const Nuc* nuc, int nn, double sigma,
-                double* partials, int blocks, cudaStream_t s);
+// from the orbitals, weighted by wu / wd when given): partials [blocks][3 nn + 1] (dE/dR of nucleus a at
+// 3a..3a+2, dE/dsigma last).
+void launch_vjp(const Layout& L, const float* up, int nup, const double* wu, const float* dn, int ndn, const double* wd, const Nuc* nuc,
+                int nn, double sigma, double* partials, int blocks, cudaStream_t s);
 void launch_forces(const Layout& L, const float* rho, const Nuc* nuc, int nn, double sigma, double* partials, int blocks,
                    cudaStream_t s);
 

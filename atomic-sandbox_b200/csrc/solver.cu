@@ -91,6 +91,12 @@ constexpr int POISSON_MAX_ITER = 5000;
 constexpr int EIGEN_MAX_ITER = 200;
 constexpr double EIG_TOL_FLOOR_FACTOR = 3.0;
 constexpr double EIG_GUESS_FACTOR = 1.5;
+// Fermi-Dirac (crates/qm/src/occupations.rs): a level with min(f, 1 - f) at or above PARTIAL_OCCUPATION_MIN is partly
+// occupied, and a step with one is tested against max(tol, GPU_PARTIAL_TOL); the columns of the block whose occupation
+// tail stays below LOOSE_F_FACTOR * tol are left out of the eigensolver's stop test (the guard tier).
+constexpr double PARTIAL_OCCUPATION_MIN = 1e-6;
+constexpr double GPU_PARTIAL_TOL = 1e-5;
+constexpr double LOOSE_F_FACTOR = 1e-2;
 constexpr double EIG_TOL_FRACTION = 0.0015;
 constexpr double EIG_TOL_MAX = 1e-3;
 constexpr double LAST_STEP_RESIDUAL_FACTOR = 3.0;
@@ -774,6 +780,11 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
     const double wait0 = wait_total();
     for (auto& l : lane_) l->dense_s = 0.0;
     if (nn < 0 || n_up < 0 || n_dn < 0 || (nn > 0 && !nuc)) { error = "invalid arguments"; return KS_INVALID; }
+    const bool fd = s.occupations == 1;
+    if (s.occupations < 0 || s.occupations > 1) { error = "occupations must be 0 (Aufbau) or 1 (Fermi-Dirac)"; return KS_INVALID; }
+    if (fd && !(std::isfinite(s.kt) && s.kt > 0.0)) { error = "Fermi-Dirac needs a finite kt > 0"; return KS_INVALID; }
+    if (fd && opt_.n_extra < 1) { error = "Fermi-Dirac needs n_extra >= 1 levels above N_sigma per channel (ks_options)"; return KS_INVALID; }
+    if (fd && std::max(n_up, n_dn) + opt_.n_extra > 64) { error = "Fermi-Dirac: at most 64 levels per channel"; return KS_INVALID; }
     if (nn > 32) { error = "at most 32 nuclei"; return KS_INVALID; }
     // E_nn (crates/qm/src/nuclear.rs:277-289)
     double e_nn = 0.0;
@@ -803,7 +814,13 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         const int nocc[2] = {n_up, n_dn};
         int kk[2];
         for (int sp = 0; sp < 2; ++sp) kk[sp] = nocc[sp] > 0 ? nocc[sp] + opt_.n_extra : 0;
-        const bool reuse = warm && have_warm_ && nocc_[0] == n_up && nocc_[1] == n_dn && ch_[0].k == kk[0] && ch_[1].k == kk[1];
+        const bool reuse = warm && have_warm_ && fd_state_ == fd && nocc_[0] == n_up && nocc_[1] == n_dn && ch_[0].k == kk[0] &&
+                           ch_[1].k == kk[1];
+        // columns held to the eigen tolerance: N_sigma, or under Fermi-Dirac the block minus its loose tail (set each step)
+        int tight[2] = {nocc[0], nocc[1]};
+        double entropy = 0.0, mu[2] = {NAN, NAN};
+        bool partial = false;
+        occ_d_.alloc(2 * 64 * sizeof(double));
         converged_ = false;
         have_warm_ = false;
         auto t_start = clk::now();
@@ -868,6 +885,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         while (iterations < s.max_iter) {
             if (abort_fn && abort_fn(user)) {
                 have_warm_ = true;  // park the iterate (orbitals, evals, input densities) as the next warm start
+                fd_state_ = fd;
                 KS_CUDA(cudaMemcpyAsync(out_up_.at(0), in_up_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
                 KS_CUDA(cudaMemcpyAsync(out_dn_.at(0), in_dn_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
                 KS_CUDA(cudaStreamSynchronize(s_));
@@ -921,7 +939,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 for (auto& l : lane_) KS_CUDA(cudaStreamWaitEvent(l->s, ev_fork_, 0));
                 auto run = [&](int sp) {
                     est[sp] = lobpcg(ch_[sp], *lane_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, guess_factor * step_tol,
-                                     EIGEN_MAX_ITER, nocc[sp]);
+                                     EIGEN_MAX_ITER, fd ? tight[sp] : nocc[sp]);
                 };
                 std::exception_ptr err_dn;
                 std::thread worker;
@@ -965,6 +983,33 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 if (es.stop == 2) last_step_maxiter = true;
             }
             profile.eigen_s += secs(te);
+            // occupations of this step's levels (crates/qm/src/scf.rs:996-1013): Aufbau 1 on the N_sigma lowest (the block
+            // is sorted by Ritz value), Fermi-Dirac f over the whole block, never mixed between steps
+            entropy = 0.0;
+            partial = false;
+            double occ_host[2 * 64] = {0.0};
+            for (int sp = 0; sp < 2; ++sp) {
+                occ_[sp].assign(kk[sp], 0.0);
+                mu[sp] = NAN;
+                if (kk[sp] == 0) continue;
+                if (!fd) {
+                    for (int i = 0; i < nocc[sp]; ++i) occ_[sp][i] = 1.0;
+                    continue;
+                }
+                double s_sp = 0.0;
+                if (!dense::fermi_dirac(ch_[sp].evals.data(), kk[sp], nocc[sp], s.kt, occ_[sp].data(), mu[sp], s_sp))
+                    throw NumericalError("Fermi-Dirac occupations refused (a non-finite level)");
+                entropy += s_sp;
+                int t = kk[sp];
+                double tail = 0.0;
+                while (t > nocc[sp] && tail + occ_[sp][t - 1] < LOOSE_F_FACTOR * s.tol) tail += occ_[sp][--t];
+                tight[sp] = t;
+                for (int i = 0; i < kk[sp]; ++i) {
+                    partial = partial || std::min(occ_[sp][i], 1.0 - occ_[sp][i]) >= PARTIAL_OCCUPATION_MIN;
+                    occ_host[64 * sp + i] = occ_[sp][i];
+                }
+            }
+            if (fd) KS_CUDA(cudaMemcpyAsync(occ_d_.p, occ_host, sizeof(occ_host), cudaMemcpyHostToDevice, s_));
             // output densities, residuals, dRho, output charges and the new DIIS Gram row in one readback
             const int fe = free_list.back();
             Entry& E = diis_pool_[fe];
@@ -974,7 +1019,8 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 Block& outb = sp ? out_dn_ : out_up_;
                 Block& r = sp ? E.r_dn : E.r_up;
                 if (nocc[sp] > 0)
-                    launch_density_residual(L_.F, nocc[sp], ch_[sp].X(), nullptr, in.at(0), outb.at(0), r.at(0), red_.partials(), nb, s_);
+                    launch_density_residual(L_.F, fd ? kk[sp] : nocc[sp], ch_[sp].X(), fd ? occ_d_.d() + 64 * sp : nullptr, in.at(0),
+                                            outb.at(0), r.at(0), red_.partials(), nb, s_);
                 else
                     launch_density_residual(L_.F, 0, in.at(0), nullptr, in.at(0), outb.at(0), r.at(0), red_.partials(), nb, s_);
                 launch_finish(red_.partials(), nb, 2, dv, red_.res() + 2 * sp, s_);
@@ -1008,7 +1054,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             if (delta_rho < best) best = delta_rho;
             if (std::isfinite(delta_rho) && (!std::isfinite(anchor) || delta_rho <= 0.5 * anchor)) { anchor = delta_rho; anchor_at = iterations; }
             const int since = iterations - anchor_at;
-            test_tol = s.tol;
+            test_tol = (fd && partial) ? std::max(s.tol, GPU_PARTIAL_TOL) : s.tol;
             if (!std::isfinite(delta_rho) || (delta_rho < test_tol && step_tol <= eig_lo)) break;
             if (!(delta_rho < test_tol) && s.stall_window > 0 && since >= s.stall_window && best >= level) { stalled = true; break; }
             // DIIS restart when a frozen orbital set is re-solved (the map rho_in -> rho_out changed)
@@ -1079,6 +1125,14 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             profile.wall_s = secs(t0);
             return KS_NOT_CONVERGED;
         }
+        if (fd)
+            for (int sp = 0; sp < 2; ++sp)
+                if (nocc[sp] > 0 && !dense::fd_witness(ch_[sp].evals.data(), kk[sp], nocc[sp], mu[sp], s.kt)) {
+                    error = "no Fermi-Dirac gap witness in the block of " + std::to_string(kk[sp]) + " levels of spin " + std::to_string(sp) +
+                            " (its top level must lie 0.1 Ha above level N and 36 kT above mu): raise n_extra";
+                    profile.wall_s = secs(t0);
+                    return KS_NUMERICAL;
+                }
         // --- energy from the output density and orbitals
         Terms tsum;
         tsum.count = 2;
@@ -1094,13 +1148,18 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         launch_xc_veff(L_.F, out_up_.at(0), out_dn_.at(0), vnuc_.at(0), vh_.at(0), exc_.at(0), nullptr, nullptr, nullptr, nullptr, s_);
         std::vector<std::pair<const float*, const float*>> pairs = {
             {rho_tot_.at(0), vnuc_.at(0)}, {rho_tot_.at(0), vh_.at(0)}, {exc_.at(0), ones_.at(0)}};
+        std::vector<double> kin_w;  // the occupation of each orbital pair after the first three entries
         for (int sp = 0; sp < 2; ++sp) {
             if (nocc[sp] == 0) continue;
+            const int cols = fd ? kk[sp] : nocc[sp];
             StencilArgs kin;
             kin.mode = ST_LAPLACIAN;
             kin.scale = (float)(-0.5 / (L_.h * L_.h));
-            launch_stencil(L_, ch_[sp].A[ch_[sp].cur].tmap, nocc[sp], kin, ch_[sp].T.at(0), s_);
-            for (int i = 0; i < nocc[sp]; ++i) pairs.push_back({ch_[sp].A[ch_[sp].cur].at(i), ch_[sp].T.at(i)});
+            launch_stencil(L_, ch_[sp].A[ch_[sp].cur].tmap, cols, kin, ch_[sp].T.at(0), s_);
+            for (int i = 0; i < cols; ++i) {
+                pairs.push_back({ch_[sp].A[ch_[sp].cur].at(i), ch_[sp].T.at(i)});
+                kin_w.push_back(occ_[sp][i]);
+            }
         }
         red_.dots(pairs, 0, dv);
         const int nvals = (int)pairs.size();
@@ -1109,7 +1168,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         const double* h = red_.read(nvals + 1);
         double kinetic = 0.0, comp = 0.0;
         for (int q = 3; q < nvals; ++q) {  // Neumaier over the orbitals (crates/qm-gpu/src/scf.rs:1664-1667)
-            double x = h[q], t = kinetic + x;
+            double x = kin_w[q - 3] * h[q], t = kinetic + x;
             if (std::fabs(kinetic) >= std::fabs(x)) comp += (kinetic - t) + x; else comp += (x - t) + kinetic;
             kinetic = t;
         }
@@ -1121,8 +1180,12 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         en.xc = h[2];
         en.nuclear = e_nn;
         en.internal = en.kinetic + en.external_ + en.hartree + en.xc + en.nuclear;
-        en.ts = 0.0;
+        en.ts = fd ? s.kt * entropy : 0.0;  // F = E - kT S (crates/qm/src/scf.rs:1015-1018)
         en.total = en.internal - en.ts;
+        out->entropy = fd ? entropy : 0.0;
+        out->mu[0] = mu[0];
+        out->mu[1] = mu[1];
+        out->partial = partial ? 1 : 0;
         out->boundary_density = h[nvals];
         out->electrons[0] = q_out[0];
         out->electrons[1] = q_out[1];
@@ -1130,6 +1193,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         if (last_step_maxiter || !(last_step_res <= LAST_STEP_RESIDUAL_FACTOR * eig_lo)) ++out->n_warnings;
         converged_ = true;
         have_warm_ = true;
+        fd_state_ = fd;
         profile.readbacks = readbacks_total() - rb0;
         profile.host_dense_s = lane_[0]->dense_s + lane_[1]->dense_s;
         profile.sync_wait_s = wait_total() - wait0;
@@ -1198,8 +1262,12 @@ ks_status Solver::vjp(const ks_nucleus* nuc, int nn, double sigma, double e_bar,
         nuc_d_.alloc(hn.size() * sizeof(Nuc));
         KS_CUDA(cudaMemcpyAsync(nuc_d_.p, hn.data(), hn.size() * sizeof(Nuc), cudaMemcpyHostToDevice, s_));
         const int nv = 3 * nn + 1;
-        launch_vjp(L_, nocc_[0] ? ch_[0].X() : nullptr, nocc_[0], nocc_[1] ? ch_[1].X() : nullptr, nocc_[1],
-                   static_cast<const Nuc*>(nuc_d_.p), nn, sigma, red_.partials(), red_.blocks(), s_);
+        // the density of the state: the N_sigma orbitals, or the Fermi-Dirac block weighted by its occupations
+        const int cu = count(0), cd = count(1);
+        const double* wu = fd_state_ ? occ_d_.d() : nullptr;
+        const double* wd = fd_state_ ? occ_d_.d() + 64 : nullptr;
+        launch_vjp(L_, cu ? ch_[0].X() : nullptr, cu, wu, cd ? ch_[1].X() : nullptr, cd, wd, static_cast<const Nuc*>(nuc_d_.p), nn, sigma,
+                   red_.partials(), red_.blocks(), s_);
         launch_finish(red_.partials(), red_.blocks(), nv, L_.h * L_.h * L_.h, red_.res(), s_);
         const double* g = red_.read(nv);
         for (int i = 0; i < 3 * nn; ++i) dE_dR3n[i] = g[i];

@@ -155,7 +155,9 @@ public:
     const Layout& layout() const { return L_; }
     cudaStream_t stream() const { return s_; }
     bool has_state() const { return converged_; }
-    int count(int spin) const { return nocc_[spin]; }
+    // stored orbitals of the converged state: N_sigma under Aufbau, the N_sigma + n_extra block under Fermi-Dirac
+    int count(int spin) const { return fd_state_ ? ch_[spin].k : nocc_[spin]; }
+    const std::vector<double>& occupations(int spin) const { return occ_[spin]; }
     const Channel& channel(int spin) const { return ch_[spin]; }
     const float* rho(int spin) const { return spin ? out_dn_.at(0) : out_up_.at(0); }
     const float* v_nuc() const { return vnuc_.at(0); }
@@ -183,6 +185,9 @@ private:
     bool converged_ = false;
     bool have_warm_ = false;
     std::unique_ptr<Lane> lane_[2];
+    std::vector<double> occ_[2];   // occupation per column of each channel's block (the last step's)
+    bool fd_state_ = false;        // the state was converged under Fermi-Dirac
+    DevBuf occ_d_;                 // device copy of the occupations (2 x 64 doubles), density weights
     cudaEvent_t ev_fork_ = nullptr;
     int dev_ = 0;
     double floor_;

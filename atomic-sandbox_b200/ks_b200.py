@@ -31,7 +31,7 @@ class Nucleus(ctypes.Structure):
 class _Settings(ctypes.Structure):
     _fields_ = [("sigma", ctypes.c_double), ("tol", ctypes.c_double), ("mixing", ctypes.c_double),
                 ("eig_tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("diis_history", ctypes.c_int),
-                ("stall_window", ctypes.c_int)]
+                ("stall_window", ctypes.c_int), ("occupations", ctypes.c_int), ("kt", ctypes.c_double)]
 
 
 class _Options(ctypes.Structure):
@@ -47,7 +47,8 @@ class _Stats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("delta_rho", ctypes.c_double), ("energy", _Energy),
                 ("boundary_density", ctypes.c_double), ("max_eigen_residual", ctypes.c_double),
                 ("poisson_residual", ctypes.c_double), ("poisson_iterations", ctypes.c_int),
-                ("electrons", ctypes.c_double * 2), ("tol_used", ctypes.c_double), ("n_warnings", ctypes.c_int)]
+                ("electrons", ctypes.c_double * 2), ("tol_used", ctypes.c_double), ("n_warnings", ctypes.c_int),
+                ("entropy", ctypes.c_double), ("mu", ctypes.c_double * 2), ("partial", ctypes.c_int)]
 
 
 class _Profile(ctypes.Structure):
@@ -101,7 +102,7 @@ EXPORTED = [
     "ks_state_density", "ks_state_potentials", "ks_state_orbitals", "ks_profile_get", "ks_apply_hamiltonian",
     "ks_apply_laplacian", "ks_apply_precond", "ks_xc_lsda", "ks_nuclear_potential", "ks_poisson_solve", "ks_gram", "ks_lobpcg",
     "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
-    "ks_gram_device_noalloc", "ks_vjp",
+    "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations",
 ]
 
 
@@ -133,6 +134,7 @@ def lib():
         L.ks_vjp.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp]
         L.ks_state_counts.argtypes = [ctypes.c_void_p, ip, ip]
         L.ks_state_evals.argtypes = [ctypes.c_void_p, dp, dp]
+        L.ks_state_occupations.argtypes = [ctypes.c_void_p, dp, dp]
         L.ks_state_density.argtypes = [ctypes.c_void_p, dp, dp]
         L.ks_state_potentials.argtypes = [ctypes.c_void_p, dp, dp]
         L.ks_state_orbitals.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
@@ -196,6 +198,8 @@ class ScfSettings:
     eig_tol: float = 1e-6
     diis_history: int = 6
     stall_window: int = 50
+    occupations: str = "aufbau"  # or "fermi_dirac" (qm::Occupations, crates/qm/src/scf.rs:278)
+    kt: float = 5e-3             # Fermi-Dirac temperature (Ha), ELECTRON_KT (crates/qm/src/occupations.rs)
 
 
 @dataclasses.dataclass
@@ -257,8 +261,10 @@ class GpuSolver:
     def solve(self, system, settings=None, warm=False, should_abort=None):
         """Runs the SCF; returns the stats dict (ScfStats) or raises a QmError subclass."""
         s = settings or ScfSettings()
+        if s.occupations not in ("aufbau", "fermi_dirac"):
+            raise ValueError("occupations: 'aufbau' or 'fermi_dirac'")
         cs = _Settings(self.h if s.sigma is None else s.sigma, s.tol, s.mixing, s.eig_tol, s.max_iter, s.diis_history,
-                       s.stall_window)
+                       s.stall_window, 1 if s.occupations == "fermi_dirac" else 0, float(s.kt))
         st = _Stats()
         arr = nuclei_array(system.nuclei)
         cb = ABORT_FN(lambda _u: 1 if should_abort() else 0) if should_abort else ABORT_FN()
@@ -273,6 +279,7 @@ class GpuSolver:
             "boundary_density": st.boundary_density, "max_eigen_residual": st.max_eigen_residual,
             "poisson_residual": st.poisson_residual, "poisson_iterations": st.poisson_iterations,
             "electrons": list(st.electrons), "tol_used": st.tol_used, "n_warnings": st.n_warnings,
+            "entropy": st.entropy, "mu": list(st.mu), "partial": bool(st.partial),
         }
 
     def forces(self, nuclei, sigma=None):
@@ -298,6 +305,13 @@ class GpuSolver:
         nu, nd = self.counts()
         up, dn = np.empty(max(nu, 1)), np.empty(max(nd, 1))
         _check(lib().ks_state_evals(self._h, _p(up), _p(dn)), self._h)
+        return up[:nu], dn[:nd]
+
+    def occupations(self):
+        """One occupation per stored orbital: 1 under Aufbau, the final Fermi-Dirac f over the block otherwise."""
+        nu, nd = self.counts()
+        up, dn = np.empty(max(nu, 1)), np.empty(max(nd, 1))
+        _check(lib().ks_state_occupations(self._h, _p(up), _p(dn)), self._h)
         return up[:nu], dn[:nd]
 
     def density(self):

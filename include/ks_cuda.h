@@ -44,6 +44,9 @@ typedef struct {
     int max_iter;      /* SCF iteration cap (200) */
     int diis_history;  /* Pulay history (6) */
     int stall_window;  /* stall stop W (50; 0 = off) */
+    int occupations;   /* qm::Occupations (crates/qm/src/scf.rs:278): 0 Aufbau, 1 Fermi-Dirac at kt over N_sigma + n_extra
+                          levels per occupied channel (ks_options.n_extra >= 1; crates/qm/src/occupations.rs) */
+    double kt;         /* Fermi-Dirac temperature (Ha), e.g. 5e-3 (ELECTRON_KT, occupations.rs) */
 } ks_settings;
 
 /* Solver construction options (no reference counterpart: B200 choices). */
@@ -69,6 +72,9 @@ typedef struct {
     double electrons[2];
     double tol_used;
     int n_warnings;
+    double entropy;    /* Fermi-Dirac: S summed over the channels (energy.ts = kt * S, energy.total = F = internal - ts) */
+    double mu[2];      /* Fermi-Dirac: mu per spin (NaN for an empty channel or under Aufbau) */
+    int partial;       /* Fermi-Dirac: the final step had a partly occupied level (stop at max(tol, 1e-5)) */
 } ks_stats;
 
 /* qm_gpu::SolveProfile (crates/qm-gpu/src/scf.rs:448-514), subset. */
@@ -112,6 +118,9 @@ const char* ks_last_error(const void* solver);
 /* State access (GpuSolver::state / ks_state, crates/qm-gpu/src/scf.rs:1172, :1713-1775). */
 ks_status ks_state_counts(const void* solver, int* n_up, int* n_dn);
 ks_status ks_state_evals(const void* solver, double* up, double* dn);
+/* One occupation per stored orbital (qm::KsState occ_up / occ_dn): all 1 under Aufbau, the final step's Fermi-Dirac f
+   otherwise, where the stored block is N_sigma + n_extra levels (ks_state_counts reports the block sizes). */
+ks_status ks_state_occupations(const void* solver, double* up, double* dn);
 ks_status ks_state_density(const void* solver, double* rho_up, double* rho_dn);   /* n^3 each */
 ks_status ks_state_potentials(const void* solver, double* v_nuc, double* v_h);     /* n^3 each */
 ks_status ks_state_orbitals(const void* solver, int spin, double* out);            /* count * n^3 */

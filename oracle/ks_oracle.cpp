@@ -636,12 +636,78 @@ double g_prime(double d, double sigma) {
     return ((2.0 / std::sqrt(PI)) * u * std::exp(-u * u) - std::erf(u)) / (d * d);
 }
 
+// ---------------------------------------------------------------- Fermi-Dirac (crates/qm/src/occupations.rs)
+// f at x = (e - mu)/kT without forming an e^|x| > 1 (occupations.rs: `occupation`)
+double fd_occupation(double x) {
+    if (x >= 0.0) {
+        double e = std::exp(-x);
+        return e / (1.0 + e);
+    }
+    return 1.0 / (1.0 + std::exp(x));
+}
+// s(x) = ln(1 + e^-|x|) + |x| / (1 + e^|x|) (occupations.rs: `fd_entropy`)
+double fd_entropy(double x) {
+    double a = std::fabs(x);
+    if (std::isinf(a)) return 0.0;
+    return std::log1p(std::exp(-a)) + a / (1.0 + std::exp(a));
+}
+double fd_total(const double* ev, int k, double mu, double kt) {
+    return neumaier_fn((size_t)k, [&](size_t i) { return fd_occupation((ev[i] - mu) / kt); });
+}
+// one tie-directed bisection: ge -> returns hi (the least mu with sum f >= n), else lo (occupations.rs: `bisect`)
+double fd_bisect(const double* ev, int k, double n, double kt, double lo, double hi, bool ge) {
+    for (int h = 0; h < 2048; ++h) {
+        double mid = 0.5 * lo + 0.5 * hi;
+        if (mid <= lo || mid >= hi) break;
+        double d = fd_total(ev, k, mid, kt) - n;
+        bool to_hi = ge ? d >= 0.0 : d > 0.0;
+        if (to_hi) hi = mid; else lo = mid;
+    }
+    return ge ? hi : lo;
+}
+// occupations.rs: `fermi_dirac` (n = 0: every f = 0, S = 0)
+int fermi_dirac(const double* ev, int k, int n, double kt, double* f, double& mu, double& S) {
+    if (n == 0) {
+        for (int i = 0; i < k; ++i) f[i] = 0.0;
+        mu = NAN;
+        S = 0.0;
+        return 0;
+    }
+    if (k < n + 1 || !(std::isfinite(kt) && kt > 0.0)) return -1;
+    double lo = INFINITY, hi = -INFINITY;
+    for (int i = 0; i < k; ++i) {
+        if (!std::isfinite(ev[i])) return -1;
+        lo = std::fmin(lo, ev[i]);
+        hi = std::fmax(hi, ev[i]);
+    }
+    lo -= 50.0 * kt;
+    hi += 50.0 * kt;
+    const double nf = (double)n;
+    if (!(std::isfinite(lo) && std::isfinite(hi) && fd_total(ev, k, lo, kt) < nf && fd_total(ev, k, hi, kt) > nf)) return -1;
+    double mu_minus = fd_bisect(ev, k, nf, kt, lo, hi, true);
+    double mu_plus = fd_bisect(ev, k, nf, kt, lo, hi, false);
+    mu = 0.5 * mu_minus + 0.5 * mu_plus;
+    for (int i = 0; i < k; ++i) f[i] = fd_occupation((ev[i] - mu) / kt);
+    S = neumaier_fn((size_t)k, [&](size_t i) { return fd_entropy((ev[i] - mu) / kt); });
+    return 0;
+}
+// occupations.rs: `witness_reached` -- the highest level at least WITNESS_GAP = 0.1 Ha above the n-th lowest and
+// 36 kT above mu
+bool fd_witness(const Vec& ev, int n, double mu, double kt) {
+    if (n == 0) return true;
+    if ((int)ev.size() <= n) return false;
+    Vec s = ev;
+    std::sort(s.begin(), s.end());
+    return s.back() >= s[n - 1] + 0.1 && s.back() - mu >= 36.0 * kt;
+}
+
 }  // namespace
 
 struct ora_state {
     Grid g{1, 1.0};
     std::vector<Vec> orb_up, orb_dn;
     Vec ev_up, ev_dn, rho_up, rho_dn, v_nuc, v_h;
+    Vec occ_up, occ_dn;  // one occupation per stored orbital (all 1 under Aufbau)
     double sigma = 0;
 };
 
@@ -747,7 +813,12 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
 
     std::vector<Vec> orb_up, orb_dn;
     Vec ev_up, ev_dn, in_up, in_dn, v_h;
-    bool reuse = warm && warm->g == g && (int)warm->orb_up.size() == n_up && (int)warm->orb_dn.size() == n_dn;
+    const bool fd = s->occupations == 1;
+    // one block of N_sigma + n_extra levels per occupied channel under Fermi-Dirac (the reference grows a
+    // witness block by doubling; a fixed block whose top level passes the witness gives the same f to e^-36)
+    const int ku = n_up + ((fd && n_up > 0) ? std::max(1, s->n_extra) : 0);
+    const int kd = n_dn + ((fd && n_dn > 0) ? std::max(1, s->n_extra) : 0);
+    bool reuse = warm && warm->g == g && (int)warm->orb_up.size() == ku && (int)warm->orb_dn.size() == kd;
     if (reuse) {
         orb_up = warm->orb_up; orb_dn = warm->orb_dn; ev_up = warm->ev_up; ev_dn = warm->ev_dn;
         in_up = warm->rho_up; in_dn = warm->rho_dn; v_h = warm->v_h;
@@ -760,14 +831,14 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
         double scale = z_tot > 0.0 ? total / z_tot : 0.0;
         double fu = total > 0.0 ? n_up / total : 0.0, fd = total > 0.0 ? n_dn / total : 0.0;
         Vec buf;
-        buf.resize((size_t)std::max(n_up, 1) * N);
-        initial_orbitals(g, nuc, nn, n_up, 1, buf.data());
-        for (int i = 0; i < n_up; ++i) orb_up.emplace_back(buf.begin() + (size_t)i * N, buf.begin() + (size_t)(i + 1) * N);
-        buf.assign((size_t)std::max(n_dn, 1) * N, 0.0);
-        initial_orbitals(g, nuc, nn, n_dn, 2, buf.data());
-        for (int i = 0; i < n_dn; ++i) orb_dn.emplace_back(buf.begin() + (size_t)i * N, buf.begin() + (size_t)(i + 1) * N);
-        ev_up.assign(n_up, -1.0);
-        ev_dn.assign(n_dn, -1.0);
+        buf.resize((size_t)std::max(ku, 1) * N);
+        initial_orbitals(g, nuc, nn, ku, 1, buf.data());
+        for (int i = 0; i < ku; ++i) orb_up.emplace_back(buf.begin() + (size_t)i * N, buf.begin() + (size_t)(i + 1) * N);
+        buf.assign((size_t)std::max(kd, 1) * N, 0.0);
+        initial_orbitals(g, nuc, nn, kd, 2, buf.data());
+        for (int i = 0; i < kd; ++i) orb_dn.emplace_back(buf.begin() + (size_t)i * N, buf.begin() + (size_t)(i + 1) * N);
+        ev_up.assign(ku, -1.0);
+        ev_dn.assign(kd, -1.0);
         in_up.resize(N); in_dn.resize(N);
         for (size_t i = 0; i < N; ++i) { in_up[i] = guess[i] * scale * fu; in_dn[i] = guess[i] * scale * fd; }
         v_h.assign(N, 0.0);
@@ -776,6 +847,8 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
     int iterations = 0;
     double delta_rho = std::numeric_limits<double>::infinity();
     Vec out_up = in_up, out_dn = in_dn;
+    Vec occ_up(orb_up.size(), 1.0), occ_dn(orb_dn.size(), 1.0);
+    double entropy = 0.0, mu_up = NAN, mu_dn = NAN;
     std::vector<DiisEntry> hist;
     // StallWatch (scf.rs:440-480)
     double anchor = INFINITY, best = INFINITY;
@@ -806,10 +879,23 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
             eig_res = std::fmax(eig_res, mr);
             st->eigen_iterations_total += it;
         }
+        // occupations of this step's levels (Aufbau: the block is exactly N_sigma, all f = 1)
+        occ_up.assign(orb_up.size(), 1.0);
+        occ_dn.assign(orb_dn.size(), 1.0);
+        entropy = 0.0;
+        if (fd) {
+            double su = 0.0, sd = 0.0;
+            if (fermi_dirac(ev_up.data(), (int)ev_up.size(), n_up, s->kt, occ_up.data(), mu_up, su) != 0 ||
+                fermi_dirac(ev_dn.data(), (int)ev_dn.size(), n_dn, s->kt, occ_dn.data(), mu_dn, sd) != 0) {
+                st->status = 4;
+                return nullptr;
+            }
+            entropy = su + sd;
+        }
         out_up.assign(N, 0.0);
         out_dn.assign(N, 0.0);
-        for (auto& psi : orb_up) for (size_t i = 0; i < N; ++i) out_up[i] += psi[i] * psi[i];
-        for (auto& psi : orb_dn) for (size_t i = 0; i < N; ++i) out_dn[i] += psi[i] * psi[i];
+        for (size_t o = 0; o < orb_up.size(); ++o) for (size_t i = 0; i < N; ++i) out_up[i] += occ_up[o] * orb_up[o][i] * orb_up[o][i];
+        for (size_t o = 0; o < orb_dn.size(); ++o) for (size_t i = 0; i < N; ++i) out_dn[i] += occ_dn[o] * orb_dn[o][i] * orb_dn[o][i];
         delta_rho = neumaier_fn(N, [&](size_t i) {
             return std::fabs(out_up[i] - in_up[i]) + std::fabs(out_dn[i] - in_dn[i]);
         }) * g.dv();
@@ -836,6 +922,7 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
     st->max_eigen_residual = eig_res;
     if (stalled) { st->status = 2; return nullptr; }
     if (!(delta_rho < s->tol)) { st->status = 1; return nullptr; }
+    if (fd && !(fd_witness(ev_up, n_up, mu_up, s->kt) && fd_witness(ev_dn, n_dn, mu_dn, s->kt))) { st->status = 5; return nullptr; }
 
     Vec rho(N);
     for (size_t i = 0; i < N; ++i) rho[i] = out_up[i] + out_dn[i];
@@ -846,11 +933,14 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
     st->poisson_iterations_total += pit;
     Vec t(N);
     double kinetic_e = 0.0;
-    for (int spin = 0; spin < 2; ++spin)
-        for (auto& psi : (spin ? orb_dn : orb_up)) {
-            kinetic(g, psi.data(), t.data());
-            kinetic_e += gdot(g, psi, t);
+    for (int spin = 0; spin < 2; ++spin) {
+        auto& orb = spin ? orb_dn : orb_up;
+        auto& occ = spin ? occ_dn : occ_up;
+        for (size_t o = 0; o < orb.size(); ++o) {
+            kinetic(g, orb[o].data(), t.data());
+            kinetic_e += occ[o] * gdot(g, orb[o], t);
         }
+    }
     lsda(N, out_up.data(), out_dn.data(), exc.data(), xu.data(), xd.data());
     double external_ = gdot(g, rho, v_nuc);
     double hartree = 0.5 * gdot(g, rho, v_h);
@@ -863,7 +953,11 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
                 if (i == 0 || j == 0 || k == 0 || i == n - 1 || j == n - 1 || k == n - 1)
                     bmax = std::fmax(bmax, std::fabs(rho[g.idx(i, j, k)]));
     st->kinetic = kinetic_e; st->external_ = external_; st->hartree = hartree; st->xc = xc_e; st->nuclear = e_nn;
-    st->total = internal - 0.0;
+    st->ts = fd ? s->kt * entropy : 0.0;
+    st->entropy = entropy;
+    st->mu[0] = mu_up;
+    st->mu[1] = mu_dn;
+    st->total = internal - st->ts;
     st->boundary_density = bmax;
     st->poisson_residual = pois_res;
     st->poisson_iterations = pois_it;
@@ -872,6 +966,7 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
     st->status = 0;
     state->orb_up = std::move(orb_up); state->orb_dn = std::move(orb_dn);
     state->ev_up = ev_up; state->ev_dn = ev_dn;
+    state->occ_up = occ_up; state->occ_dn = occ_dn;
     state->rho_up = std::move(out_up); state->rho_dn = std::move(out_dn);
     state->v_nuc = std::move(v_nuc); state->v_h = std::move(v_h);
     return state.release();
@@ -888,6 +983,19 @@ int ora_state_counts(const ora_state* st, int* n_up, int* n_dn) {
 void ora_state_evals(const ora_state* st, double* up, double* dn) {
     std::copy(st->ev_up.begin(), st->ev_up.end(), up);
     std::copy(st->ev_dn.begin(), st->ev_dn.end(), dn);
+}
+
+void ora_state_occupations(const ora_state* st, double* up, double* dn) {
+    std::copy(st->occ_up.begin(), st->occ_up.end(), up);
+    std::copy(st->occ_dn.begin(), st->occ_dn.end(), dn);
+}
+
+int ora_fermi_dirac(const double* evals, int k, int n, double kt, double* f, double* mu, double* entropy) {
+    double m = NAN, S = 0.0;
+    int rc = fermi_dirac(evals, k, n, kt, f, m, S);
+    *mu = m;
+    *entropy = S;
+    return rc;
 }
 
 void ora_state_density(const ora_state* st, double* rho_up, double* rho_dn) {

@@ -19,10 +19,13 @@ extern "C" {
 
 typedef struct { double pos[3]; int z; } ora_nucleus;
 
-/* Settings of one SCF (crates/qm/src/scf.rs:375 ScfSettings, Aufbau occupations only). */
+/* Settings of one SCF (crates/qm/src/scf.rs:375 ScfSettings). occupations: 0 Aufbau, 1 Fermi-Dirac at kt
+   (crates/qm/src/occupations.rs) over a block of n_sigma + n_extra levels per occupied channel. */
 typedef struct {
     double sigma, tol, mixing, eig_tol;
     int max_iter, diis_history, stall_window;
+    int occupations, n_extra;
+    double kt;
 } ora_settings;
 
 typedef struct {
@@ -32,9 +35,14 @@ typedef struct {
     double boundary_density, max_eigen_residual, poisson_residual;
     int poisson_iterations;
     double electrons[2];
-    int status;          /* 0 ok, 1 not converged, 2 stalled, 3 coincident nuclei */
+    int status;          /* 0 ok, 1 not converged, 2 stalled, 3 coincident nuclei, 5 no Fermi-Dirac gap witness */
     int eigen_iterations_total, poisson_iterations_total;  /* work counters over the whole solve */
+    double ts, entropy, mu[2];  /* Fermi-Dirac: kT*S (total = internal - ts), S, mu per spin (NaN when empty) */
 } ora_stats;
+
+/* Fermi-Dirac occupations of one channel (crates/qm/src/occupations.rs fermi_dirac): f in evals' order, mu the
+   plateau midpoint of two tie-directed bisections, S Neumaier. Returns 0, or -1 on refused inputs. */
+int ora_fermi_dirac(const double* evals, int k, int n, double kt, double* f, double* mu, double* entropy);
 
 /* thread count for the parallel loops (stencils, pointwise); sums stay sequential */
 void ora_set_threads(int n);
@@ -74,6 +82,7 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
 void ora_state_free(ora_state* st);
 int  ora_state_counts(const ora_state* st, int* n_up, int* n_dn);
 void ora_state_evals(const ora_state* st, double* up, double* dn);
+void ora_state_occupations(const ora_state* st, double* up, double* dn);
 void ora_state_density(const ora_state* st, double* rho_up, double* rho_dn);
 void ora_state_potentials(const ora_state* st, double* v_nuc, double* v_h);
 void ora_state_orbitals(const ora_state* st, int spin, double* out);

@@ -22,7 +22,7 @@ class Nucleus(ctypes.Structure):
 class Settings(ctypes.Structure):
     _fields_ = [("sigma", ctypes.c_double), ("tol", ctypes.c_double), ("mixing", ctypes.c_double),
                 ("eig_tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("diis_history", ctypes.c_int),
-                ("stall_window", ctypes.c_int)]
+                ("stall_window", ctypes.c_int), ("occupations", ctypes.c_int), ("n_extra", ctypes.c_int), ("kt", ctypes.c_double)]
 
 
 class Stats(ctypes.Structure):
@@ -32,7 +32,8 @@ class Stats(ctypes.Structure):
                 ("boundary_density", ctypes.c_double), ("max_eigen_residual", ctypes.c_double),
                 ("poisson_residual", ctypes.c_double), ("poisson_iterations", ctypes.c_int),
                 ("electrons", ctypes.c_double * 2), ("status", ctypes.c_int),
-                ("eigen_iterations_total", ctypes.c_int), ("poisson_iterations_total", ctypes.c_int)]
+                ("eigen_iterations_total", ctypes.c_int), ("poisson_iterations_total", ctypes.c_int),
+                ("ts", ctypes.c_double), ("entropy", ctypes.c_double), ("mu", ctypes.c_double * 2)]
 
 
 def build():
@@ -62,6 +63,8 @@ def lib():
         L.ora_state_potentials.argtypes = [ctypes.c_void_p, dp, dp]
         L.ora_state_orbitals.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
         L.ora_forces.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, dp]
+        L.ora_state_occupations.argtypes = [ctypes.c_void_p, dp, dp]
+        L.ora_fermi_dirac.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -239,6 +242,12 @@ class State:
         lib().ora_state_evals(self.ptr, _p(up), _p(dn))
         return up[:nu], dn[:nd]
 
+    def occupations(self):
+        nu, nd = self.counts()
+        up, dn = np.empty(max(nu, 1)), np.empty(max(nd, 1))
+        lib().ora_state_occupations(self.ptr, _p(up), _p(dn))
+        return up[:nu], dn[:nd]
+
     def density(self):
         up, dn = np.empty(self.n ** 3), np.empty(self.n ** 3)
         lib().ora_state_density(self.ptr, _p(up), _p(dn))
@@ -258,15 +267,28 @@ class State:
 
 
 def scf(n, h, nuclei, n_up, n_dn, sigma=None, tol=1e-6, mixing=0.3, eig_tol=1e-6, max_iter=200, diis_history=6,
-        stall_window=50, warm=None):
-    """Aufbau SCF (crates/qm/src/scf.rs:909). Returns (State or None, stats dict)."""
-    s = Settings(h if sigma is None else sigma, tol, mixing, eig_tol, max_iter, diis_history, stall_window)
+        stall_window=50, warm=None, kt=None, n_extra=1):
+    """SCF (crates/qm/src/scf.rs:909): Aufbau, or Fermi-Dirac occupations at temperature kt (Ha) over
+    N_sigma + n_extra levels per occupied channel. Returns (State or None, stats dict)."""
+    s = Settings(h if sigma is None else sigma, tol, mixing, eig_tol, max_iter, diis_history, stall_window,
+                 0 if kt is None else 1, int(n_extra), 0.0 if kt is None else float(kt))
     st = Stats()
     ptr = lib().ora_scf(n, ctypes.c_double(h), nuclei_array(nuclei), len(nuclei), n_up, n_dn, ctypes.byref(s),
                         warm.ptr if warm is not None else None, ctypes.byref(st))
     stats = {f[0]: getattr(st, f[0]) for f in Stats._fields_}
     stats["electrons"] = list(st.electrons)
+    stats["mu"] = list(st.mu)
     return (State(ptr, n) if ptr else None), stats
+
+
+def fermi_dirac(evals, n, kt):
+    """Fermi-Dirac occupations of one channel (crates/qm/src/occupations.rs fermi_dirac): (f, mu, S)."""
+    ev = _f64(evals)
+    f = np.empty(max(ev.size, 1))
+    mu, S = ctypes.c_double(), ctypes.c_double()
+    if lib().ora_fermi_dirac(_p(ev), ev.size, int(n), ctypes.c_double(kt), _p(f), ctypes.byref(mu), ctypes.byref(S)) != 0:
+        raise ValueError("Fermi-Dirac occupations refused (fewer than n + 1 levels, a non-finite level or kT)")
+    return f[:ev.size], mu.value, S.value
 
 
 def forces(state, nuclei, sigma):
