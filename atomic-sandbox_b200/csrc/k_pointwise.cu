@@ -147,32 +147,50 @@ __global__ void lincomb_kernel(long long n4, float4* __restrict__ y, Terms t) {
     }
 }
 
-// out_j = sum_i C_ij S_i for up to QG outputs per CTA row (blockIdx.y picks the output group)
+// out_j = sum_i C_ij S_i for up to QG outputs per CTA row (blockIdx.y picks the output group). A thread
+// owns a float4 of the grid; its inputs are loaded 4 at a time (four 16-byte loads in flight per
+// thread, the loop is otherwise one dependent load per input; two CTAs per SM) and combined with
+// packed f32x2 FMAs on (x, y) and (z, w), in input order: the same roundings as one fmaf chain per
+// output element. m = 24, q = 16 at 95^3: 59 -> 47 us.
 constexpr int QG = 16;
-__global__ void block_lincomb_kernel(long long F4, int m, const float4* __restrict__ S, int q, const double* __restrict__ C,
-                                     float4* __restrict__ out, int split, int gap) {
-    __shared__ float cs[64 * QG];
+constexpr int LC_UNROLL = 4;
+__device__ __forceinline__ unsigned long long lc_fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__global__ void __launch_bounds__(TPB, 2) block_lincomb_kernel(long long F4, int m, const ulonglong2* __restrict__ S, int q,
+                                                            const double* __restrict__ C, ulonglong2* __restrict__ out, int split,
+                                                            int gap) {
+    __shared__ unsigned long long cs[64 * QG];  // (c, c) pairs
     const int j0 = blockIdx.y * QG;
     const int qn = min(QG, q - j0);
     for (int t = threadIdx.x; t < m * qn; t += blockDim.x) {
         int i = t % m, jj = t / m;
-        cs[jj * 64 + i] = (float)C[i + (size_t)m * (j0 + jj)];
+        const float c = (float)C[i + (size_t)m * (j0 + jj)];
+        cs[jj * 64 + i] = ((unsigned long long)__float_as_uint(c) << 32) | __float_as_uint(c);
     }
     __syncthreads();
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < F4; e += (long long)gridDim.x * blockDim.x) {
-        float4 acc[QG];
+        unsigned long long acc[QG][2];
 #pragma unroll
-        for (int jj = 0; jj < QG; ++jj) acc[jj] = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int i = 0; i < m; ++i) {
-            float4 s = S[(long long)i * F4 + e];
+        for (int jj = 0; jj < QG; ++jj) acc[jj][0] = acc[jj][1] = 0ull;
+        for (int i0 = 0; i0 < m; i0 += LC_UNROLL) {
+            ulonglong2 sv[LC_UNROLL];
 #pragma unroll
-            for (int jj = 0; jj < QG; ++jj) {
-                if (jj < qn) {
-                    float c = cs[jj * 64 + i];
-                    acc[jj].x = fmaf(c, s.x, acc[jj].x);
-                    acc[jj].y = fmaf(c, s.y, acc[jj].y);
-                    acc[jj].z = fmaf(c, s.z, acc[jj].z);
-                    acc[jj].w = fmaf(c, s.w, acc[jj].w);
+            for (int u = 0; u < LC_UNROLL; ++u)
+                if (i0 + u < m) sv[u] = S[(long long)(i0 + u) * F4 + e];
+#pragma unroll
+            for (int u = 0; u < LC_UNROLL; ++u) {
+                if (i0 + u < m) {
+#pragma unroll
+                    for (int jj = 0; jj < QG; ++jj) {
+                        if (jj < qn) {
+                            const unsigned long long c2 = cs[jj * 64 + i0 + u];
+                            acc[jj][0] = lc_fma2(c2, sv[u].x, acc[jj][0]);
+                            acc[jj][1] = lc_fma2(c2, sv[u].y, acc[jj][1]);
+                        }
+                    }
                 }
             }
         }
@@ -180,7 +198,7 @@ __global__ void block_lincomb_kernel(long long F4, int m, const float4* __restri
         for (int jj = 0; jj < QG; ++jj)
             if (jj < qn) {
                 int j = j0 + jj;
-                out[(long long)(j < split ? j : j + gap) * F4 + e] = acc[jj];
+                out[(long long)(j < split ? j : j + gap) * F4 + e] = make_ulonglong2(acc[jj][0], acc[jj][1]);
             }
     }
 }
@@ -401,7 +419,8 @@ void launch_block_lincomb(long long F, int m, const float* S, int q, const doubl
     if (m > 64) throw std::invalid_argument("block_lincomb: at most 64 input fields");
     long long F4 = F / 4;
     dim3 grid(stream_blocks(F4), ceil_div(q, QG));
-    block_lincomb_kernel<<<grid, TPB, 0, s>>>(F4, m, reinterpret_cast<const float4*>(S), q, C, reinterpret_cast<float4*>(out), split, gap);
+    block_lincomb_kernel<<<grid, TPB, 0, s>>>(F4, m, reinterpret_cast<const ulonglong2*>(S), q, C, reinterpret_cast<ulonglong2*>(out),
+                                              split, gap);
     KS_LAUNCH_CHECK();
 }
 
