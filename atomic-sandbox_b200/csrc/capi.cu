@@ -196,6 +196,67 @@ ks_status ks_state_density(const void* solver, double* rho_up, double* rho_dn) {
     });
 }
 
+ks_status ks_sample_density(void* solver, const double* pts3, int count, float* out) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h) return KS_INVALID;
+    if (count < 0 || (count > 0 && (!pts3 || !out))) return fail(h, KS_INVALID, "sample_density: need count >= 0 and points/out");
+    if (count > (1 << 28)) return fail(h, KS_INVALID, "sample_density: at most 2^28 points per call");
+    if (!h->solver->has_state()) return fail(h, KS_NO_STATE, "no converged state");
+    if (count == 0) return KS_OK;
+    return guarded(h, [&] {
+        h->solver->sample_density(pts3, count, out);
+        return KS_OK;
+    });
+}
+
+ks_status ks_sampling_counters(const void* solver, int* readbacks, int* allocations) {
+    auto* h = static_cast<const Handle*>(solver);
+    if (!h || !readbacks || !allocations) return KS_INVALID;
+    *readbacks = h->solver->sampling_readbacks;
+    *allocations = h->solver->sampling_allocations;
+    return KS_OK;
+}
+
+ks_status ks_state_density_f32(void* solver, float* rho) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h || !rho) return KS_INVALID;
+    if (!h->solver->has_state()) return fail(h, KS_NO_STATE, "no converged state");
+    return guarded(h, [&] {
+        h->solver->density_f32(rho);
+        return KS_OK;
+    });
+}
+
+ks_status ks_density_to_volume(void* solver, float* dense_dev, void* stream) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h || !dense_dev) return KS_INVALID;
+    if (!h->solver->has_state()) return fail(h, KS_NO_STATE, "no converged state");
+    return guarded(h, [&] {
+        h->solver->density_to_volume(dense_dev, static_cast<cudaStream_t>(stream));
+        return KS_OK;
+    });
+}
+
+ks_status ks_density_max(void* solver, double* out) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h || !out) return KS_INVALID;
+    if (!h->solver->has_state()) return fail(h, KS_NO_STATE, "no converged state");
+    return guarded(h, [&] {
+        *out = h->solver->density_max();
+        return KS_OK;
+    });
+}
+
+ks_status ks_spin_abs_integral(void* solver, double* out) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h || !out) return KS_INVALID;
+    if (!h->solver->has_state()) return fail(h, KS_NO_STATE, "no converged state");
+    return guarded(h, [&] {
+        *out = h->solver->spin_abs_integral();
+        return KS_OK;
+    });
+}
+
 ks_status ks_state_potentials(const void* solver, double* v_nuc, double* v_h) {
     auto* h = const_cast<Handle*>(static_cast<const Handle*>(solver));
     if (!h || !h->solver->has_state()) return KS_NO_STATE;

@@ -110,6 +110,14 @@ void launch_finish_max(const double* partials, int blocks, double* out, cudaStre
 // 3a..3a+2, dE/dsigma last).
 void launch_vjp(const Layout& L, const float* up, int nup, const double* wu, const float* dn, int ndn, const double* wd, const Nuc* nuc,
                 int nn, double sigma, double* partials, int blocks, cudaStream_t s);
+// ---------------------------------------------------------------- readouts (k_readout.cu)
+// out[q] = trilinear blend of f at pts[3q..3q+3) (Bohr), 0 outside [origin, origin + (n-1)h]^3
+// (crates/qm-gpu/src/sample.rs:84-121, crates/qm/src/grid.rs:54-86).
+void launch_sample(const Layout& L, const float* f, const double* pts, int count, float* out, cudaStream_t s);
+// dense n^3 f32 (x fastest) = f (+ g) without the pads, and per-block maxima in partials[blocks].
+void launch_volume(const Layout& L, const float* f, const float* g, float* dense, double* partials, int blocks, cudaStream_t s);
+// partials[blocks] of sum |a - b| over F floats (f64)
+void launch_abs_diff(long long F, const float* a, const float* b, double* partials, int blocks, cudaStream_t s);
 void launch_forces(const Layout& L, const float* rho, const Nuc* nuc, int nn, double sigma, double* partials, int blocks,
                    cudaStream_t s);
 

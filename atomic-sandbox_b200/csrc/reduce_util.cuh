@@ -51,3 +51,24 @@ __device__ __forceinline__ double block_max(double v) {
 }
 
 }  // namespace ks
+
+namespace ks {
+
+// Maximum over a 1-D CTA for values of any sign (empty lanes count as -inf); valid in thread 0.
+__device__ __forceinline__ double block_max_signed(double v) {
+    __shared__ double warp_part_s[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_max(v);
+    __syncthreads();
+    if (lane == 0) warp_part_s[warp] = v;
+    __syncthreads();
+    double s = -INFINITY;
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        s = lane < nw ? warp_part_s[lane] : -INFINITY;
+        s = warp_max(s);
+    }
+    return s;
+}
+
+}  // namespace ks

@@ -1293,4 +1293,81 @@ ks_status Solver::vjp(const ks_nucleus* nuc, int nn, double sigma, double e_bar,
     }
 }
 
+// ---------------------------------------------------------------- readouts of the converged state
+void Solver::total_density() {
+    Terms tsum;
+    tsum.count = 2;
+    tsum.x[0] = out_up_.at(0); tsum.c[0] = 1.f;
+    tsum.x[1] = out_dn_.at(0); tsum.c[1] = 1.f;
+    launch_lincomb(L_.F, 1, rho_tot_.at(0), tsum, s_);
+}
+
+// crates/qm-gpu/src/sample.rs:84-121: one launch and one readback per non-empty call; the point and
+// output buffers grow to the largest request and are reused.
+void Solver::sample_density(const double* pts3, int count, float* out) {
+    if (count <= 0) return;
+    if ((size_t)count > sample_cap_) {
+        sample_pts_.alloc((size_t)count * 3 * sizeof(double));
+        sample_out_.alloc((size_t)count * sizeof(float));
+        sample_cap_ = (size_t)count;
+        ++sampling_allocations;
+    }
+    KS_CUDA(cudaMemcpyAsync(sample_pts_.p, pts3, (size_t)count * 3 * sizeof(double), cudaMemcpyHostToDevice, s_));
+    total_density();
+    launch_sample(L_, rho_tot_.at(0), sample_pts_.d(), count, sample_out_.f(), s_);
+    KS_CUDA(cudaMemcpyAsync(out, sample_out_.p, (size_t)count * sizeof(float), cudaMemcpyDeviceToHost, s_));
+    KS_CUDA(cudaStreamSynchronize(s_));
+    ++sampling_readbacks;
+}
+
+// crates/qm-gpu/src/scf.rs:1776-1779 (density_f32): the interior of rho_up + rho_dn as stored, f32
+void Solver::density_f32(float* host_n3) {
+    const size_t bytes = (size_t)L_.interior() * sizeof(float);
+    if (volume_.bytes < bytes) volume_.alloc(bytes);
+    total_density();
+    launch_volume(L_, rho_tot_.at(0), nullptr, volume_.f(), red_.partials(), red_.blocks(), s_);
+    KS_CUDA(cudaMemcpyAsync(host_n3, volume_.p, bytes, cudaMemcpyDeviceToHost, s_));
+    KS_CUDA(cudaStreamSynchronize(s_));
+}
+
+// crates/qm-gpu/src/scf.rs:1780-1797: the dense n^3 image of the density on the device, enqueued on
+// `s` after the solver's own work; does not wait. (A headless buffer in place of the texture.)
+void Solver::density_to_volume(float* dense_dev, cudaStream_t s) {
+    total_density();
+    if (s && s != s_) {
+        cudaEvent_t ev;
+        KS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        KS_CUDA(cudaEventRecord(ev, s_));
+        KS_CUDA(cudaStreamWaitEvent(s, ev, 0));
+        KS_CUDA(cudaEventDestroy(ev));
+    }
+    // the per-block maxima land in the reducer's partials, unread; the stream joins keep them ordered
+    launch_volume(L_, rho_tot_.at(0), nullptr, dense_dev, red_.partials(), red_.blocks(), s ? s : s_);
+    if (s && s != s_) {
+        // the solver's stream must not reuse rho_tot_ or the partials before the copy is done
+        cudaEvent_t ev;
+        KS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        KS_CUDA(cudaEventRecord(ev, s));
+        KS_CUDA(cudaStreamWaitEvent(s_, ev, 0));
+        KS_CUDA(cudaEventDestroy(ev));
+    }
+}
+
+// crates/qm-gpu/src/scf.rs:1831-1834: max rho over the interior (one readback)
+double Solver::density_max() {
+    total_density();
+    const size_t bytes = (size_t)L_.interior() * sizeof(float);
+    if (volume_.bytes < bytes) volume_.alloc(bytes);
+    launch_volume(L_, rho_tot_.at(0), nullptr, volume_.f(), red_.partials(), red_.blocks(), s_);
+    launch_finish_max(red_.partials(), red_.blocks(), red_.res(), s_);
+    return red_.read(1)[0];
+}
+
+// crates/qm-gpu/src/scf.rs:1836-1842: integral of |rho_up - rho_dn| (electrons)
+double Solver::spin_abs_integral() {
+    launch_abs_diff(L_.F, out_up_.at(0), out_dn_.at(0), red_.partials(), red_.blocks(), s_);
+    launch_finish(red_.partials(), red_.blocks(), 1, L_.h * L_.h * L_.h, red_.res(), s_);
+    return red_.read(1)[0];
+}
+
 }  // namespace ks

@@ -162,6 +162,13 @@ public:
     const float* rho(int spin) const { return spin ? out_dn_.at(0) : out_up_.at(0); }
     const float* v_nuc() const { return vnuc_.at(0); }
     const float* v_h() const { return vh_.at(0); }
+    // readouts of the converged state (crates/qm-gpu/src/sample.rs, scf.rs:1776-1842)
+    void sample_density(const double* pts3, int count, float* out);
+    void density_f32(float* host_n3);
+    void density_to_volume(float* dense_dev, cudaStream_t s);
+    double density_max();
+    double spin_abs_integral();
+    int sampling_readbacks = 0, sampling_allocations = 0;
     ks_profile profile{};
     Poisson& poisson() { return poisson_; }
     Reducer& reducer() { return red_; }
@@ -182,6 +189,9 @@ private:
     struct Entry { Block rho_up, rho_dn, r_up, r_dn; };
     std::vector<Entry> diis_pool_;
     DevBuf nuc_d_;
+    DevBuf sample_pts_, sample_out_, volume_;  // grow-only readout buffers
+    size_t sample_cap_ = 0;
+    void total_density();                      // rho_tot_ = rho_up + rho_dn (f32) of the state
     bool converged_ = false;
     bool have_warm_ = false;
     std::unique_ptr<Lane> lane_[2];

@@ -102,7 +102,8 @@ EXPORTED = [
     "ks_state_density", "ks_state_potentials", "ks_state_orbitals", "ks_profile_get", "ks_apply_hamiltonian",
     "ks_apply_laplacian", "ks_apply_precond", "ks_xc_lsda", "ks_nuclear_potential", "ks_poisson_solve", "ks_gram", "ks_lobpcg",
     "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
-    "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations",
+    "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations", "ks_sample_density", "ks_sampling_counters",
+    "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral",
 ]
 
 
@@ -158,6 +159,13 @@ def lib():
                                      ctypes.c_void_p]
         L.ks_gram_device_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                              ctypes.c_void_p, ctypes.c_void_p]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.ks_sample_density.argtypes = [ctypes.c_void_p, dp, ctypes.c_int, fp]
+        L.ks_sampling_counters.argtypes = [ctypes.c_void_p, ip, ip]
+        L.ks_state_density_f32.argtypes = [ctypes.c_void_p, fp]
+        L.ks_density_to_volume.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.ks_density_max.argtypes = [ctypes.c_void_p, dp]
+        L.ks_spin_abs_integral.argtypes = [ctypes.c_void_p, dp]
         _lib = L
     return _lib
 
@@ -318,6 +326,46 @@ class GpuSolver:
         up, dn = np.empty(self.n ** 3), np.empty(self.n ** 3)
         _check(lib().ks_state_density(self._h, _p(up), _p(dn)), self._h)
         return up, dn
+
+    # ---- readouts (crates/qm-gpu/src/sample.rs, crates/qm-gpu/src/scf.rs:1776-1842)
+    def sample_density(self, points):
+        """rho_up + rho_dn at points (m, 3) Bohr by trilinear interpolation (f32 values, 0 outside the box);
+        one launch and one readback per non-empty call."""
+        pts = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 3))
+        out = np.empty(len(pts), dtype=np.float32)
+        if len(pts) == 0:
+            _check(lib().ks_sample_density(self._h, None, 0, None), self._h)
+            return out
+        _check(lib().ks_sample_density(self._h, _p(pts), len(pts), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self._h)
+        return out
+
+    def sampling_counters(self):
+        """(readbacks, buffer allocations) of sample_density so far."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(lib().ks_sampling_counters(self._h, ctypes.byref(a), ctypes.byref(b)), self._h)
+        return a.value, b.value
+
+    def density_f32(self):
+        """The stored total density rho_up + rho_dn, f32, n^3 (x fastest)."""
+        out = np.empty(self.n ** 3, dtype=np.float32)
+        _check(lib().ks_state_density_f32(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self._h)
+        return out
+
+    def copy_density_to_volume(self, dense_dev_ptr, stream=None):
+        """Writes the n^3 f32 image of the density to a device buffer (e.g. a torch tensor's data_ptr()), enqueued
+        on `stream` (a cudaStream_t as an int; None = the solver's stream). Does not wait."""
+        _check(lib().ks_density_to_volume(self._h, ctypes.c_void_p(int(dense_dev_ptr)), ctypes.c_void_p(stream or 0)), self._h)
+
+    def density_max(self):
+        v = ctypes.c_double()
+        _check(lib().ks_density_max(self._h, ctypes.byref(v)), self._h)
+        return v.value
+
+    def spin_abs_integral(self):
+        """The integral of |rho_up - rho_dn| (electrons)."""
+        v = ctypes.c_double()
+        _check(lib().ks_spin_abs_integral(self._h, ctypes.byref(v)), self._h)
+        return v.value
 
     def potentials(self):
         a, b = np.empty(self.n ** 3), np.empty(self.n ** 3)

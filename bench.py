@@ -242,6 +242,7 @@ def bench_ours(args):
             for _ in range(args.warmup):
                 solver.solve(system, settings)
                 solver.forces(NUCLEI, SIGMA)
+                solver.density()  # the e2e readback path, warmed like the rest
         except ValueError:
             solver.close()
             return None

@@ -126,6 +126,29 @@ ks_status ks_state_potentials(const void* solver, double* v_nuc, double* v_h);  
 ks_status ks_state_orbitals(const void* solver, int spin, double* out);            /* count * n^3 */
 ks_status ks_profile_get(const void* solver, ks_profile* out);                     /* GpuSolver::profile */
 
+/* ---- readouts of the converged state (display and diagnostics; nothing is fed back into a solve) ---- */
+/* GpuSolver::sample_density (crates/qm-gpu/src/sample.rs:84-121): rho_up + rho_dn at count points (pts3[3*q + axis],
+   Bohr) by trilinear interpolation with the cell and fractions of qm::Grid::trilinear_cell (crates/qm/src/grid.rs:54-67,
+   resolved in f64) and the blend a(1 - t) + b t along x, then y, then z in f32; 0 outside [origin, origin + (n-1)h]^3
+   (NaN coordinates included); a grid point returns the stored f32 exactly. One launch and one readback per call with
+   count > 0; count = 0 does no GPU work. The point buffers grow to the largest request and are reused. */
+ks_status ks_sample_density(void* solver, const double* pts3, int count, float* out);
+/* Calls of ks_sample_density that reached the GPU, and the buffer sets it has allocated (the reuse witness:
+   sample.rs sampling_readbacks / sampling_buffer_allocations). */
+ks_status ks_sampling_counters(const void* solver, int* readbacks, int* allocations);
+/* GpuSolver::density_f32 (crates/qm-gpu/src/scf.rs:1776-1779): the interior of rho_up + rho_dn as stored (f32, n^3,
+   x fastest). */
+ks_status ks_state_density_f32(void* solver, float* rho);
+/* GpuSolver::copy_density_to_volume (crates/qm-gpu/src/scf.rs:1780-1797) with a headless device buffer in place of
+   the 3-D texture: writes the n^3 f32 image (x fastest, no padding) of rho_up + rho_dn to dense_dev on the solver's
+   device, enqueued on `stream` (a cudaStream_t; NULL = the solver's stream) after the solver's own work. Does not
+   wait. */
+ks_status ks_density_to_volume(void* solver, float* dense_dev, void* stream);
+/* GpuSolver::density_max (scf.rs:1831-1834): max of rho_up + rho_dn over the interior (one readback). */
+ks_status ks_density_max(void* solver, double* out);
+/* GpuSolver::spin_abs_integral (scf.rs:1836-1842): the integral of |rho_up - rho_dn| in electrons (one readback). */
+ks_status ks_spin_abs_integral(void* solver, double* out);
+
 /* ---- grid-kernel entry points (host f64 in / out; the kernels run on the solver's device in f32) ----
    One parity hook per hot-path kernel; each mirrors the reference kernel named beside it. */
 /* hamiltonian (crates/qm-gpu/src/shaders/stencil.wgsl:77-90): out_v = -1/2 lap psi_v + V psi_v for count vectors */

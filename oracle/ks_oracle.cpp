@@ -1046,4 +1046,30 @@ int ora_forces(const ora_state* st, const ora_nucleus* nuc, int nn, double sigma
     return 0;
 }
 
+// crates/qm/src/grid.rs:54-67 (trilinear_cell) and :74-86 (trilinear)
+void ora_trilinear(int n, double h, const double* f, const double* pts3, int count, double* out) {
+    const double origin = -((double)(n - 1) * h / 2.0);
+    for (int q = 0; q < count; ++q) {
+        int c[3];
+        double t[3];
+        bool inside = true;
+        for (int a = 0; a < 3 && inside; ++a) {
+            const double x = (pts3[3 * q + a] - origin) / h;
+            if (!(x >= 0.0 && x <= (double)(n - 1))) { inside = false; break; }
+            const double i0 = std::floor(x);
+            c[a] = (int)i0;
+            t[a] = x - i0;
+        }
+        if (!inside) { out[q] = 0.0; continue; }
+        auto at = [&](int di, int dj, int dk) {
+            const int a = c[0] + di, b = c[1] + dj, cc = c[2] + dk;
+            return (a < n && b < n && cc < n) ? f[(size_t)a + (size_t)n * ((size_t)b + (size_t)n * cc)] : 0.0;
+        };
+        auto lerp = [](double a, double b, double tt) { return a * (1.0 - tt) + b * tt; };
+        auto xl = [&](int dj, int dk) { return lerp(at(0, dj, dk), at(1, dj, dk), t[0]); };
+        auto yl = [&](int dk) { return lerp(xl(0, dk), xl(1, dk), t[1]); };
+        out[q] = lerp(yl(0), yl(1), t[2]);
+    }
+}
+
 }  // extern "C"

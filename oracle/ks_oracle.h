@@ -44,6 +44,11 @@ typedef struct {
    plateau midpoint of two tie-directed bisections, S Neumaier. Returns 0, or -1 on refused inputs. */
 int ora_fermi_dirac(const double* evals, int k, int n, double kt, double* f, double* mu, double* entropy);
 
+/* qm::Grid::trilinear (crates/qm/src/grid.rs:54-86) of an n^3 field f at count points (pts3, Bohr): the cell and
+   fractions of trilinear_cell, neighbours beyond an upper face read 0, blended a(1 - t) + b t along x, then y,
+   then z in f64; 0 outside [origin, origin + (n-1)h]^3 (NaN included). */
+void ora_trilinear(int n, double h, const double* f, const double* pts3, int count, double* out);
+
 /* thread count for the parallel loops (stencils, pointwise); sums stay sequential */
 void ora_set_threads(int n);
 

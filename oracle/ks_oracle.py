@@ -64,6 +64,7 @@ def lib():
         L.ora_state_orbitals.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
         L.ora_forces.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, dp]
         L.ora_state_occupations.argtypes = [ctypes.c_void_p, dp, dp]
+        L.ora_trilinear.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp, ctypes.c_int, dp]
         L.ora_fermi_dirac.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
         _lib = L
     return _lib
@@ -279,6 +280,14 @@ def scf(n, h, nuclei, n_up, n_dn, sigma=None, tol=1e-6, mixing=0.3, eig_tol=1e-6
     stats["electrons"] = list(st.electrons)
     stats["mu"] = list(st.mu)
     return (State(ptr, n) if ptr else None), stats
+
+
+def trilinear(n, h, f, points):
+    """qm::Grid::trilinear (crates/qm/src/grid.rs:54-86) of the n^3 field f at points (m, 3), f64."""
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 3))
+    out = np.empty(max(len(pts), 1))
+    lib().ora_trilinear(int(n), ctypes.c_double(h), _p(_f64(f, n ** 3)), _p(pts), len(pts), _p(out))
+    return out[:len(pts)]
 
 
 def fermi_dirac(evals, n, kt):

@@ -198,3 +198,43 @@ def test_fermi_dirac_known_answers(oracle):
         evals = -spread * rng.uniform(size=k)
         f, _, _ = oracle.fermi_dirac(evals, n, kt)
         assert abs(f.sum() - n) <= 1e-12 and ((f >= 0) & (f <= 1)).all()
+
+
+def _xorshift_uniforms(seed):
+    """A deterministic xorshift64* stream of uniforms in [0, 1) (the generator of the reference's sampling tests)."""
+    s = seed
+
+    def u():
+        nonlocal s
+        s ^= s >> 12
+        s ^= (s << 25) & 0xFFFFFFFFFFFFFFFF
+        s ^= s >> 27
+        return (((s * 0x2545F4914F6CDD1D) & 0xFFFFFFFFFFFFFFFF) >> 11) / float(1 << 53)
+    return u
+
+
+def test_trilinear_known_answers(oracle):
+    """trilinear_reproduces_a_linear_field_exactly_and_is_zero_outside (crates/qm/src/grid.rs:143-165): on the
+    9^3 grid of spacing 0.5 ([-2, 2]^3) a linear field is reproduced to 1e-13 at random points; grid points,
+    the 8 corners and a face centre return the stored value bitwise; points outside by a little or a lot, and
+    NaN, give 0."""
+    n, h = 9, 0.5
+    xs = -2.0 + h * np.arange(n)
+    z, y, x = np.meshgrid(xs, xs, xs, indexing="ij")
+    lin = lambda p: 1.0 + 2.0 * p[..., 0] - p[..., 1] + 3.0 * p[..., 2]
+    f = lin(np.stack([x, y, z], axis=-1)).reshape(-1)
+    u = _xorshift_uniforms(0x5EED0001)
+    pts = np.array([[-2.0 + 4.0 * u(), -2.0 + 4.0 * u(), -2.0 + 4.0 * u()] for _ in range(50)])
+    got = oracle.trilinear(n, h, f, pts)
+    assert np.max(np.abs(got - lin(pts))) <= 1e-13
+
+    def idx(i, j, k):
+        return i + n * (j + n * k)
+    nodes = [(0, 0, 0), (3, 5, 7), (8, 0, 0), (0, 8, 0), (0, 0, 8), (8, 8, 0), (8, 0, 8), (0, 8, 8), (8, 8, 8), (8, 4, 4), (4, 4, 4)]
+    pn = np.array([[xs[i], xs[j], xs[k]] for i, j, k in nodes])
+    gn = oracle.trilinear(n, h, f, pn)
+    for (i, j, k), v in zip(nodes, gn):
+        assert v == f[idx(i, j, k)]
+    outside = np.array([[2.0 + 1e-12, 0, 0], [-2.0 - 1e-12, 0, 0], [0, 2.5, 0], [0, -7.0, 0], [0, 0, 2.000001], [0, 0, -2.1],
+                        [3.0, 3.0, 3.0], [np.nan, 0, 0]])
+    assert np.all(oracle.trilinear(n, h, f, outside) == 0.0)
