@@ -196,6 +196,36 @@ ks_status ks_state_density(const void* solver, double* rho_up, double* rho_dn) {
     });
 }
 
+ks_status ks_set_ionic(void* solver, const ks_species* species, int n_species) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h) return KS_INVALID;
+    return guarded(h, [&] {
+        h->solver->set_ionic(species, n_species);
+        return KS_OK;
+    });
+}
+
+ks_status ks_apply_nonlocal(void* solver, const ks_nucleus* nuclei, int n_nuclei, int count, const double* x, double* out, double* c,
+                            int* rows) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h) return KS_INVALID;
+    if (!nuclei || !x || !out || !rows) return fail(h, KS_INVALID, "apply_nonlocal: nuclei, x, out and rows are required");
+    return guarded(h, [&] {
+        *rows = h->solver->apply_nonlocal(nuclei, n_nuclei, count, x, out, c);
+        return KS_OK;
+    });
+}
+
+ks_status ks_density_with_core_to_volume(void* solver, float* dense_dev, void* stream, double* max_out) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h || !dense_dev || !max_out) return KS_INVALID;
+    if (!h->solver->has_state()) return fail(h, KS_NO_STATE, "no converged state");
+    return guarded(h, [&] {
+        h->solver->density_to_volume(dense_dev, static_cast<cudaStream_t>(stream), true, max_out);
+        return KS_OK;
+    });
+}
+
 ks_status ks_sample_density(void* solver, const double* pts3, int count, float* out) {
     auto* h = static_cast<Handle*>(solver);
     if (!h) return KS_INVALID;

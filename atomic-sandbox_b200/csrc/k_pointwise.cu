@@ -286,10 +286,17 @@ __device__ __forceinline__ void lsda_point(double nu, double nd, double& e, doub
 
 __global__ void xc_veff_kernel(long long F, const float* __restrict__ up, const float* __restrict__ dn,
                                const float* __restrict__ vnuc, const float* __restrict__ vh, float* __restrict__ exc,
-                               float* __restrict__ vup, float* __restrict__ vdn, float* __restrict__ xcu, float* __restrict__ xcd) {
+                               float* __restrict__ vup, float* __restrict__ vdn, float* __restrict__ xcu, float* __restrict__ xcd,
+                               const float* __restrict__ pc) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < F; e += (long long)gridDim.x * blockDim.x) {
         double en, vu, vd;
-        lsda_point((double)up[e], (double)dn[e], en, vu, vd);
+        double nu = (double)up[e], nd = (double)dn[e];
+        if (pc) {  // the unpolarised partial core, half per spin (crates/qm/src/scf.rs:759-768)
+            const double c = 0.5 * (double)pc[e];
+            nu += c;
+            nd += c;
+        }
+        lsda_point(nu, nd, en, vu, vd);
         exc[e] = (float)en;
         if (vup) {
             double base = (double)vnuc[e] + (double)vh[e];
@@ -434,8 +441,8 @@ void launch_residual_precond(const Layout& L, int k, const float* HX, const floa
 }
 
 void launch_xc_veff(long long F, const float* up, const float* dn, const float* vnuc, const float* vh, float* exc, float* vup,
-                    float* vdn, float* vxc_up, float* vxc_dn, cudaStream_t s) {
-    xc_veff_kernel<<<stream_blocks(F), TPB, 0, s>>>(F, up, dn, vnuc, vh, exc, vup, vdn, vxc_up, vxc_dn);
+                    float* vdn, float* vxc_up, float* vxc_dn, cudaStream_t s, const float* pc) {
+    xc_veff_kernel<<<stream_blocks(F), TPB, 0, s>>>(F, up, dn, vnuc, vh, exc, vup, vdn, vxc_up, vxc_dn, pc);
     KS_LAUNCH_CHECK();
 }
 

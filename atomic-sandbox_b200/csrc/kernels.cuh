@@ -42,9 +42,10 @@ void launch_block_lincomb(long long F, int m, const float* S, int q, const doubl
 void launch_residual_precond(const Layout& L, int k, const float* HX, const float* X, const double* theta, const float* V,
                              const double* lambda, double diag_t, float* R, float* W0, double* partials, int blocks, cudaStream_t s);
 // XC (LSDA: Slater exchange + PW92, crates/qm/src/xc.rs:88-207) on (up, dn), f64 arithmetic, and the
-// effective potentials v_sigma = vnuc + vh + vxc_sigma. exc gets n*eps_xc.
+// effective potentials v_sigma = vnuc + vh + vxc_sigma. exc gets n*eps_xc. With a partial core pc, XC runs on
+// (up + pc/2, dn + pc/2).
 void launch_xc_veff(long long F, const float* up, const float* dn, const float* vnuc, const float* vh, float* exc, float* vup,
-                    float* vdn, float* vxc_up, float* vxc_dn, cudaStream_t s);
+                    float* vdn, float* vxc_up, float* vxc_dn, cudaStream_t s, const float* pc = nullptr);
 // rho_out = sum_i f_i psi_i^2 over k orbitals (f: device f64 or null = 1), r = rho_out - rho_in, and
 // partials [blocks][2] = (sum |rho_out - rho_in|, sum rho_out).
 void launch_density_residual(long long F, int k, const float* psi, const double* f, const float* rho_in, float* rho_out, float* r,

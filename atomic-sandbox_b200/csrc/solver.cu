@@ -574,6 +574,8 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         a.V = V;
         a.vec0 = vec0;
         launch_stencil(L_, in.tmap, count, a, out, lane.s);
+        // + V_NL under a pseudopotential setup (crates/qm-gpu/src/eigen.rs:216-227; the preconditioner stays local)
+        if (nl_on_) ionic_.apply_nl(L_, in.at(vec0), count, out, lane.nl, lane.s);
     };
     // --- guess: one readback of X^T X and <x_i, H x_i>; dependent columns are re-seeded
     std::vector<double> theta(k), lambda(k);
@@ -786,7 +788,9 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
     if (fd && opt_.n_extra < 1) { error = "Fermi-Dirac needs n_extra >= 1 levels above N_sigma per channel (ks_options)"; return KS_INVALID; }
     if (fd && std::max(n_up, n_dn) + opt_.n_extra > 64) { error = "Fermi-Dirac: at most 64 levels per channel"; return KS_INVALID; }
     if (nn > 32) { error = "at most 32 nuclei"; return KS_INVALID; }
-    // E_nn (crates/qm/src/nuclear.rs:277-289)
+    const bool ionic = ionic_.active();
+    // E_nn (crates/qm/src/nuclear.rs:277-289); under a setup the valence charges (ionic_repulsion, :368-378)
+    auto charge = [&](int a) { return ionic ? ionic_.charge_of(nuc[a].z) : (double)nuc[a].z; };
     double e_nn = 0.0;
     for (int i = 0; i < nn; ++i)
         for (int j = i + 1; j < nn; ++j) {
@@ -797,13 +801,14 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 converged_ = false;
                 return KS_COINCIDENT_NUCLEI;
             }
-            e_nn += (double)nuc[i].z * (double)nuc[j].z / d;
+            e_nn += charge(i) * charge(j) / d;
         }
+    // under a setup each centre carries its charge q (Z_v or Z): the cold guess deposits q (nuclear.rs:195-206)
     std::vector<Nuc> hn(std::max(nn, 1));
     double z_tot = 0.0;
     for (int i = 0; i < nn; ++i) {
-        hn[i] = Nuc{nuc[i].pos[0], nuc[i].pos[1], nuc[i].pos[2], (double)nuc[i].z};
-        z_tot += nuc[i].z;
+        hn[i] = Nuc{nuc[i].pos[0], nuc[i].pos[1], nuc[i].pos[2], charge(i)};
+        z_tot += charge(i);
     }
     try {
         nuc_d_.alloc(hn.size() * sizeof(Nuc));
@@ -815,7 +820,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         int kk[2];
         for (int sp = 0; sp < 2; ++sp) kk[sp] = nocc[sp] > 0 ? nocc[sp] + opt_.n_extra : 0;
         const bool reuse = warm && have_warm_ && fd_state_ == fd && nocc_[0] == n_up && nocc_[1] == n_dn && ch_[0].k == kk[0] &&
-                           ch_[1].k == kk[1];
+                           ch_[1].k == kk[1] && state_gen_ == ionic_gen();
         // columns held to the eigen tolerance: N_sigma, or under Fermi-Dirac the block minus its loose tail (set each step)
         int tight[2] = {nocc[0], nocc[1]};
         double entropy = 0.0, mu[2] = {NAN, NAN};
@@ -846,7 +851,22 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         }
         nocc_[0] = n_up;
         nocc_[1] = n_dn;
-        launch_nuclear_potential(L_, dnuc, nn, s.sigma, vnuc_.at(0), s_);
+        const float* pc = nullptr;
+        nl_on_ = false;
+        if (ionic) {
+            // V_loc = sum V_LR + sum V_SR, the partial core, the projector spheres (crates/qm/src/scf.rs:720-745)
+            ionic_.update(L_, nuc, nn, s.sigma, s_);
+            ionic_.local_potential(L_, vnuc_.at(0), s_);
+            if (ionic_.has_core()) {
+                if (pc_.count == 0) pc_.create(L_, 1);
+                ionic_.partial_core(L_, pc_.at(0), s_);
+                pc = pc_.at(0);
+            }
+            nl_on_ = ionic_.has_nl();
+        } else {
+            launch_nuclear_potential(L_, dnuc, nn, s.sigma, vnuc_.at(0), s_);
+        }
+        state_gen_ = ionic_gen();
         if (!reuse) KS_CUDA(cudaStreamSynchronize(s_));
         profile.start_s = reuse ? 0.0 : secs(t_start);
 
@@ -924,7 +944,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             if (ps.stop == 3) ++out->n_warnings;
             // XC and the effective potentials
             launch_xc_veff(L_.F, in_up_.at(0), in_dn_.at(0), vnuc_.at(0), vh_.at(0), exc_.at(0), v_up_.at(0), v_dn_.at(0), nullptr,
-                           nullptr, s_);
+                           nullptr, s_, pc);
             // eigensolves
             int eig_its = 0;
             last_step_res = 0.0;
@@ -1145,7 +1165,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         profile.poisson_iterations += ps.iterations;
         out->poisson_residual = std::max(out->poisson_residual, ps.residual);
         out->poisson_iterations = std::max(out->poisson_iterations, ps.iterations);
-        launch_xc_veff(L_.F, out_up_.at(0), out_dn_.at(0), vnuc_.at(0), vh_.at(0), exc_.at(0), nullptr, nullptr, nullptr, nullptr, s_);
+        launch_xc_veff(L_.F, out_up_.at(0), out_dn_.at(0), vnuc_.at(0), vh_.at(0), exc_.at(0), nullptr, nullptr, nullptr, nullptr, s_, pc);
         std::vector<std::pair<const float*, const float*>> pairs = {
             {rho_tot_.at(0), vnuc_.at(0)}, {rho_tot_.at(0), vh_.at(0)}, {exc_.at(0), ones_.at(0)}};
         std::vector<double> kin_w;  // the occupation of each orbital pair after the first three entries
@@ -1173,11 +1193,30 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             kinetic = t;
         }
         kinetic += comp;
+        const double h_ext = h[0], h_har = h[1], h_xc = h[2], h_bnd = h[nvals];
+        // E_NL = sum_sigma sum_i f_i sum_rows E_KB c^2 (crates/qm/src/nonlocal.rs, f64 finish; one readback per spin)
+        double e_nl = 0.0, e_nl_c = 0.0;
+        if (nl_on_)
+            for (int sp = 0; sp < 2; ++sp) {
+                if (nocc[sp] == 0) continue;
+                const int cols = fd ? kk[sp] : nocc[sp];
+                std::vector<double> c;
+                ionic_.project(L_, ch_[sp].X(), cols, nl_sc_, s_, c);
+                const int R = ionic_.rows();
+                for (int i = 0; i < cols; ++i)
+                    for (int r = 0; r < R; ++r) {
+                        const double x = occ_[sp][i] * ionic_.row_ekb()[r] * c[(size_t)i * R + r] * c[(size_t)i * R + r];
+                        const double t = e_nl + x;
+                        if (std::fabs(e_nl) >= std::fabs(x)) e_nl_c += (e_nl - t) + x; else e_nl_c += (x - t) + e_nl;
+                        e_nl = t;
+                    }
+            }
+        e_nl += e_nl_c;
         ks_energy& en = out->energy;
         en.kinetic = kinetic;
-        en.external_ = h[0];
-        en.hartree = 0.5 * h[1];
-        en.xc = h[2];
+        en.external_ = h_ext + e_nl;
+        en.hartree = 0.5 * h_har;
+        en.xc = h_xc;
         en.nuclear = e_nn;
         en.internal = en.kinetic + en.external_ + en.hartree + en.xc + en.nuclear;
         en.ts = fd ? s.kt * entropy : 0.0;  // F = E - kT S (crates/qm/src/scf.rs:1015-1018)
@@ -1186,7 +1225,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         out->mu[0] = mu[0];
         out->mu[1] = mu[1];
         out->partial = partial ? 1 : 0;
-        out->boundary_density = h[nvals];
+        out->boundary_density = h_bnd;
         out->electrons[0] = q_out[0];
         out->electrons[1] = q_out[1];
         if (out->boundary_density > BOUNDARY_DENSITY_WARN) ++out->n_warnings;
@@ -1215,6 +1254,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
 ks_status Solver::forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n) {
     if (!converged_) { error = "no converged state"; return KS_NO_STATE; }
     if (nn <= 0 || nn > 32 || !nuc || !out3n) { error = "invalid arguments"; return KS_INVALID; }
+    if (state_gen_ != 0) return ionic_forces(nuc, nn, sigma, out3n);
     try {
         std::vector<Nuc> hn(nn);
         for (int i = 0; i < nn; ++i) hn[i] = Nuc{nuc[i].pos[0], nuc[i].pos[1], nuc[i].pos[2], (double)nuc[i].z};
@@ -1250,7 +1290,74 @@ ks_status Solver::forces(const ks_nucleus* nuc, int nn, double sigma, double* ou
     }
 }
 
+// Forces of a state solved under a pseudopotential setup (crates/qm/src/forces.rs, pseudised ions; the GPU form
+// crates/qm-gpu/src/ionic.rs "Forces"): F_I = -dE/dR_I at frozen orbitals and occupations, five terms:
+//   local long range    integral rho V_LR,I'(d) (r - R_I)/d            (every centre, its own charge and width)
+//   local short range   integral rho V_SR,I'(d) (r - R_I)/d            (pseudised, within r_sr)
+//   partial core        integral vbar rho_pc,I'(d) (r - R_I)/d          (vbar = (v_xc,up + v_xc,dn)/2 on rho + rho_pc/2)
+//   nonlocal            sum_{sigma,i} 2 f_i sum_{rows of I} E_KB c <grad beta | psi_i>
+//   ion-ion             sum_J q_I q_J (R_I - R_J)/|R_I - R_J|^3          (valence charges)
+ks_status Solver::ionic_forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n) {
+    if (state_gen_ != ionic_gen()) { error = "the ionic setup changed after the solve"; return KS_INVALID; }
+    try {
+        ionic_.update(L_, nuc, nn, sigma, s_);
+        total_density();
+        const float* xu = nullptr;
+        const float* xd = nullptr;
+        if (ionic_.has_core()) {
+            if (pc_.count == 0) pc_.create(L_, 1);
+            if (xcu_.count == 0) { xcu_.create(L_, 1); xcd_.create(L_, 1); }
+            ionic_.partial_core(L_, pc_.at(0), s_);
+            launch_xc_veff(L_.F, out_up_.at(0), out_dn_.at(0), vnuc_.at(0), vh_.at(0), exc_.at(0), nullptr, nullptr, xcu_.at(0), xcd_.at(0),
+                           s_, pc_.at(0));
+            xu = xcu_.at(0);
+            xd = xcd_.at(0);
+        }
+        launch_local_forces(L_, ionic_.centres(), ionic_.n_centres(), ionic_.species_dev(), rho_tot_.at(0), xu, xd, red_.partials(),
+                            red_.blocks(), s_);
+        launch_finish(red_.partials(), red_.blocks(), 3 * nn, L_.h * L_.h * L_.h, red_.res(), s_);
+        const double* h = red_.read(3 * nn);
+        for (int i = 0; i < 3 * nn; ++i) out3n[i] = h[i];
+        if (ionic_.has_nl()) {
+            const int R = ionic_.rows();
+            for (int sp = 0; sp < 2; ++sp) {
+                if (nocc_[sp] == 0) continue;
+                const int cols = count(sp);
+                std::vector<double> g;
+                ionic_.nl_force_sums(L_, ch_[sp].X(), cols, nl_sc_, s_, g);
+                for (int i = 0; i < cols; ++i)
+                    for (int r = 0; r < R; ++r) {
+                        const double* q = &g[((size_t)i * R + r) * 4];
+                        const double w = 2.0 * occ_[sp][i] * ionic_.row_ekb()[r] * q[3];
+                        const int a = ionic_.row_ion()[r];
+                        for (int c = 0; c < 3; ++c) out3n[3 * a + c] += w * q[c];
+                    }
+            }
+        }
+        for (int a = 0; a < nn; ++a)
+            for (int b = 0; b < nn; ++b) {
+                if (a == b) continue;
+                double dv[3] = {nuc[a].pos[0] - nuc[b].pos[0], nuc[a].pos[1] - nuc[b].pos[1], nuc[a].pos[2] - nuc[b].pos[2]};
+                double d = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+                if (d < 1e-8) {
+                    error = "nuclei " + std::to_string(std::min(a, b)) + " and " + std::to_string(std::max(a, b)) + " coincide";
+                    return KS_COINCIDENT_NUCLEI;
+                }
+                const double sc = ionic_.charge_of(nuc[a].z) * ionic_.charge_of(nuc[b].z) / (d * d * d);
+                for (int c = 0; c < 3; ++c) out3n[3 * a + c] += sc * dv[c];
+            }
+        return KS_OK;
+    } catch (const DeviceError& e) {
+        error = e.what();
+        return KS_DEVICE;
+    } catch (const std::invalid_argument& e) {
+        error = e.what();
+        return KS_INVALID;
+    }
+}
+
 ks_status Solver::vjp(const ks_nucleus* nuc, int nn, double sigma, double e_bar, double* dE_dR3n, double* dE_dsigma) {
+    if (state_gen_ != 0) { error = "vjp: all-electron states only (no pseudopotential terms)"; return KS_INVALID; }
     if (!converged_) { error = "no converged state"; return KS_NO_STATE; }
     if (nn <= 0 || nn > 32 || !nuc || !dE_dR3n || !dE_dsigma || !(sigma > 0) || !std::isfinite(e_bar)) {
         error = "invalid arguments";
@@ -1332,8 +1439,10 @@ void Solver::density_f32(float* host_n3) {
 
 // crates/qm-gpu/src/scf.rs:1780-1797: the dense n^3 image of the density on the device, enqueued on
 // `s` after the solver's own work; does not wait. (A headless buffer in place of the texture.)
-void Solver::density_to_volume(float* dense_dev, cudaStream_t s) {
+void Solver::density_to_volume(float* dense_dev, cudaStream_t s, bool with_core, double* max_out) {
     total_density();
+    // the partial core of the state's setup and geometry (crates/qm-gpu/src/scf.rs:1798-1829); none: the plain density
+    const float* core = (with_core && state_gen_ != 0 && state_gen_ == ionic_gen() && ionic_.has_core() && pc_.count > 0) ? pc_.at(0) : nullptr;
     if (s && s != s_) {
         cudaEvent_t ev;
         KS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -1341,8 +1450,8 @@ void Solver::density_to_volume(float* dense_dev, cudaStream_t s) {
         KS_CUDA(cudaStreamWaitEvent(s, ev, 0));
         KS_CUDA(cudaEventDestroy(ev));
     }
-    // the per-block maxima land in the reducer's partials, unread; the stream joins keep them ordered
-    launch_volume(L_, rho_tot_.at(0), nullptr, dense_dev, red_.partials(), red_.blocks(), s ? s : s_);
+    // the per-block maxima land in the reducer's partials; the stream joins keep them ordered
+    launch_volume(L_, rho_tot_.at(0), core, dense_dev, red_.partials(), red_.blocks(), s ? s : s_);
     if (s && s != s_) {
         // the solver's stream must not reuse rho_tot_ or the partials before the copy is done
         cudaEvent_t ev;
@@ -1351,6 +1460,33 @@ void Solver::density_to_volume(float* dense_dev, cudaStream_t s) {
         KS_CUDA(cudaStreamWaitEvent(s_, ev, 0));
         KS_CUDA(cudaEventDestroy(ev));
     }
+    if (max_out) {
+        launch_finish_max(red_.partials(), red_.blocks(), red_.res(), s_);
+        *max_out = red_.read(1)[0];
+    }
+}
+
+int Solver::apply_nonlocal(const ks_nucleus* nuc, int nn, int count, const double* x, double* out, double* c) {
+    if (!ionic_.active()) throw std::invalid_argument("apply_nonlocal: no ionic setup (ks_set_ionic)");
+    if (nn < 1 || nn > MAX_CENTRES || count < 1) throw std::invalid_argument("apply_nonlocal: 1..32 nuclei, count >= 1");
+    ionic_.update(L_, nuc, nn, L_.h, s_);
+    Block in, res;
+    in.create(L_, count);
+    res.create(L_, count);
+    DevBuf tmp((size_t)L_.interior() * count * sizeof(double));
+    KS_CUDA(cudaMemcpyAsync(tmp.p, x, (size_t)L_.interior() * count * sizeof(double), cudaMemcpyHostToDevice, s_));
+    launch_pack(L_, count, tmp.d(), in.at(0), s_);
+    launch_fill(res.at(0), 0.0f, L_.F * count, s_);
+    ionic_.apply_nl(L_, in.at(0), count, res.at(0), nl_sc_, s_);
+    if (c) {
+        std::vector<double> cc;
+        ionic_.project(L_, in.at(0), count, nl_sc_, s_, cc);
+        std::copy(cc.begin(), cc.end(), c);
+    }
+    launch_unpack(L_, count, res.at(0), tmp.d(), s_);
+    KS_CUDA(cudaMemcpyAsync(out, tmp.p, (size_t)L_.interior() * count * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    KS_CUDA(cudaStreamSynchronize(s_));
+    return ionic_.rows();
 }
 
 // crates/qm-gpu/src/scf.rs:1831-1834: max rho over the interior (one readback)

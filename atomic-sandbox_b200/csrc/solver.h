@@ -5,6 +5,7 @@
 #include <vector>
 #include "common.cuh"
 #include "kernels.cuh"
+#include "ionic.cuh"
 #include "../../include/ks_cuda.h"
 
 namespace ks {
@@ -74,6 +75,60 @@ public:
     ~Reducer();
 };
 
+// The ionic setup of a solver (crates/qm/src/ionic.rs IonicSetup, its tables from ks_species) and the
+// terms of the current geometry: centres, projector spheres and their beta values on the device.
+class Ionic {
+public:
+    struct Scratch {
+        DevBuf partials, coef;
+        size_t cap = 0;
+    };
+    void set(const ks_species* sp, int nsp);  // throws std::invalid_argument on a bad table
+    bool active() const { return !species_.empty(); }
+    int generation() const { return gen_; }
+    int species_of(int z) const;              // index, or -1 for an all-electron species
+    double charge_of(int z) const;            // z_v when pseudised, else z
+    void update(const Layout& L, const ks_nucleus* nuc, int nn, double sigma_ae, cudaStream_t s);
+    bool has_core() const { return has_core_; }
+    bool has_nl() const { return !sph_h_.empty(); }
+    int rows() const { return rows_total_; }
+    const std::vector<double>& row_ekb() const { return row_ekb_; }
+    const std::vector<int>& row_ion() const { return row_ion_; }
+    const IonicCentre* centres() const { return static_cast<const IonicCentre*>(centres_.p); }
+    int n_centres() const { return (int)centres_h_.size(); }
+    const IonicSpeciesDev* species_dev() const { return static_cast<const IonicSpeciesDev*>(species_dev_.p); }
+    void local_potential(const Layout& L, float* out, cudaStream_t s) const;
+    void partial_core(const Layout& L, float* out, cudaStream_t s) const;
+    // out_v += V_NL x_v, v < count (blocks of stride F)
+    void apply_nl(const Layout& L, const float* x, int count, float* out, Scratch& sc, cudaStream_t s) const;
+    // c[v * rows + row] = h^3 <beta_row, x_v> (synchronises s)
+    void project(const Layout& L, const float* x, int count, Scratch& sc, cudaStream_t s, std::vector<double>& c) const;
+    // [(v * rows + row) * 4 + {x, y, z, beta}] = h^3 <(grad beta_row, beta_row), psi_v> (synchronises s)
+    void nl_force_sums(const Layout& L, const float* psi, int count, Scratch& sc, cudaStream_t s, std::vector<double>& sums) const;
+
+private:
+    void ensure(Scratch& sc, int count) const;
+    struct Proj { int l; double e_kb, radius; std::vector<double> t; };
+    struct Species {
+        int z;
+        double z_v, sigma_lr, du, r_sr, pc_radius;
+        std::vector<double> v_sr, rho_pc;
+        std::vector<Proj> proj;
+    };
+    std::vector<Species> species_;
+    std::vector<size_t> off_v_sr_, off_pc_;
+    std::vector<std::vector<size_t>> off_t_;
+    DevBuf tables_, species_dev_, centres_, spheres_, chunk_sphere_, beta_;
+    std::vector<IonicCentre> centres_h_;
+    std::vector<Sphere> sph_h_;
+    std::vector<int> chunk_sphere_h_, row_ion_;
+    std::vector<double> row_ekb_;
+    int rows_total_ = 0, total_chunks_ = 0, max_pts_ = 0;
+    int ubox_[6] = {0, 0, 0, 0, 0, 0};
+    int gen_ = 0;
+    bool has_core_ = false;
+};
+
 struct PoissonStats { int iterations = 0; double residual = 0; int stop = 0; int readbacks = 0; };
 
 // Multigrid-preconditioned CG Hartree solve (crates/qm-gpu/src/poisson.rs:111-343).
@@ -131,6 +186,7 @@ struct Lane {
     double* up = nullptr;
     size_t up_cap = 0;
     double dense_s = 0;  // host time in the Rayleigh-Ritz algebra (profile)
+    Ionic::Scratch nl;   // the nonlocal operator's projections on this lane's stream
     Lane() = default;
     Lane(const Lane&) = delete;
     Lane& operator=(const Lane&) = delete;
@@ -149,6 +205,8 @@ public:
                     void* user, ks_stats* out);
     ks_status forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n);
     ks_status vjp(const ks_nucleus* nuc, int nn, double sigma, double e_bar, double* dE_dR3n, double* dE_dsigma);
+    // the ionic setup of the next solves (n = 0: all-electron); throws std::invalid_argument on bad tables
+    void set_ionic(const ks_species* sp, int n) { ionic_.set(sp, n); }
     EigenStats lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked);
     Lane& lane(int i) { return *lane_[i]; }
     std::string error;
@@ -165,7 +223,9 @@ public:
     // readouts of the converged state (crates/qm-gpu/src/sample.rs, scf.rs:1776-1842)
     void sample_density(const double* pts3, int count, float* out);
     void density_f32(float* host_n3);
-    void density_to_volume(float* dense_dev, cudaStream_t s);
+    void density_to_volume(float* dense_dev, cudaStream_t s, bool with_core = false, double* max_out = nullptr);
+    // out_v = V_NL x_v of the ionic setup at nuc (host f64 n^3 each); c = projections; returns the row count
+    int apply_nonlocal(const ks_nucleus* nuc, int nn, int count, const double* x, double* out, double* c);
     double density_max();
     double spin_abs_integral();
     int sampling_readbacks = 0, sampling_allocations = 0;
@@ -190,6 +250,13 @@ private:
     std::vector<Entry> diis_pool_;
     DevBuf nuc_d_;
     DevBuf sample_pts_, sample_out_, volume_;  // grow-only readout buffers
+    Ionic ionic_;                              // the pseudopotential setup (inactive: all-electron)
+    Ionic::Scratch nl_sc_;                     // projections on the solver's stream (energy, forces)
+    Block pc_, xcu_, xcd_;                     // partial core of the geometry; v_xc scratch of the forces
+    bool nl_on_ = false;                       // H psi includes V_NL (inside a solve under a setup)
+    int state_gen_ = 0;                        // ionic generation the state was solved under (0: all-electron)
+    int ionic_gen() const { return ionic_.active() ? ionic_.generation() : 0; }
+    ks_status ionic_forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n);
     size_t sample_cap_ = 0;
     void total_density();                      // rho_tot_ = rho_up + rho_dn (f32) of the state
     bool converged_ = false;

@@ -59,6 +59,74 @@ class _Profile(ctypes.Structure):
 
 ABORT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
 
+
+@dataclasses.dataclass
+class Projector:
+    """One Kleinman-Bylander projector of a pseudised species: angular momentum l <= 2, E_KB (Ha), the radius of
+    its ball (Bohr) and its radial table t_l(k du) (crates/qm/src/radial/filter.rs:323 FilteredProjector)."""
+    l: int
+    e_kb: float
+    radius: float
+    t: np.ndarray
+
+
+@dataclasses.dataclass
+class Species:
+    """One pseudised species as the grid samples it (crates/qm/src/radial/filter.rs:330-363 FilteredTable): valence
+    charge, width of the long-range erf part, the uniform-table spacing du and the V_SR / rho_pc / projector tables
+    (even functions at d = k du, read by 4-point Lagrange, 0 beyond their radius). pc_radius <= 0: no partial core."""
+    z: int
+    z_v: float
+    sigma_lr: float
+    du: float
+    v_sr: np.ndarray
+    r_sr: float
+    rho_pc: np.ndarray = None
+    pc_radius: float = 0.0
+    projectors: list = dataclasses.field(default_factory=list)
+
+
+class SpeciesStruct(ctypes.Structure):
+    """ks_species (include/ks_cuda.h); the oracle's ora_species has the same layout."""
+    _fields_ = [("z", ctypes.c_int), ("z_v", ctypes.c_double), ("sigma_lr", ctypes.c_double), ("du", ctypes.c_double),
+                ("v_sr", ctypes.POINTER(ctypes.c_double)), ("n_v_sr", ctypes.c_int), ("r_sr", ctypes.c_double),
+                ("rho_pc", ctypes.POINTER(ctypes.c_double)), ("n_rho_pc", ctypes.c_int), ("pc_radius", ctypes.c_double),
+                ("n_proj", ctypes.c_int), ("proj_l", ctypes.POINTER(ctypes.c_int)), ("proj_e_kb", ctypes.POINTER(ctypes.c_double)),
+                ("proj_radius", ctypes.POINTER(ctypes.c_double)), ("proj_t", ctypes.POINTER(ctypes.POINTER(ctypes.c_double))),
+                ("proj_n", ctypes.POINTER(ctypes.c_int))]
+
+
+def species_array(species):
+    """(ctypes array of SpeciesStruct, keep-alive list) for a list of Species."""
+    keep = []
+
+    def dptr(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size
+
+    arr = (SpeciesStruct * max(len(species), 1))()
+    for i, sp in enumerate(species):
+        st = arr[i]
+        st.z, st.z_v, st.sigma_lr, st.du = int(sp.z), float(sp.z_v), float(sp.sigma_lr), float(sp.du)
+        st.v_sr, st.n_v_sr = dptr(sp.v_sr if sp.v_sr is not None else np.zeros(0))
+        st.r_sr = float(sp.r_sr)
+        st.rho_pc, st.n_rho_pc = dptr(sp.rho_pc if sp.rho_pc is not None else np.zeros(0))
+        st.pc_radius = float(sp.pc_radius)
+        k = len(sp.projectors)
+        st.n_proj = k
+        ls = (ctypes.c_int * max(k, 1))(*[p.l for p in sp.projectors])
+        ek = (ctypes.c_double * max(k, 1))(*[p.e_kb for p in sp.projectors])
+        rr = (ctypes.c_double * max(k, 1))(*[p.radius for p in sp.projectors])
+        tp = (ctypes.POINTER(ctypes.c_double) * max(k, 1))()
+        tn = (ctypes.c_int * max(k, 1))()
+        for j, p in enumerate(sp.projectors):
+            tp[j], tn[j] = dptr(p.t)
+        keep += [ls, ek, rr, tp, tn]
+        st.proj_l, st.proj_e_kb, st.proj_radius = ls, ek, rr
+        st.proj_t, st.proj_n = tp, tn
+    return arr, keep
+
 KS_OK, KS_COINCIDENT_NUCLEI, KS_NOT_CONVERGED, KS_STALLED, KS_NUMERICAL, KS_DEVICE, KS_INVALID, KS_ABORTED, KS_NO_STATE = range(9)
 
 
@@ -103,7 +171,8 @@ EXPORTED = [
     "ks_apply_laplacian", "ks_apply_precond", "ks_xc_lsda", "ks_nuclear_potential", "ks_poisson_solve", "ks_gram", "ks_lobpcg",
     "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
     "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations", "ks_sample_density", "ks_sampling_counters",
-    "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral",
+    "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
+    "ks_apply_nonlocal", "ks_density_with_core_to_volume",
 ]
 
 
@@ -166,6 +235,9 @@ def lib():
         L.ks_density_to_volume.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.ks_density_max.argtypes = [ctypes.c_void_p, dp]
         L.ks_spin_abs_integral.argtypes = [ctypes.c_void_p, dp]
+        L.ks_set_ionic.argtypes = [ctypes.c_void_p, ctypes.POINTER(SpeciesStruct), ctypes.c_int]
+        L.ks_apply_nonlocal.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, dp, dp, dp, ip]
+        L.ks_density_with_core_to_volume.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, dp]
         _lib = L
     return _lib
 
@@ -326,6 +398,29 @@ class GpuSolver:
         up, dn = np.empty(self.n ** 3), np.empty(self.n ** 3)
         _check(lib().ks_state_density(self._h, _p(up), _p(dn)), self._h)
         return up, dn
+
+    def set_ionic(self, species):
+        """The ionic setup of the next solves (ks_set_ionic): a list of Species (pseudised Z), [] = all-electron."""
+        arr, keep = species_array(list(species))
+        _check(lib().ks_set_ionic(self._h, arr, len(species)), self._h)
+
+    def apply_nonlocal(self, nuclei, x):
+        """(V_NL x for each row of x (count, n^3), projections c (count, rows)) under the ionic setup at nuclei."""
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1, self.n ** 3))
+        out = np.empty_like(x)
+        c = np.empty(len(x) * 640)
+        rows = ctypes.c_int()
+        _check(lib().ks_apply_nonlocal(self._h, nuclei_array(nuclei), len(nuclei), len(x), _p(x), _p(out), _p(c), ctypes.byref(rows)),
+               self._h)
+        return out, c[:len(x) * rows.value].reshape(len(x), rows.value)
+
+    def copy_density_with_core_to_volume(self, dense_dev_ptr, stream=None):
+        """The n^3 f32 image of rho + rho_pc (the plain density without a partial core) on a device buffer, ordered after
+        the solver's work on `stream`; returns the maximum of the field written."""
+        m = ctypes.c_double()
+        _check(lib().ks_density_with_core_to_volume(self._h, ctypes.c_void_p(int(dense_dev_ptr)), ctypes.c_void_p(stream or 0),
+                                                    ctypes.byref(m)), self._h)
+        return m.value
 
     # ---- readouts (crates/qm-gpu/src/sample.rs, crates/qm-gpu/src/scf.rs:1776-1842)
     def sample_density(self, points):

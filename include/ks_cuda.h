@@ -94,6 +94,43 @@ typedef int (*ks_abort_fn)(void* user);
 void* ks_solver_create(int n, double h, const ks_options* opts);
 void ks_solver_destroy(void* solver);
 
+/* One pseudised species: what the grid samples of the reference's qm::radial::filter::FilteredTable
+   (crates/qm/src/radial/filter.rs:323-363) for one element at this grid's h. Every table is an even function
+   tabulated at d = k du, k = 0 .. n-1 (the reference's du = h / 256), read by 4-point Lagrange with index -1
+   mirrored onto 1 and 0 beyond its radius (filter.rs:302-317). The caller keeps the arrays; ks_set_ionic copies them.
+     V_LR(d)  = -z_v erf(d / (sigma_lr sqrt2)) / d           (analytic; every pseudised centre)
+     V_SR(d)  = v_sr table within r_sr                         (n_v_sr = 0: none)
+     rho_pc   = rho_pc table within pc_radius                 (pc_radius <= 0: no partial core)
+     beta_lm  = t_l(d) sqrt((2l+1)/4pi) R_lm(d - R)           (projector i: l <= 2, E_KB, radius, table t) */
+typedef struct {
+    int z;                       /* nuclei of this atomic number are pseudised */
+    double z_v;                  /* valence charge */
+    double sigma_lr;             /* width of the long-range part (the reference uses 2h) */
+    double du;                   /* table spacing (Bohr) */
+    const double* v_sr; int n_v_sr; double r_sr;
+    const double* rho_pc; int n_rho_pc; double pc_radius;
+    int n_proj;                  /* at most 4 */
+    const int* proj_l; const double* proj_e_kb; const double* proj_radius;
+    const double* const* proj_t; const int* proj_n;
+} ks_species;
+
+/* The ionic setup of the solver's next solves (qm::ionic::IonicSetup, crates/qm/src/ionic.rs:56-63, its tables given
+   as above): nuclei whose Z is listed are pseudised, every other nucleus stays an all-electron smeared charge of width
+   settings.sigma. n_species = 0 restores the all-electron solver. Under a setup (crates/qm/src/scf.rs:114-140):
+   V_ext is V_loc = sum V_LR + sum V_SR; every H psi adds the Kleinman-Bylander V_NL = sum E_KB |beta><beta| (the
+   Jacobi preconditioner stays local); XC runs on (rho_up + rho_pc/2, rho_dn + rho_pc/2); energy.external_ =
+   integral rho V_loc + E_NL; energy.nuclear is the repulsion of the valence charges; the cold guess deposits each
+   centre's charge. n_up / n_dn passed to ks_solve count the valence electrons. A converged state from another setup
+   is never reused as a warm start. At most 8 species, 4 projectors each (l <= 2), 32 nuclei. */
+ks_status ks_set_ionic(void* solver, const ks_species* species, int n_species);
+
+/* The Kleinman-Bylander operator of the solver's ionic setup at these nuclei (the GPU's proj_dot / proj_finish /
+   proj_axpy, crates/qm-gpu/src/ionic.rs; qm::nonlocal::NonlocalOp::apply_add): out_v = V_NL x_v for count host
+   vectors (n^3 each, f64 in and out, f32 on the device), and, when c is not NULL, the projections
+   c[v * rows + row] = h^3 <beta_row, x_v> in sphere order (ion, projector, m = -l..l). *rows gets the row count. */
+ks_status ks_apply_nonlocal(void* solver, const ks_nucleus* nuclei, int n_nuclei, int count, const double* x, double* out, double* c,
+                            int* rows);
+
 /* GpuSolver::solve / solve_with (crates/qm-gpu/src/scf.rs:1195-1235): n_up / n_dn electrons per spin,
    warm != 0 reuses the last converged state when its counts match. abort may be NULL. */
 ks_status ks_solve(void* solver, const ks_nucleus* nuclei, int n_nuclei, int n_up, int n_dn, const ks_settings* settings,
@@ -144,6 +181,10 @@ ks_status ks_state_density_f32(void* solver, float* rho);
    device, enqueued on `stream` (a cudaStream_t; NULL = the solver's stream) after the solver's own work. Does not
    wait. */
 ks_status ks_density_to_volume(void* solver, float* dense_dev, void* stream);
+/* GpuSolver::copy_density_with_core_to_volume (crates/qm-gpu/src/scf.rs:1798-1829): as ks_density_to_volume for
+   rho_up + rho_dn + rho_pc, the model partial core of a state solved under an ionic setup (the plain density when
+   there is none); *max_out gets the maximum of the field written (one readback). */
+ks_status ks_density_with_core_to_volume(void* solver, float* dense_dev, void* stream, double* max_out);
 /* GpuSolver::density_max (scf.rs:1831-1834): max of rho_up + rho_dn over the interior (one readback). */
 ks_status ks_density_max(void* solver, double* out);
 /* GpuSolver::spin_abs_integral (scf.rs:1836-1842): the integral of |rho_up - rho_dn| in electrons (one readback). */

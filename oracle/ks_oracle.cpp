@@ -439,6 +439,209 @@ double jacobi_omega() {
     return 4.0 / (3.0 * rho);
 }
 
+// ---------------------------------------------------------------- pseudised ions (ionic.rs, nonlocal.rs)
+// An ionic setup restated from the tables a caller passes (the reference's FilteredTable as the grid
+// samples it, crates/qm/src/radial/filter.rs:323-363).
+struct OraIonic {
+    struct Proj { int l; double e_kb, radius; Vec t; };
+    struct Sp { int z; double z_v, sigma_lr, du, r_sr, pc_radius; Vec v_sr, rho_pc; std::vector<Proj> proj; };
+    std::vector<Sp> sp;
+    int find(int z) const {
+        for (size_t i = 0; i < sp.size(); ++i) if (sp[i].z == z) return (int)i;
+        return -1;
+    }
+    double charge(int z) const { int i = find(z); return i < 0 ? (double)z : sp[i].z_v; }
+};
+
+OraIonic make_ionic(const ora_species* s, int nsp) {
+    OraIonic io;
+    for (int i = 0; i < nsp; ++i) {
+        OraIonic::Sp t;
+        t.z = s[i].z; t.z_v = s[i].z_v; t.sigma_lr = s[i].sigma_lr; t.du = s[i].du;
+        t.r_sr = s[i].n_v_sr > 0 ? s[i].r_sr : 0.0;
+        t.v_sr.assign(s[i].v_sr, s[i].v_sr + s[i].n_v_sr);
+        t.pc_radius = s[i].pc_radius > 0.0 ? s[i].pc_radius : 0.0;
+        if (t.pc_radius > 0.0) t.rho_pc.assign(s[i].rho_pc, s[i].rho_pc + s[i].n_rho_pc);
+        for (int k = 0; k < s[i].n_proj; ++k)
+            t.proj.push_back({s[i].proj_l[k], s[i].proj_e_kb[k], s[i].proj_radius[k], Vec(s[i].proj_t[k], s[i].proj_t[k] + s[i].proj_n[k])});
+        io.sp.push_back(std::move(t));
+    }
+    return io;
+}
+
+// filter.rs:302-317 uniform_lagrange, and :355 read (0 beyond the radius): value and d/dd
+void table_read(const Vec& f, double du, double radius, double d, double& v, double& dv) {
+    v = dv = 0.0;
+    if (d > radius) return;
+    const double s = d / du;
+    const long i0 = (long)std::floor(s) - 1;
+    if (i0 + 3 >= (long)f.size()) return;
+    auto at = [&](long i) { return f[(size_t)(i < 0 ? -i : i)]; };
+    const double t = s - (double)i0;
+    const double a = at(i0), b = at(i0 + 1), c = at(i0 + 2), e = at(i0 + 3);
+    const double l[4] = {-(t - 1.0) * (t - 2.0) * (t - 3.0) / 6.0, t * (t - 2.0) * (t - 3.0) / 2.0, -t * (t - 1.0) * (t - 3.0) / 2.0,
+                         t * (t - 1.0) * (t - 2.0) / 6.0};
+    const double dl[4] = {-((t - 2.0) * (t - 3.0) + (t - 1.0) * (t - 3.0) + (t - 1.0) * (t - 2.0)) / 6.0,
+                          ((t - 2.0) * (t - 3.0) + t * (t - 3.0) + t * (t - 2.0)) / 2.0,
+                          -((t - 1.0) * (t - 3.0) + t * (t - 3.0) + t * (t - 1.0)) / 2.0,
+                          ((t - 1.0) * (t - 2.0) + t * (t - 2.0) + t * (t - 1.0)) / 6.0};
+    v = a * l[0] + b * l[1] + c * l[2] + e * l[3];
+    dv = (a * dl[0] + b * dl[1] + c * dl[2] + e * dl[3]) / du;
+}
+
+// nuclear.rs:320-336 points_within: a clipped index box, then |r - c| <= radius, ascending
+std::vector<size_t> points_within(const Grid& g, const double c[3], double radius) {
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        double l = std::fmax(std::floor((c[a] - radius - g.origin) / g.h), 0.0);
+        double h = std::fmin(std::ceil((c[a] + radius - g.origin) / g.h), (double)(g.n - 1));
+        if (!(h >= l)) return {};
+        lo[a] = (int)l;
+        hi[a] = (int)h;
+    }
+    std::vector<size_t> out;
+    for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+                size_t p = g.idx(i, j, k);
+                double r[3];
+                g.point(p, r);
+                if (dist2(r, c) <= radius * radius) out.push_back(p);
+            }
+    return out;
+}
+
+// nuclear.rs:297-302 smeared_potential with per-centre (q, sigma) + :338-346 the V_SR tables
+void ionic_local_potential(const Grid& g, const ora_nucleus* nuc, int nn, double sigma_ae, const OraIonic& io, double* out) {
+    const size_t N = g.len();
+    par_for((long)N, [&](long id) {
+        double r[3];
+        g.point(id, r);
+        double acc = -0.0;
+        for (int a = 0; a < nn; ++a) {
+            const int si = io.find(nuc[a].z);
+            const double q = si < 0 ? (double)nuc[a].z : io.sp[si].z_v, sg = si < 0 ? sigma_ae : io.sp[si].sigma_lr;
+            const double d = std::sqrt(dist2(r, nuc[a].pos));
+            const double on_site = std::sqrt(2.0 / PI) / sg;
+            acc += (d < 1e-10) ? -q * on_site : -q * std::erf(d / (sg * std::sqrt(2.0))) / d;
+        }
+        out[id] = acc;
+    });
+    for (int a = 0; a < nn; ++a) {
+        const int si = io.find(nuc[a].z);
+        if (si < 0 || io.sp[si].v_sr.empty()) continue;
+        const auto& t = io.sp[si];
+        for (size_t p : points_within(g, nuc[a].pos, t.r_sr)) {
+            double r[3], v, dv;
+            g.point(p, r);
+            table_read(t.v_sr, t.du, t.r_sr, std::sqrt(dist2(r, nuc[a].pos)), v, dv);
+            out[p] += v;
+        }
+    }
+}
+
+// nuclear.rs:350-359
+void partial_core_field(const Grid& g, const ora_nucleus* nuc, int nn, const OraIonic& io, double* out) {
+    std::fill(out, out + g.len(), 0.0);
+    for (int a = 0; a < nn; ++a) {
+        const int si = io.find(nuc[a].z);
+        if (si < 0 || !(io.sp[si].pc_radius > 0.0)) continue;
+        const auto& t = io.sp[si];
+        for (size_t p : points_within(g, nuc[a].pos, t.pc_radius)) {
+            double r[3], v, dv;
+            g.point(p, r);
+            table_read(t.rho_pc, t.du, t.pc_radius, std::sqrt(dist2(r, nuc[a].pos)), v, dv);
+            out[p] += v;
+        }
+    }
+}
+
+// nonlocal.rs:87-98 grad R_lm, l <= 2, lm order
+void grad_rlm(int l, int m, const double d[3], double g[3]) {
+    const double s3 = std::sqrt(3.0), x = d[0], y = d[1], z = d[2];
+    g[0] = g[1] = g[2] = 0.0;
+    if (l == 1) { if (m == -1) g[1] = 1.0; else if (m == 0) g[2] = 1.0; else g[0] = 1.0; }
+    if (l == 2) {
+        if (m == -2) { g[0] = s3 * y; g[1] = s3 * x; }
+        else if (m == -1) { g[1] = s3 * z; g[2] = s3 * y; }
+        else if (m == 0) { g[0] = -x; g[1] = -y; g[2] = 2.0 * z; }
+        else if (m == 1) { g[0] = s3 * z; g[2] = s3 * x; }
+        else { g[0] = s3 * x; g[1] = -s3 * y; }
+    }
+}
+
+// One projector sphere (nonlocal.rs Sphere): its ion, l, E_KB, points and beta_lm[m + l][point] (+ gradients)
+struct OraSphere {
+    int ion, l;
+    double e_kb;
+    std::vector<size_t> pts;
+    std::vector<Vec> beta;
+    std::vector<std::vector<double>> grad;  // [m + l][3 * point + axis]
+};
+
+// nonlocal.rs build_inner
+std::vector<OraSphere> build_nonlocal(const Grid& g, const ora_nucleus* nuc, int nn, const OraIonic& io, bool with_grad) {
+    std::vector<OraSphere> out;
+    for (int a = 0; a < nn; ++a) {
+        const int si = io.find(nuc[a].z);
+        if (si < 0) continue;
+        const auto& t = io.sp[si];
+        for (const auto& p : t.proj) {
+            OraSphere s;
+            s.ion = a;
+            s.l = p.l;
+            s.e_kb = p.e_kb;
+            s.pts = points_within(g, nuc[a].pos, p.radius);
+            const double norm = std::sqrt((2.0 * p.l + 1.0) / (4.0 * PI));
+            s.beta.assign(2 * p.l + 1, Vec(s.pts.size()));
+            if (with_grad) s.grad.assign(2 * p.l + 1, std::vector<double>(3 * s.pts.size()));
+            for (size_t q = 0; q < s.pts.size(); ++q) {
+                double r[3];
+                g.point(s.pts[q], r);
+                double d[3] = {r[0] - nuc[a].pos[0], r[1] - nuc[a].pos[1], r[2] - nuc[a].pos[2]};
+                double dd = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                double sh[N_MOM];
+                solid_harmonics(d, sh);
+                double tv, dt;
+                table_read(p.t, t.du, p.radius, dd, tv, dt);
+                const double tn = tv * norm;
+                for (int m = -p.l; m <= p.l; ++m) {
+                    const int lm = lm_index(p.l, m);
+                    s.beta[m + p.l][q] = tn * sh[lm];
+                    if (with_grad) {
+                        double gr[3];
+                        grad_rlm(p.l, m, d, gr);
+                        const double radial = dd > 1e-12 ? dt * norm * sh[lm] / dd : 0.0;
+                        for (int ax = 0; ax < 3; ++ax) s.grad[m + p.l][3 * q + ax] = radial * d[ax] + tn * gr[ax];
+                    }
+                }
+            }
+            out.push_back(std::move(s));
+        }
+    }
+    return out;
+}
+
+// c_lm[x] = h^3 Neumaier sum over the sphere of beta x (nonlocal.rs "On the grid")
+double project(const Grid& g, const OraSphere& s, int row, const double* x) {
+    return neumaier_fn(s.pts.size(), [&](size_t q) { return s.beta[row][q] * x[s.pts[q]]; }) * g.dv();
+}
+
+// y += V_NL x = sum_spheres sum_m E_KB c_lm[x] beta_lm
+void nonlocal_add(const Grid& g, const std::vector<OraSphere>& nl, const double* x, double* y) {
+    for (const auto& s : nl)
+        for (int r = 0; r < 2 * s.l + 1; ++r) {
+            const double w = s.e_kb * project(g, s, r, x);
+            for (size_t q = 0; q < s.pts.size(); ++q) y[s.pts[q]] += w * s.beta[r][q];
+        }
+}
+
+// H = -1/2 lap + V (+ V_NL)
+void ham(const Grid& g, const double* v, const std::vector<OraSphere>* nl, const double* x, double* y) {
+    hamiltonian(g, v, x, y);
+    if (nl && !nl->empty()) nonlocal_add(g, *nl, x, y);
+}
+
 struct Precond {
     const Grid& g;
     const double* v;
@@ -481,7 +684,7 @@ void orthonormalise(const Grid& g, std::vector<Vec>& s) {
 
 // eigen.rs:285-369 lobpcg_impl with head = k (no tiers)
 int lobpcg(const Grid& g, const double* v, std::vector<Vec>& x, Vec& evals, const Precond* pc, double tol, int max_iter,
-           double& max_residual) {
+           double& max_residual, const std::vector<OraSphere>* nl = nullptr) {
     const int k = (int)x.size();
     const size_t N = g.len();
     std::vector<Vec> xs = x;
@@ -492,7 +695,7 @@ int lobpcg(const Grid& g, const double* v, std::vector<Vec>& x, Vec& evals, cons
     int iterations = 0;
     max_residual = std::numeric_limits<double>::infinity();
     for (;;) {
-        for (int i = 0; i < k; ++i) { hamiltonian(g, v, xs[i].data(), hx[i].data()); evals[i] = gdot(g, xs[i], hx[i]); }
+        for (int i = 0; i < k; ++i) { ham(g, v, nl, xs[i].data(), hx[i].data()); evals[i] = gdot(g, xs[i], hx[i]); }
         std::vector<Vec> w;
         double max_res = 0.0;
         Vec r(N);
@@ -515,7 +718,7 @@ int lobpcg(const Grid& g, const double* v, std::vector<Vec>& x, Vec& evals, cons
         orthonormalise(g, s);
         const int m = (int)s.size();
         std::vector<Vec> hs(m, Vec(N));
-        for (int i = 0; i < m; ++i) hamiltonian(g, v, s[i].data(), hs[i].data());
+        for (int i = 0; i < m; ++i) ham(g, v, nl, s[i].data(), hs[i].data());
         Vec a((size_t)m * m);
         for (int i = 0; i < m; ++i)
             for (int j = 0; j <= i; ++j) {
@@ -709,6 +912,7 @@ struct ora_state {
     Vec ev_up, ev_dn, rho_up, rho_dn, v_nuc, v_h;
     Vec occ_up, occ_dn;  // one occupation per stored orbital (all 1 under Aufbau)
     double sigma = 0;
+    bool ionic = false;  // solved under an ionic setup
 };
 
 extern "C" {
@@ -792,19 +996,42 @@ int ora_diis_coefficients(int m, const double* gram, double* c) {
     return 1;
 }
 
-// scf.rs:928-1098 scf_tiered, Aufbau branch, no ionic setup
-ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, int n_dn, const ora_settings* s,
-                   const ora_state* warm, ora_stats* st) {
+// scf.rs:928-1098 scf_tiered, with the ionic setup of scf.rs:114-140 when io holds species
+static ora_state* scf_impl(int n, double h, const ora_nucleus* nuc, int nn, int n_up, int n_dn, const ora_settings* s,
+                           const OraIonic* io, const ora_state* warm, ora_stats* st) {
     Grid g(n, h);
     const size_t N = g.len();
     std::memset(st, 0, sizeof(*st));
+    const bool ionic = io && !io->sp.empty();
     double e_nn;
     if (nuclear_repulsion(nuc, nn, e_nn) != 0) { st->status = 3; return nullptr; }
+    if (ionic) {  // nuclear.rs:368-378 ionic_repulsion: valence charges
+        e_nn = 0.0;
+        for (int i = 0; i < nn; ++i)
+            for (int j = i + 1; j < nn; ++j) e_nn += io->charge(nuc[i].z) * io->charge(nuc[j].z) / std::sqrt(dist2(nuc[i].pos, nuc[j].pos));
+    }
     auto state = std::make_unique<ora_state>();
     state->g = g;
     state->sigma = s->sigma;
-    Vec v_nuc(N);
-    nuclear_potential(g, nuc, nn, s->sigma, v_nuc.data());
+    state->ionic = ionic;
+    Vec v_nuc(N), rho_pc;
+    std::vector<OraSphere> nl;
+    if (ionic) {
+        ionic_local_potential(g, nuc, nn, s->sigma, *io, v_nuc.data());
+        bool core = false;
+        for (int a = 0; a < nn; ++a) { int si = io->find(nuc[a].z); core = core || (si >= 0 && io->sp[si].pc_radius > 0.0); }
+        if (core) { rho_pc.resize(N); partial_core_field(g, nuc, nn, *io, rho_pc.data()); }
+        nl = build_nonlocal(g, nuc, nn, *io, false);
+    } else {
+        nuclear_potential(g, nuc, nn, s->sigma, v_nuc.data());
+    }
+    // LSDA on (up + pc/2, dn + pc/2) (scf.rs:759-768)
+    auto xc = [&](const Vec& up, const Vec& dn, Vec& e, Vec& xu, Vec& xd) {
+        if (rho_pc.empty()) { lsda(N, up.data(), dn.data(), e.data(), xu.data(), xd.data()); return; }
+        Vec u(N), d(N);
+        for (size_t i = 0; i < N; ++i) { u[i] = up[i] + 0.5 * rho_pc[i]; d[i] = dn[i] + 0.5 * rho_pc[i]; }
+        lsda(N, u.data(), d.data(), e.data(), xu.data(), xd.data());
+    };
     Poisson poisson(g);
     const double ptol = std::fmin(1e-10, 1e-3 * s->tol);   // scf.rs:503 poisson_tol
     const int PMAX = 5000;
@@ -818,16 +1045,26 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
     // witness block by doubling; a fixed block whose top level passes the witness gives the same f to e^-36)
     const int ku = n_up + ((fd && n_up > 0) ? std::max(1, s->n_extra) : 0);
     const int kd = n_dn + ((fd && n_dn > 0) ? std::max(1, s->n_extra) : 0);
-    bool reuse = warm && warm->g == g && (int)warm->orb_up.size() == ku && (int)warm->orb_dn.size() == kd;
+    bool reuse = warm && warm->g == g && (int)warm->orb_up.size() == ku && (int)warm->orb_dn.size() == kd && !ionic && !warm->ionic;
     if (reuse) {
         orb_up = warm->orb_up; orb_dn = warm->orb_dn; ev_up = warm->ev_up; ev_dn = warm->ev_dn;
         in_up = warm->rho_up; in_dn = warm->rho_dn; v_h = warm->v_h;
     } else {
         double total = (double)(n_up + n_dn);
         double z_tot = 0.0;
-        for (int a = 0; a < nn; ++a) z_tot += (double)nuc[a].z;
+        for (int a = 0; a < nn; ++a) z_tot += ionic ? io->charge(nuc[a].z) : (double)nuc[a].z;
         Vec guess(N);
         deposit_charge(g, nuc, nn, 1.0, guess.data());   // nuclear.rs:212-214, Aufbau: σ = 1 blobs
+        if (ionic) {  // nuclear.rs:204-206 deposit_centres: each centre's charge q in a σ = 1 blob
+            const double norm = 1.0 / std::pow(2.0 * PI, 1.5);
+            par_for((long)N, [&](long id) {
+                double r[3];
+                g.point(id, r);
+                double acc = -0.0;
+                for (int a = 0; a < nn; ++a) acc += io->charge(nuc[a].z) * norm * std::exp(-dist2(r, nuc[a].pos) * 0.5);
+                guess[id] = acc;
+            });
+        }
         double scale = z_tot > 0.0 ? total / z_tot : 0.0;
         double fu = total > 0.0 ? n_up / total : 0.0, fd = total > 0.0 ? n_dn / total : 0.0;
         Vec buf;
@@ -864,7 +1101,7 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
         pois_res = std::fmax(pois_res, pr);
         pois_it = std::max(pois_it, pit);
         st->poisson_iterations_total += pit;
-        lsda(N, in_up.data(), in_dn.data(), exc.data(), xu.data(), xd.data());
+        xc(in_up, in_dn, exc, xu, xd);
         for (size_t i = 0; i < N; ++i) { vu[i] = v_nuc[i] + v_h[i] + xu[i]; vd[i] = v_nuc[i] + v_h[i] + xd[i]; }
         for (int spin = 0; spin < 2; ++spin) {
             auto& orb = spin ? orb_dn : orb_up;
@@ -874,7 +1111,7 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
             double lambda = ev.empty() ? -1.0 : ev[0];
             Precond pc(g, v.data(), lambda);
             double mr;
-            int it = lobpcg(g, v.data(), orb, ev, &pc, s->eig_tol, 200, mr);
+            int it = lobpcg(g, v.data(), orb, ev, &pc, s->eig_tol, 200, mr, &nl);
             if (it < 0) { st->status = 4; return nullptr; }
             eig_res = std::fmax(eig_res, mr);
             st->eigen_iterations_total += it;
@@ -941,8 +1178,22 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
             kinetic_e += occ[o] * gdot(g, orb[o], t);
         }
     }
-    lsda(N, out_up.data(), out_dn.data(), exc.data(), xu.data(), xd.data());
+    xc(out_up, out_dn, exc, xu, xd);
     double external_ = gdot(g, rho, v_nuc);
+    if (!nl.empty()) {  // E_NL = sum f E_KB c^2, Neumaier over (orbital, sphere, m) (nonlocal.rs)
+        Vec terms;
+        for (int spin = 0; spin < 2; ++spin) {
+            auto& orb = spin ? orb_dn : orb_up;
+            auto& occ = spin ? occ_dn : occ_up;
+            for (size_t o = 0; o < orb.size(); ++o)
+                for (const auto& sp : nl)
+                    for (int r = 0; r < 2 * sp.l + 1; ++r) {
+                        double c = project(g, sp, r, orb[o].data());
+                        terms.push_back(occ[o] * sp.e_kb * c * c);
+                    }
+        }
+        external_ += neumaier_fn(terms.size(), [&](size_t i) { return terms[i]; });
+    }
     double hartree = 0.5 * gdot(g, rho, v_h);
     double xc_e = integrate(g, exc);
     double internal = kinetic_e + external_ + hartree + xc_e + e_nn;
@@ -970,6 +1221,150 @@ ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, in
     state->rho_up = std::move(out_up); state->rho_dn = std::move(out_dn);
     state->v_nuc = std::move(v_nuc); state->v_h = std::move(v_h);
     return state.release();
+}
+
+ora_state* ora_scf(int n, double h, const ora_nucleus* nuc, int nn, int n_up, int n_dn, const ora_settings* s,
+                   const ora_state* warm, ora_stats* st) {
+    return scf_impl(n, h, nuc, nn, n_up, n_dn, s, nullptr, warm, st);
+}
+
+ora_state* ora_scf_ionic(int n, double h, const ora_nucleus* nuc, int nn, int n_up, int n_dn, const ora_settings* s,
+                         const ora_species* species, int n_species, const ora_state* warm, ora_stats* st) {
+    OraIonic io = make_ionic(species, n_species);
+    return scf_impl(n, h, nuc, nn, n_up, n_dn, s, &io, warm, st);
+}
+
+void ora_ionic_local_potential(int n, double h, const ora_nucleus* nuc, int nn, double sigma_ae, const ora_species* species,
+                               int n_species, double* out) {
+    ionic_local_potential(Grid(n, h), nuc, nn, sigma_ae, make_ionic(species, n_species), out);
+}
+
+void ora_partial_core(int n, double h, const ora_nucleus* nuc, int nn, const ora_species* species, int n_species, double* out) {
+    partial_core_field(Grid(n, h), nuc, nn, make_ionic(species, n_species), out);
+}
+
+int ora_nonlocal_apply(int n, double h, const ora_nucleus* nuc, int nn, const ora_species* species, int n_species, const double* x,
+                       int count, double* out, double* c) {
+    Grid g(n, h);
+    const size_t N = g.len();
+    auto nl = build_nonlocal(g, nuc, nn, make_ionic(species, n_species), false);
+    int rows = 0;
+    for (const auto& sp : nl) rows += 2 * sp.l + 1;
+    for (int v = 0; v < count; ++v) {
+        std::fill(out + (size_t)v * N, out + (size_t)(v + 1) * N, 0.0);
+        nonlocal_add(g, nl, x + (size_t)v * N, out + (size_t)v * N);
+        if (c) {
+            int row = 0;
+            for (const auto& sp : nl)
+                for (int r = 0; r < 2 * sp.l + 1; ++r) c[(size_t)v * rows + row++] = project(g, sp, r, x + (size_t)v * N);
+        }
+    }
+    return rows;
+}
+
+double ora_frozen_energy(const ora_state* st, const ora_nucleus* nuc, int nn, double sigma, const ora_species* species,
+                         int n_species) {
+    const Grid& g = st->g;
+    const size_t N = g.len();
+    OraIonic io = make_ionic(species, n_species);
+    Vec rho(N), vloc(N), pc(N, 0.0), e(N), xu(N), xd(N), u(N), d(N);
+    for (size_t i = 0; i < N; ++i) rho[i] = st->rho_up[i] + st->rho_dn[i];
+    ionic_local_potential(g, nuc, nn, sigma, io, vloc.data());
+    partial_core_field(g, nuc, nn, io, pc.data());
+    for (size_t i = 0; i < N; ++i) { u[i] = st->rho_up[i] + 0.5 * pc[i]; d[i] = st->rho_dn[i] + 0.5 * pc[i]; }
+    lsda(N, u.data(), d.data(), e.data(), xu.data(), xd.data());
+    double en = gdot(g, rho, vloc) + integrate(g, e);
+    auto nl = build_nonlocal(g, nuc, nn, io, false);
+    for (int spin = 0; spin < 2; ++spin) {
+        const auto& orb = spin ? st->orb_dn : st->orb_up;
+        const auto& occ = spin ? st->occ_dn : st->occ_up;
+        for (size_t o = 0; o < orb.size(); ++o)
+            for (const auto& sp : nl)
+                for (int r = 0; r < 2 * sp.l + 1; ++r) {
+                    const double c = project(g, sp, r, orb[o].data());
+                    en += occ[o] * sp.e_kb * c * c;
+                }
+    }
+    for (int i = 0; i < nn; ++i)
+        for (int j = i + 1; j < nn; ++j) en += io.charge(nuc[i].z) * io.charge(nuc[j].z) / std::sqrt(dist2(nuc[i].pos, nuc[j].pos));
+    return en;
+}
+
+void ora_table_read(const double* f, int len, double du, double radius, double d, double* v, double* dv) {
+    table_read(Vec(f, f + len), du, radius, d, *v, *dv);
+}
+
+void ora_solid_harmonic_gradients(const double r[3], double out[27]) {
+    for (int l = 0; l <= 2; ++l)
+        for (int m = -l; m <= l; ++m) grad_rlm(l, m, r, out + 3 * lm_index(l, m));
+}
+
+// forces.rs (pseudised ions): F_I = -dE/dR_I at frozen orbitals and occupations
+int ora_forces_ionic(const ora_state* st, const ora_nucleus* nuc, int nn, double sigma, const ora_species* species, int n_species,
+                     double* out3n) {
+    const Grid& g = st->g;
+    const size_t N = g.len();
+    OraIonic io = make_ionic(species, n_species);
+    Vec rho(N), pc(N, 0.0), vbar(N, 0.0);
+    for (size_t i = 0; i < N; ++i) rho[i] = st->rho_up[i] + st->rho_dn[i];
+    bool core = false;
+    for (int a = 0; a < nn; ++a) { int si = io.find(nuc[a].z); core = core || (si >= 0 && io.sp[si].pc_radius > 0.0); }
+    if (core) {
+        partial_core_field(g, nuc, nn, io, pc.data());
+        par_for((long)N, [&](long i) {
+            double e, vu, vd;
+            exc_point(st->rho_up[i] + 0.5 * pc[i], st->rho_dn[i] + 0.5 * pc[i], e, vu, vd);
+            vbar[i] = 0.5 * (vu + vd);
+        });
+    }
+    Vec comp[3] = {Vec(N), Vec(N), Vec(N)};
+    for (int a = 0; a < nn; ++a) {
+        const int si = io.find(nuc[a].z);
+        const double q = si < 0 ? (double)nuc[a].z : io.sp[si].z_v, sg = si < 0 ? sigma : io.sp[si].sigma_lr;
+        for (int c = 0; c < 3; ++c) std::fill(comp[c].begin(), comp[c].end(), 0.0);
+        par_for((long)N, [&](long p) {
+            double r[3];
+            g.point(p, r);
+            double dv[3] = {r[0] - nuc[a].pos[0], r[1] - nuc[a].pos[1], r[2] - nuc[a].pos[2]};
+            double d = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+            if (d < 1e-8) return;
+            const double u = d / (sg * std::sqrt(2.0));
+            double gsum = -q * ((2.0 / std::sqrt(PI)) * u * std::exp(-u * u) - std::erf(u)) / (d * d) * rho[p];
+            if (si >= 0) {
+                const auto& t = io.sp[si];
+                double v, dvv;
+                if (!t.v_sr.empty()) { table_read(t.v_sr, t.du, t.r_sr, d, v, dvv); gsum += rho[p] * dvv; }
+                if (t.pc_radius > 0.0) { table_read(t.rho_pc, t.du, t.pc_radius, d, v, dvv); gsum += vbar[p] * dvv; }
+            }
+            for (int c = 0; c < 3; ++c) comp[c][p] = gsum / d * dv[c];
+        });
+        for (int c = 0; c < 3; ++c) out3n[3 * a + c] = integrate(g, comp[c]);
+    }
+    // nonlocal: sum_{sigma, i} 2 f_i E_KB c <grad beta | psi_i>
+    auto nl = build_nonlocal(g, nuc, nn, io, true);
+    for (int spin = 0; spin < 2; ++spin) {
+        const auto& orb = spin ? st->orb_dn : st->orb_up;
+        const auto& occ = spin ? st->occ_dn : st->occ_up;
+        for (size_t o = 0; o < orb.size(); ++o)
+            for (const auto& sp : nl)
+                for (int r = 0; r < 2 * sp.l + 1; ++r) {
+                    const double c = project(g, sp, r, orb[o].data());
+                    for (int ax = 0; ax < 3; ++ax) {
+                        const double gb = neumaier_fn(sp.pts.size(), [&](size_t q) { return sp.grad[r][3 * q + ax] * orb[o][sp.pts[q]]; }) * g.dv();
+                        out3n[3 * sp.ion + ax] += 2.0 * occ[o] * sp.e_kb * c * gb;
+                    }
+                }
+    }
+    for (int a = 0; a < nn; ++a)
+        for (int b = 0; b < nn; ++b) {
+            if (b == a) continue;
+            double dv[3] = {nuc[a].pos[0] - nuc[b].pos[0], nuc[a].pos[1] - nuc[b].pos[1], nuc[a].pos[2] - nuc[b].pos[2]};
+            double d = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+            if (d < 1e-8) return -1;
+            double s = io.charge(nuc[a].z) * io.charge(nuc[b].z) / (d * d * d);
+            for (int c = 0; c < 3; ++c) out3n[3 * a + c] += s * dv[c];
+        }
+    return 0;
 }
 
 void ora_state_free(ora_state* st) { delete st; }

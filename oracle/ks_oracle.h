@@ -19,6 +19,18 @@ extern "C" {
 
 typedef struct { double pos[3]; int z; } ora_nucleus;
 
+/* One pseudised species: the uniform tables (spacing du, index 0 at d = 0) the reference's grid samples of a
+   qm::radial::filter::FilteredTable (crates/qm/src/radial/filter.rs:323-363); the same layout as ks_species. */
+typedef struct {
+    int z;
+    double z_v, sigma_lr, du;
+    const double* v_sr; int n_v_sr; double r_sr;
+    const double* rho_pc; int n_rho_pc; double pc_radius;
+    int n_proj;
+    const int* proj_l; const double* proj_e_kb; const double* proj_radius;
+    const double* const* proj_t; const int* proj_n;
+} ora_species;
+
 /* Settings of one SCF (crates/qm/src/scf.rs:375 ScfSettings). occupations: 0 Aufbau, 1 Fermi-Dirac at kt
    (crates/qm/src/occupations.rs) over a block of n_sigma + n_extra levels per occupied channel. */
 typedef struct {
@@ -92,6 +104,32 @@ void ora_state_density(const ora_state* st, double* rho_up, double* rho_dn);
 void ora_state_potentials(const ora_state* st, double* v_nuc, double* v_h);
 void ora_state_orbitals(const ora_state* st, int spin, double* out);
 int  ora_forces(const ora_state* st, const ora_nucleus* nuc, int nn, double sigma, double* out3n);
+
+/* ---- pseudised ions (crates/qm/src/scf.rs:114-140, ionic.rs, nonlocal.rs, forces.rs) ---- */
+/* ora_scf under an ionic setup: nuclei whose Z is listed are pseudised, the others all-electron at s->sigma.
+   n_species = 0 is ora_scf. A warm state is reused only between all-electron solves. */
+ora_state* ora_scf_ionic(int n, double h, const ora_nucleus* nuc, int nn, int n_up, int n_dn, const ora_settings* s,
+                         const ora_species* species, int n_species, const ora_state* warm, ora_stats* stats);
+/* V_loc (nuclear.rs:338-346) and rho_pc (:350-359) of the geometry */
+void ora_ionic_local_potential(int n, double h, const ora_nucleus* nuc, int nn, double sigma_ae, const ora_species* species,
+                               int n_species, double* out);
+void ora_partial_core(int n, double h, const ora_nucleus* nuc, int nn, const ora_species* species, int n_species, double* out);
+/* out_v = V_NL x_v for count vectors (n^3 each), and c[v * rows + row] = h^3 <beta_row, x_v> when c is not NULL;
+   returns the number of projector rows */
+int ora_nonlocal_apply(int n, double h, const ora_nucleus* nuc, int nn, const ora_species* species, int n_species, const double* x,
+                       int count, double* out, double* c);
+/* The R-dependent energy at the state's frozen orbitals and densities: integral rho V_loc + E_NL +
+   E_xc[rho_up + rho_pc/2, rho_dn + rho_pc/2] + E_ii (valence charges). Its R-derivative is minus ora_forces_ionic. */
+double ora_frozen_energy(const ora_state* st, const ora_nucleus* nuc, int nn, double sigma, const ora_species* species,
+                         int n_species);
+/* filter.rs:302-317 uniform_lagrange behind the radius test of FilteredTable::read: value and derivative */
+void ora_table_read(const double* f, int len, double du, double radius, double d, double* v, double* dv);
+/* nonlocal.rs:87-98 grad R_lm for l <= 2, out[3 * lm + axis], lm = l^2 + l + m */
+void ora_solid_harmonic_gradients(const double r[3], double out[27]);
+/* forces of a state solved by ora_scf_ionic with the same setup: local long/short range, partial core, nonlocal,
+   ion-ion (crates/qm/src/forces.rs, pseudised ions). Returns 0, or -1 on coincident nuclei. */
+int ora_forces_ionic(const ora_state* st, const ora_nucleus* nuc, int nn, double sigma, const ora_species* species, int n_species,
+                     double* out3n);
 
 #ifdef __cplusplus
 }

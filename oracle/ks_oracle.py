@@ -66,6 +66,20 @@ def lib():
         L.ora_state_occupations.argtypes = [ctypes.c_void_p, dp, dp]
         L.ora_trilinear.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp, ctypes.c_int, dp]
         L.ora_fermi_dirac.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
+        sp = ctypes.POINTER(SpeciesStruct)
+        L.ora_scf_ionic.restype = ctypes.c_void_p
+        L.ora_scf_ionic.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(Settings), sp, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(Stats)]
+        L.ora_ionic_local_potential.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double,
+                                                sp, ctypes.c_int, dp]
+        L.ora_partial_core.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(Nucleus), ctypes.c_int, sp, ctypes.c_int, dp]
+        L.ora_nonlocal_apply.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(Nucleus), ctypes.c_int, sp, ctypes.c_int, dp,
+                                         ctypes.c_int, dp, dp]
+        L.ora_frozen_energy.restype = ctypes.c_double
+        L.ora_frozen_energy.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, sp, ctypes.c_int]
+        L.ora_table_read.argtypes = [dp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp, dp]
+        L.ora_solid_harmonic_gradients.argtypes = [dp, dp]
+        L.ora_forces_ionic.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, sp, ctypes.c_int, dp]
         _lib = L
     return _lib
 
@@ -280,6 +294,119 @@ def scf(n, h, nuclei, n_up, n_dn, sigma=None, tol=1e-6, mixing=0.3, eig_tol=1e-6
     stats["electrons"] = list(st.electrons)
     stats["mu"] = list(st.mu)
     return (State(ptr, n) if ptr else None), stats
+
+
+# ---- pseudised ions (crates/qm/src/scf.rs:114-140, ionic.rs, nonlocal.rs, forces.rs)
+class SpeciesStruct(ctypes.Structure):
+    """ora_species (ks_oracle.h): one pseudised species' uniform tables."""
+    _fields_ = [("z", ctypes.c_int), ("z_v", ctypes.c_double), ("sigma_lr", ctypes.c_double), ("du", ctypes.c_double),
+                ("v_sr", ctypes.POINTER(ctypes.c_double)), ("n_v_sr", ctypes.c_int), ("r_sr", ctypes.c_double),
+                ("rho_pc", ctypes.POINTER(ctypes.c_double)), ("n_rho_pc", ctypes.c_int), ("pc_radius", ctypes.c_double),
+                ("n_proj", ctypes.c_int), ("proj_l", ctypes.POINTER(ctypes.c_int)), ("proj_e_kb", ctypes.POINTER(ctypes.c_double)),
+                ("proj_radius", ctypes.POINTER(ctypes.c_double)), ("proj_t", ctypes.POINTER(ctypes.POINTER(ctypes.c_double))),
+                ("proj_n", ctypes.POINTER(ctypes.c_int))]
+
+
+def species_array(species):
+    """(ctypes array, keep-alive list) from objects with the fields z, z_v, sigma_lr, du, v_sr, r_sr, rho_pc,
+    pc_radius and projectors (each with l, e_kb, radius, t)."""
+    keep = []
+
+    def dptr(a):
+        a = np.ascontiguousarray(a if a is not None else np.zeros(0), dtype=np.float64)
+        keep.append(a)
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size
+
+    arr = (SpeciesStruct * max(len(species), 1))()
+    for i, sp in enumerate(species):
+        st = arr[i]
+        st.z, st.z_v, st.sigma_lr, st.du = int(sp.z), float(sp.z_v), float(sp.sigma_lr), float(sp.du)
+        st.v_sr, st.n_v_sr = dptr(sp.v_sr)
+        st.r_sr = float(sp.r_sr)
+        st.rho_pc, st.n_rho_pc = dptr(sp.rho_pc)
+        st.pc_radius = float(sp.pc_radius)
+        k = len(sp.projectors)
+        st.n_proj = k
+        ls = (ctypes.c_int * max(k, 1))(*[p.l for p in sp.projectors])
+        ek = (ctypes.c_double * max(k, 1))(*[p.e_kb for p in sp.projectors])
+        rr = (ctypes.c_double * max(k, 1))(*[p.radius for p in sp.projectors])
+        tp = (ctypes.POINTER(ctypes.c_double) * max(k, 1))()
+        tn = (ctypes.c_int * max(k, 1))()
+        for j, p in enumerate(sp.projectors):
+            tp[j], tn[j] = dptr(p.t)
+        keep += [ls, ek, rr, tp, tn]
+        st.proj_l, st.proj_e_kb, st.proj_radius, st.proj_t, st.proj_n = ls, ek, rr, tp, tn
+    return arr, keep
+
+
+def scf_ionic(n, h, nuclei, n_up, n_dn, species, sigma=None, tol=1e-6, mixing=0.3, eig_tol=1e-6, max_iter=200, diis_history=6,
+              stall_window=50, kt=None, n_extra=1):
+    """SCF under an ionic setup (the species listed are pseudised). Returns (State or None, stats dict)."""
+    s = Settings(h if sigma is None else sigma, tol, mixing, eig_tol, max_iter, diis_history, stall_window,
+                 0 if kt is None else 1, int(n_extra), 0.0 if kt is None else float(kt))
+    st = Stats()
+    arr, keep = species_array(species)
+    ptr = lib().ora_scf_ionic(n, ctypes.c_double(h), nuclei_array(nuclei), len(nuclei), n_up, n_dn, ctypes.byref(s), arr, len(species),
+                              None, ctypes.byref(st))
+    stats = {f[0]: getattr(st, f[0]) for f in Stats._fields_}
+    stats["electrons"] = list(st.electrons)
+    stats["mu"] = list(st.mu)
+    return (State(ptr, n) if ptr else None), stats
+
+
+def ionic_local_potential(n, h, nuclei, sigma_ae, species):
+    arr, keep = species_array(species)
+    out = np.empty(n ** 3)
+    lib().ora_ionic_local_potential(n, ctypes.c_double(h), nuclei_array(nuclei), len(nuclei), ctypes.c_double(sigma_ae), arr,
+                                    len(species), _p(out))
+    return out
+
+
+def partial_core(n, h, nuclei, species):
+    arr, keep = species_array(species)
+    out = np.empty(n ** 3)
+    lib().ora_partial_core(n, ctypes.c_double(h), nuclei_array(nuclei), len(nuclei), arr, len(species), _p(out))
+    return out
+
+
+def nonlocal_apply(n, h, nuclei, species, x):
+    """(V_NL x for each row of x (count, n^3), c (count, rows) = h^3 <beta_row, x>)."""
+    arr, keep = species_array(species)
+    x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1, n ** 3))
+    out = np.empty_like(x)
+    c = np.empty(len(x) * 4096)
+    rows = lib().ora_nonlocal_apply(n, ctypes.c_double(h), nuclei_array(nuclei), len(nuclei), arr, len(species), _p(x), len(x),
+                                    _p(out), _p(c))
+    return out, c[:len(x) * rows].reshape(len(x), rows)
+
+
+def frozen_energy(state, nuclei, sigma, species):
+    """integral rho V_loc + E_NL + E_xc[rho + rho_pc/2 per spin] + E_ii at the state's frozen orbitals and densities."""
+    arr, keep = species_array(species)
+    return lib().ora_frozen_energy(state.ptr, nuclei_array(nuclei), len(nuclei), ctypes.c_double(sigma), arr, len(species))
+
+
+def table_read(f, du, radius, d):
+    """(value, d/dd) of the 4-point Lagrange read of a uniform table (0 beyond radius)."""
+    f = _f64(f)
+    v, dv = ctypes.c_double(), ctypes.c_double()
+    lib().ora_table_read(_p(f), f.size, ctypes.c_double(du), ctypes.c_double(radius), ctypes.c_double(d), ctypes.byref(v), ctypes.byref(dv))
+    return v.value, dv.value
+
+
+def solid_harmonic_gradients(r):
+    """(9, 3): grad R_lm for l <= 2 in lm order."""
+    out = np.empty(27)
+    lib().ora_solid_harmonic_gradients(_p(_f64(r)), _p(out))
+    return out.reshape(9, 3)
+
+
+def forces_ionic(state, nuclei, sigma, species):
+    arr, keep = species_array(species)
+    out = np.empty(3 * len(nuclei))
+    if lib().ora_forces_ionic(state.ptr, nuclei_array(nuclei), len(nuclei), ctypes.c_double(sigma), arr, len(species), _p(out)) != 0:
+        raise ValueError("coincident nuclei")
+    return out.reshape(-1, 3)
 
 
 def trilinear(n, h, f, points):
