@@ -114,6 +114,14 @@ void* ks_solver_create(int n, double h, const ks_options* opts) {
 
 void ks_solver_destroy(void* solver) { delete static_cast<Handle*>(solver); }
 
+long long ks_footprint_bytes(int n, int n_up, int n_dn, const ks_options* opts, int diis_history, int with_core) {
+    if (n < 5 || n > 1024 || n_up < 0 || n_dn < 0 || n_up > 4096 || n_dn > 4096 || diis_history < 0 || diis_history > 64) return -1;
+    SolverOptions o;
+    if (opts) o.n_extra = opts->n_extra;
+    if (o.n_extra < 0 || o.n_extra > 4096) return -1;
+    return (long long)Solver::footprint_bytes(n, n_up, n_dn, o, diis_history, with_core != 0);
+}
+
 const char* ks_last_error(const void* solver) {
     if (!solver) return g_create_error.c_str();
     auto* h = static_cast<const Handle*>(solver);

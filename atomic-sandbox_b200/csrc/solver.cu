@@ -520,6 +520,31 @@ void Channel::create(const Layout& L, int kk) {
 }
 
 // ------------------------------------------------------------------ solver
+// Mirrors the allocations of the constructor, Poisson::init, Reducer::init, Channel::create, the DIIS pool and the
+// ionic fields; each buffer is counted at cudaMalloc's 2 MiB granularity for large and 512 B for small requests.
+size_t Solver::footprint_bytes(int n, int n_up, int n_dn, const SolverOptions& o, int diis_history, bool pseudo_core) {
+    const Layout L = Layout::make(n, 1.0);
+    auto rounded = [](size_t b) { return b >= ((size_t)1 << 20) ? (b + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1) : (b + 511) & ~(size_t)511; };
+    const size_t field = (size_t)L.F * sizeof(float);
+    size_t total = 0;
+    total += 11 * rounded(field);                                        // potentials, densities, XC, ones
+    total += 3 * (rounded(((size_t)1 << 20) * sizeof(double)) + rounded(Reducer::RES_CAP * sizeof(double)));  // reducers
+    total += 7 * rounded(field) + rounded(24 * (size_t)n * n * sizeof(double));  // Poisson CG fields and ghost table
+    for (int m = n; m > 2;) {                                            // multigrid levels, four fields each
+        m /= 2;
+        total += 4 * rounded((size_t)Layout::make(m, 1.0).F * sizeof(float));
+    }
+    for (int ne : {n_up, n_dn}) {
+        if (ne <= 0) continue;
+        const int k = ne + o.n_extra;
+        total += 2 * rounded(3 * k * field) + rounded(3 * k * field) + 2 * rounded(k * field);  // [X W P] x2, T, HX, Q
+        total += rounded((size_t)(2 * k + 6 * k * k) * sizeof(double));
+    }
+    total += (size_t)(std::max(diis_history, 1) + 1) * 4 * rounded(field);  // DIIS pool
+    if (pseudo_core) total += 3 * rounded(field);                          // partial core and the forces' v_xc
+    return total;
+}
+
 Solver::Solver(int n, double h, const SolverOptions& o) : L_(Layout::make(n, h)), opt_(o) {
     if (n < 5 || !(h > 0)) throw std::invalid_argument("grid: n >= 5 and h > 0 required");
     KS_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));

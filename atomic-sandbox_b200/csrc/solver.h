@@ -199,6 +199,10 @@ struct SolverOptions { int gram_mode = 0; int n_extra = 0; int init_mode = 0; };
 
 class Solver {
 public:
+    // Device bytes a solver of this grid holds through a solve and its forces with n_up / n_dn electrons, the
+    // options' extra bands and a DIIS history (its buffers as allocated below; the CUDA context and the loaded
+    // kernels are not counted). pseudo_core adds the partial-core fields of an ionic setup.
+    static size_t footprint_bytes(int n, int n_up, int n_dn, const SolverOptions& o, int diis_history, bool pseudo_core);
     Solver(int n, double h, const SolverOptions& o);
     ~Solver();
     ks_status solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,

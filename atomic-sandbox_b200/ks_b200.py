@@ -172,7 +172,7 @@ EXPORTED = [
     "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
     "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations", "ks_sample_density", "ks_sampling_counters",
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
-    "ks_apply_nonlocal", "ks_density_with_core_to_volume",
+    "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes",
 ]
 
 
@@ -237,6 +237,8 @@ def lib():
         L.ks_spin_abs_integral.argtypes = [ctypes.c_void_p, dp]
         L.ks_set_ionic.argtypes = [ctypes.c_void_p, ctypes.POINTER(SpeciesStruct), ctypes.c_int]
         L.ks_apply_nonlocal.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, dp, dp, dp, ip]
+        L.ks_footprint_bytes.restype = ctypes.c_longlong
+        L.ks_footprint_bytes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Options), ctypes.c_int, ctypes.c_int]
         L.ks_density_with_core_to_volume.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, dp]
         _lib = L
     return _lib
@@ -351,6 +353,11 @@ class GpuSolver:
         self._abort_ref = cb
         rc = lib().ks_solve(self._h, arr, len(system.nuclei), int(system.n_up), int(system.n_dn), ctypes.byref(cs),
                             1 if warm else 0, cb, None, ctypes.byref(st))
+        if rc in (KS_NOT_CONVERGED, KS_STALLED):
+            # QmError::ScfNotConverged(iterations, dRho) / ScfStalled { iterations, .. }: the counts ride on the exception
+            err = _ERRORS[rc](lib().ks_last_error(self._h).decode(errors="replace"))
+            err.iterations, err.delta_rho = st.iterations, st.delta_rho
+            raise err
         _check(rc, self._h)
         e = st.energy
         return {
@@ -482,6 +489,15 @@ class GpuSolver:
         p = _Profile()
         _check(lib().ks_profile_get(self._h, ctypes.byref(p)), self._h)
         return {n: getattr(p, n) for n, _ in _Profile._fields_}
+
+
+def footprint_bytes(n, n_up, n_dn, n_extra=0, diis_history=6, with_core=False):
+    """Device bytes a GpuSolver of the n^3 grid holds through a solve and its forces (ks_footprint_bytes)."""
+    o = _Options(0, int(n_extra), 0, 0)
+    b = lib().ks_footprint_bytes(int(n), int(n_up), int(n_dn), ctypes.byref(o), int(diis_history), 1 if with_core else 0)
+    if b < 0:
+        raise ValueError("footprint: invalid grid, counts or history")
+    return int(b)
 
 
 # ---- grid-kernel entry points (host f64 in/out)

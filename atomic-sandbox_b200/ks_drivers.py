@@ -1,6 +1,7 @@
-"""Callers either side of the SCF path, on the B200 solver: Born-Oppenheimer molecular dynamics
-(velocity Verlet with warm-started solves), concurrent solves of a batch of geometries, and the
-synthetic workload geometries (H2, H2O, NH3, n-butane and the batch templates).
+"""Callers either side of the SCF path, on the B200 solver: the provider's evaluation semantics (GpuKs: one solver per
+grid, warm starts, the cold retry of a failed warm solve, the GPU-memory guard), Born-Oppenheimer molecular dynamics
+(velocity Verlet with warm-started solves), concurrent solves of a batch of geometries, and the synthetic workload
+geometries (H2, H2O, NH3, n-butane and the batch templates).
 
 Reference anchors: the integrator is crates/sim/src/integrator.rs (kick-drift-kick, atomic units,
 dt converted once from fs); masses are isotope masses in amu times AMU_IN_ME
@@ -8,6 +9,7 @@ dt converted once from fs); masses are isotope masses in amu times AMU_IN_ME
 solves (one GpuSolver per grid, crates/providers/src/ks.rs) run concurrently on one GPU.
 """
 import concurrent.futures
+import dataclasses
 import math
 import time
 
@@ -120,6 +122,113 @@ def batch_workload(count=64, seed=0x5EED, n_min=48, n_max=96, h=0.25, jitter=0.0
     return out
 
 
+# ------------------------------------------------------------------ the provider's evaluation (crates/providers/src/ks.rs)
+@dataclasses.dataclass(frozen=True)
+class Stall:
+    """A warm solve that failed before the cold retry (crates/providers/src/ks.rs:566-584): its SCF iterations and
+    dRho, and whether the stall stop ended it."""
+    iterations: int
+    delta_rho: float
+    stalled: bool
+
+    def note(self):
+        if self.stalled:
+            return (f"warm SCF stalled (dRho {self.delta_rho:.2e}, not improved 2x in the stall window; stopped after "
+                    f"{self.iterations} iterations); retried cold")
+        return f"warm SCF did not converge (dRho {self.delta_rho:.2e} after {self.iterations} steps); retried cold"
+
+
+def retry_cold_on_stall(warm, solve):
+    """crates/providers/src/ks.rs:585-601: `solve(w)` runs one SCF, warm iff w. A warm attempt that ends in
+    ScfNotConverged or ScfStalled is retried cold exactly once and that outcome returned, with the Stall; every other
+    outcome (success, a cold failure, another error) is the first attempt's. Returns (result, Stall or None)."""
+    try:
+        return solve(warm), None
+    except ks.ScfNotConverged as e:
+        if not warm:
+            raise
+        stall = Stall(getattr(e, "iterations", 0), getattr(e, "delta_rho", float("nan")), False)
+    except ks.ScfStalled as e:
+        if not warm:
+            raise
+        stall = Stall(getattr(e, "iterations", 0), getattr(e, "delta_rho", float("nan")), True)
+    return solve(False), stall
+
+
+VRAM_SLACK = 1.1
+
+
+class GpuKs:
+    """The Kohn-Sham force provider's semantics on the B200 solver (crates/providers/src/ks.rs:1014-1700, GpuKs):
+
+    - one GpuSolver per grid; a grid change (n or h) rebuilds it and drops the warm state (ks.rs:12-14);
+    - every evaluation starts warm from the previous converged state on the same grid and setup, with the cold retry
+      of retry_cold_on_stall; its note is returned with the result;
+    - with a memory budget, a scene whose solver footprint (ks_footprint_bytes) exceeds it is refused with a
+      ValueError before any solver is built (GpuKs::check_vram, ks.rs:1303-1324);
+    - a device failure drops the solver and its state (the next evaluation rebuilds it), and is raised;
+    - should_abort is polled before every SCF step (ks.Aborted).
+    """
+
+    def __init__(self, gram_mode=1, n_extra=3, vram_budget=None, vram_note=None, init_mode=1):
+        self.gram_mode, self.n_extra, self.init_mode = gram_mode, n_extra, init_mode
+        self.vram_budget, self.vram_note = vram_budget, vram_note
+        self.solver = None
+        self._grid = None
+        self._species = None
+        self._warm = False
+
+    def with_vram_budget(self, nbytes, note=None):
+        self.vram_budget, self.vram_note = int(nbytes), note
+        return self
+
+    def _budget_words(self):
+        b = f"the {self.vram_budget / 1e9:.1f} GB budget"
+        return f"{b} ({self.vram_note})" if self.vram_note else b
+
+    def check_vram(self, n, n_up, n_dn, settings, species=None):
+        if self.vram_budget is None:
+            return
+        core = any(getattr(sp, "pc_radius", 0.0) > 0.0 for sp in (species or []))
+        # the solver's buffers (measured within a few percent on B200) plus 10 % for the allocator's granularity
+        need = int(VRAM_SLACK * ks.footprint_bytes(n, n_up, n_dn, self.n_extra, settings.diis_history, core))
+        if need > self.vram_budget:
+            kind = "valence " if species else ""
+            raise ValueError(f"this scene needs ~{need / 1e9:.2f} GB of GPU memory at {n}^3 ({n_up + n_dn} {kind}electrons), "
+                             f"over {self._budget_words()}: choose a coarser grid or fewer atoms")
+
+    def close(self):
+        if self.solver is not None:
+            self.solver.close()
+        self.solver, self._grid, self._warm = None, None, False
+
+    def evaluate(self, nuclei, n, h, n_up, n_dn, settings=None, species=None, should_abort=None):
+        """One evaluation: {energy, forces (n, 3), stats, notes}. Raises the solver's QmError subclasses."""
+        settings = settings or ks.ScfSettings(sigma=h)
+        self.check_vram(n, n_up, n_dn, settings, species)
+        if self._grid != (n, h):
+            self.close()
+            self.solver = ks.GpuSolver(n, h, gram_mode=self.gram_mode, n_extra=self.n_extra, init_mode=self.init_mode)
+            self._grid, self._species = (n, h), None
+        sp_key = None if not species else [id(x) for x in species]
+        if sp_key != self._species:
+            self.solver.set_ionic(list(species or []))
+            self._species = sp_key
+        system = ks.System(nuclei, n_up, n_dn)
+        try:
+            stats, stall = retry_cold_on_stall(self._warm, lambda w: self.solver.solve(system, settings, warm=w,
+                                                                                       should_abort=should_abort))
+            forces = self.solver.forces(nuclei, settings.sigma if settings.sigma is not None else h)
+        except ks.Device:
+            self.close()
+            raise
+        except ks.QmError:
+            self._warm = False
+            raise
+        self._warm = True
+        return {"energy": stats["energy"]["total"], "forces": forces, "stats": stats, "notes": [stall.note()] if stall else []}
+
+
 # ------------------------------------------------------------------ molecular dynamics
 def velocity_verlet(solver, nuclei, n_up, n_dn, settings, dt_au, steps, velocities=None, sigma=None, retry_cold=True):
     """Born-Oppenheimer MD, kick-drift-kick velocity Verlet (crates/sim/src/integrator.rs): one SCF
@@ -135,15 +244,12 @@ def velocity_verlet(solver, nuclei, n_up, n_dn, settings, dt_au, steps, velociti
 
     def solve(pos, warm):
         nuc = [tuple(p) + (q,) for p, q in zip(pos, z)]
-        retried = False
-        try:
-            st = solver.solve(ks.System(nuc, n_up, n_dn), settings, warm=warm)
-        except (ks.ScfNotConverged, ks.ScfStalled):
-            if not (warm and retry_cold):
-                raise
-            retried = True
-            st = solver.solve(ks.System(nuc, n_up, n_dn), settings, warm=False)
-        return st, solver.forces(nuc, sigma), retried
+        system = ks.System(nuc, n_up, n_dn)
+        if retry_cold:
+            st, stall = retry_cold_on_stall(warm, lambda w: solver.solve(system, settings, warm=w))
+        else:
+            st, stall = solver.solve(system, settings, warm=warm), None
+        return st, solver.forces(nuc, sigma), stall is not None
 
     st, f, retried = solve(r, False)
     traj = []

@@ -94,6 +94,13 @@ typedef int (*ks_abort_fn)(void* user);
 void* ks_solver_create(int n, double h, const ks_options* opts);
 void ks_solver_destroy(void* solver);
 
+/* The device memory (bytes) a solver of the n^3 grid holds through a solve with n_up / n_dn electrons and its forces:
+   its own buffers, not the CUDA context or the loaded kernels; with_core adds the fields of an ionic setup with a
+   partial core. The B200 counterpart of the provider's footprint estimate (crates/providers/src/ks.rs:465-470,
+   solve_footprint_bytes), which a caller compares with a memory budget before building a solver
+   (GpuKs::check_vram, ks.rs:1303-1324). opts may be NULL; negative for invalid arguments. */
+long long ks_footprint_bytes(int n, int n_up, int n_dn, const ks_options* opts, int diis_history, int with_core);
+
 /* One pseudised species: what the grid samples of the reference's qm::radial::filter::FilteredTable
    (crates/qm/src/radial/filter.rs:323-363) for one element at this grid's h. Every table is an even function
    tabulated at d = k du, k = 0 .. n-1 (the reference's du = h / 256), read by 4-point Lagrange with index -1
