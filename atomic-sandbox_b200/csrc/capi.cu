@@ -141,6 +141,19 @@ ks_status ks_solve(void* solver, const ks_nucleus* nuclei, int n_nuclei, int n_u
     });
 }
 
+ks_status ks_solve_observed(void* solver, const ks_nucleus* nuclei, int n_nuclei, int n_up, int n_dn, const ks_settings* settings,
+                            int warm, ks_abort_fn abort_fn, ks_abort_fn inner_abort, ks_observe_fn observe, void* user, ks_stats* out) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h || !settings || !out) return fail(h, KS_INVALID, "null argument");
+    if (!(settings->sigma > 0) || !(settings->tol > 0) || settings->max_iter < 1 || !(settings->eig_tol > 0))
+        return fail(h, KS_INVALID, "invalid settings");
+    return guarded(h, [&] {
+        ks_status st = h->solver->solve(nuclei, n_nuclei, n_up, n_dn, *settings, warm != 0, abort_fn, user, out, inner_abort, observe);
+        if (st != KS_OK) h->error = h->solver->error;
+        return st;
+    });
+}
+
 ks_status ks_forces(void* solver, const ks_nucleus* nuclei, int n_nuclei, double sigma, double* out3n) {
     auto* h = static_cast<Handle*>(solver);
     if (!h) return fail(h, KS_INVALID, "null solver");

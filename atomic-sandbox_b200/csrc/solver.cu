@@ -658,6 +658,9 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
     std::vector<double> prev_theta;
     std::vector<double> res(k);
     for (;;) {
+        // the inner cancellation point (crates/qm-gpu/src/scf.rs:1224-1235): the calling thread polls, every channel obeys
+        if (inner_fn_ && std::this_thread::get_id() == poll_thread_ && inner_fn_(inner_user_)) inner_flag_.store(1);
+        if (inner_flag_.load()) throw AbortInside();
         Block& S = ch.A[ch.cur];
         // 1. R = HX - theta X with the first Jacobi sweep fused (into Q), then 3 damped sweeps Q -> W -> Q -> W
         double* norm_partials = lane.red.partials();
@@ -799,8 +802,16 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
 }
 
 ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,
-                        void* user, ks_stats* out) {
+                        void* user, ks_stats* out, ks_abort_fn inner_abort, ks_observe_fn observe) {
     auto t0 = clk::now();
+    inner_fn_ = inner_abort;
+    inner_user_ = user;
+    poll_thread_ = std::this_thread::get_id();
+    inner_flag_.store(0);
+    struct ClearInner {
+        Solver* so;
+        ~ClearInner() { so->inner_fn_ = nullptr; so->inner_user_ = nullptr; }
+    } clear_inner{this};
     std::memset(out, 0, sizeof(*out));
     profile = ks_profile{};
     const int rb0 = readbacks_total();
@@ -927,21 +938,23 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         double max_eig_res = 0.0, last_step_res = 0.0, pois_res = 0.0;
         int pois_it_max = 0;
         bool last_step_maxiter = false;
+        // park the iterate (orbitals, evals, input densities) as the next warm start and report the abort
+        auto park = [&](const std::string& why) {
+            have_warm_ = true;
+            fd_state_ = fd;
+            KS_CUDA(cudaMemcpyAsync(out_up_.at(0), in_up_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+            KS_CUDA(cudaMemcpyAsync(out_dn_.at(0), in_dn_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+            KS_CUDA(cudaStreamSynchronize(s_));
+            profile.steps = iterations;
+            profile.readbacks = readbacks_total() - rb0;
+            profile.host_dense_s = lane_[0]->dense_s + lane_[1]->dense_s;
+            profile.sync_wait_s = wait_total() - wait0;
+            profile.wall_s = secs(t0);
+            error = why;
+            return KS_ABORTED;
+        };
         while (iterations < s.max_iter) {
-            if (abort_fn && abort_fn(user)) {
-                have_warm_ = true;  // park the iterate (orbitals, evals, input densities) as the next warm start
-                fd_state_ = fd;
-                KS_CUDA(cudaMemcpyAsync(out_up_.at(0), in_up_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
-                KS_CUDA(cudaMemcpyAsync(out_dn_.at(0), in_dn_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
-                KS_CUDA(cudaStreamSynchronize(s_));
-                profile.steps = iterations;
-                profile.readbacks = readbacks_total() - rb0;
-                profile.host_dense_s = lane_[0]->dense_s + lane_[1]->dense_s;
-                profile.sync_wait_s = wait_total() - wait0;
-                profile.wall_s = secs(t0);
-                error = "abandoned before SCF step " + std::to_string(iterations + 1);
-                return KS_ABORTED;
-            }
+            if (abort_fn && abort_fn(user)) return park("abandoned before SCF step " + std::to_string(iterations + 1));
             ++iterations;
             // a warm guess is accepted within the 1.5x band only in the convergence phase (the previous step's dRho
             // already below tol); before that only within the step's own tol. This is the reference's rule for its
@@ -968,8 +981,9 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             pois_it_max = std::max(pois_it_max, ps.iterations);
             if (ps.stop == 3) ++out->n_warnings;
             // XC and the effective potentials
-            launch_xc_veff(L_.F, in_up_.at(0), in_dn_.at(0), vnuc_.at(0), vh_.at(0), exc_.at(0), v_up_.at(0), v_dn_.at(0), nullptr,
-                           nullptr, s_, pc);
+            if (observe && xcu_.count == 0) { xcu_.create(L_, 1); xcd_.create(L_, 1); }
+            launch_xc_veff(L_.F, in_up_.at(0), in_dn_.at(0), vnuc_.at(0), vh_.at(0), exc_.at(0), v_up_.at(0), v_dn_.at(0),
+                           observe ? xcu_.at(0) : nullptr, observe ? xcd_.at(0) : nullptr, s_, pc);
             // eigensolves
             int eig_its = 0;
             last_step_res = 0.0;
@@ -1005,13 +1019,27 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 } catch (...) {
                     err_up = std::current_exception();
                 }
-                if (worker.joinable()) worker.join();
+                if (worker.joinable()) {
+                    if (err_up) inner_flag_.store(1);  // the other channel leaves at its next iteration
+                    worker.join();
+                }
                 for (auto& l : lane_) {
                     KS_CUDA(cudaEventRecord(l->ev_join, l->s));
                     KS_CUDA(cudaStreamWaitEvent(s_, l->ev_join, 0));
                 }
-                if (err_up) std::rethrow_exception(err_up);
-                if (err_dn) std::rethrow_exception(err_dn);
+                auto is_abort = [](std::exception_ptr e) {
+                    try {
+                        std::rethrow_exception(e);
+                    } catch (const AbortInside&) {
+                        return true;
+                    } catch (...) {
+                        return false;
+                    }
+                };
+                // a real error wins over the abort it triggered in the other channel
+                if (err_up && !is_abort(err_up)) std::rethrow_exception(err_up);
+                if (err_dn && !is_abort(err_dn)) std::rethrow_exception(err_dn);
+                if (err_up || err_dn) return park("abandoned inside SCF step " + std::to_string(iterations) + " (an eigensolve)");
             }
             for (int sp = 0; sp < 2; ++sp) {
                 if (nocc[sp] == 0) continue;
@@ -1078,7 +1106,13 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             pairs.push_back({E.r_up.at(0), E.r_up.at(0)});
             pairs.push_back({E.r_dn.at(0), E.r_dn.at(0)});
             red_.dots(pairs, 4, dv);
-            const double* h = red_.read(4 + (int)pairs.size());
+            // observed solves only: the Harris-Foulkes double counting of rho_in rides on this readback
+            // (int rho_in V_H, int rho_in,sigma v_xc,sigma, E_xc[rho_in]; crates/qm-gpu/src/scf.rs:1500-1505)
+            const int hf_off = 4 + (int)pairs.size();
+            if (observe)
+                red_.dots({{rho_tot_.at(0), vh_.at(0)}, {in_up_.at(0), xcu_.at(0)}, {in_dn_.at(0), xcd_.at(0)}, {exc_.at(0), ones_.at(0)}},
+                          hf_off, dv);
+            const double* h = red_.read(hf_off + (observe ? 4 : 0));
             delta_rho = h[0] + h[2];
             q_out[0] = h[1];
             q_out[1] = h[3];
@@ -1099,6 +1133,33 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             if (delta_rho < best) best = delta_rho;
             if (std::isfinite(delta_rho) && (!std::isfinite(anchor) || delta_rho <= 0.5 * anchor)) { anchor = delta_rho; anchor_at = iterations; }
             const int since = iterations - anchor_at;
+            if (observe) {
+                // qm::ScfProgress (crates/qm/src/scf.rs:488-498): F_HF = sum f eps + double counting - kT S, Neumaier sums
+                auto neumaier = [](const std::vector<double>& v) {
+                    double sum = 0.0, comp = 0.0;
+                    for (double x : v) {
+                        const double t = sum + x;
+                        if (std::fabs(sum) >= std::fabs(x)) comp += (sum - t) + x; else comp += (x - t) + sum;
+                        sum = t;
+                    }
+                    return sum + comp;
+                };
+                std::vector<double> band;
+                for (int sp = 0; sp < 2; ++sp)
+                    for (int i = 0; i < (int)occ_[sp].size() && i < (int)ch_[sp].evals.size(); ++i) band.push_back(occ_[sp][i] * ch_[sp].evals[i]);
+                const double dc = neumaier({-0.5 * h[hf_off], -h[hf_off + 1], -h[hf_off + 2], h[hf_off + 3], e_nn});
+                ks_progress pg{};
+                pg.iteration = iterations;
+                pg.max_iter = s.max_iter;
+                pg.delta_rho = delta_rho;
+                pg.tol = s.tol;
+                pg.energy = neumaier(band) + dc - (fd ? s.kt * entropy : 0.0);
+                pg.best_delta_rho = best;
+                pg.since_gain = since;
+                pg.window = s.stall_window;
+                pg.stall_level = level;
+                observe(&pg, user);
+            }
             test_tol = (fd && partial) ? std::max(s.tol, GPU_PARTIAL_TOL) : s.tol;
             if (!std::isfinite(delta_rho) || (delta_rho < test_tol && step_tol <= eig_lo)) break;
             if (!(delta_rho < test_tol) && s.stall_window > 0 && since >= s.stall_window && best >= level) { stalled = true; break; }

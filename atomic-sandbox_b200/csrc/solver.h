@@ -1,7 +1,9 @@
 // solver.h -- the B200 Kohn-Sham solver behind the C ABI (include/ks_cuda.h).
 #pragma once
+#include <atomic>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 #include "common.cuh"
 #include "kernels.cuh"
@@ -195,6 +197,9 @@ struct Lane {
     ~Lane();
 };
 
+// Thrown out of an eigensolve when the inner cancellation point fired.
+struct AbortInside {};
+
 struct SolverOptions { int gram_mode = 0; int n_extra = 0; int init_mode = 0; };
 
 class Solver {
@@ -206,7 +211,7 @@ public:
     Solver(int n, double h, const SolverOptions& o);
     ~Solver();
     ks_status solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,
-                    void* user, ks_stats* out);
+                    void* user, ks_stats* out, ks_abort_fn inner_abort = nullptr, ks_observe_fn observe = nullptr);
     ks_status forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n);
     ks_status vjp(const ks_nucleus* nuc, int nn, double sigma, double e_bar, double* dE_dR3n, double* dE_dsigma);
     // the ionic setup of the next solves (n = 0: all-electron); throws std::invalid_argument on bad tables
@@ -258,6 +263,12 @@ private:
     Ionic::Scratch nl_sc_;                     // projections on the solver's stream (energy, forces)
     Block pc_, xcu_, xcd_;                     // partial core of the geometry; v_xc scratch of the forces
     bool nl_on_ = false;                       // H psi includes V_NL (inside a solve under a setup)
+    // the inner cancellation point: polled by the calling thread once per LOBPCG iteration; a hit sets the flag, which
+    // every channel's eigensolve checks at its next iteration and leaves by AbortInside
+    ks_abort_fn inner_fn_ = nullptr;
+    void* inner_user_ = nullptr;
+    std::thread::id poll_thread_;
+    std::atomic<int> inner_flag_{0};
     int state_gen_ = 0;                        // ionic generation the state was solved under (0: all-electron)
     int ionic_gen() const { return ionic_.active() ? ionic_.generation() : 0; }
     ks_status ionic_forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n);

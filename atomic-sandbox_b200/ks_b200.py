@@ -60,6 +60,16 @@ class _Profile(ctypes.Structure):
 ABORT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
 
 
+class Progress(ctypes.Structure):
+    """ks_progress: qm::ScfProgress (crates/qm/src/scf.rs:488-498)."""
+    _fields_ = [("iteration", ctypes.c_int), ("max_iter", ctypes.c_int), ("delta_rho", ctypes.c_double), ("tol", ctypes.c_double),
+                ("energy", ctypes.c_double), ("best_delta_rho", ctypes.c_double), ("since_gain", ctypes.c_int), ("window", ctypes.c_int),
+                ("stall_level", ctypes.c_double)]
+
+
+OBSERVE_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(Progress), ctypes.c_void_p)
+
+
 @dataclasses.dataclass
 class Projector:
     """One Kleinman-Bylander projector of a pseudised species: angular momentum l <= 2, E_KB (Ha), the radius of
@@ -172,7 +182,7 @@ EXPORTED = [
     "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
     "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations", "ks_sample_density", "ks_sampling_counters",
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
-    "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes",
+    "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed",
 ]
 
 
@@ -237,6 +247,9 @@ def lib():
         L.ks_spin_abs_integral.argtypes = [ctypes.c_void_p, dp]
         L.ks_set_ionic.argtypes = [ctypes.c_void_p, ctypes.POINTER(SpeciesStruct), ctypes.c_int]
         L.ks_apply_nonlocal.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, dp, dp, dp, ip]
+        L.ks_solve_observed.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(_Settings), ctypes.c_int, ABORT_FN, ABORT_FN, OBSERVE_FN, ctypes.c_void_p,
+                                        ctypes.POINTER(_Stats)]
         L.ks_footprint_bytes.restype = ctypes.c_longlong
         L.ks_footprint_bytes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Options), ctypes.c_int, ctypes.c_int]
         L.ks_density_with_core_to_volume.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, dp]
@@ -340,8 +353,10 @@ class GpuSolver:
     def __exit__(self, *exc):
         self.close()
 
-    def solve(self, system, settings=None, warm=False, should_abort=None):
-        """Runs the SCF; returns the stats dict (ScfStats) or raises a QmError subclass."""
+    def solve(self, system, settings=None, warm=False, should_abort=None, inner_abort=None, observe=None):
+        """Runs the SCF; returns the stats dict (ScfStats) or raises a QmError subclass. should_abort is polled before
+        every SCF step, inner_abort once per LOBPCG iteration (GpuSolver::solve_polled); observe(progress_dict) gets one
+        qm::ScfProgress per step (GpuSolver::solve_observed)."""
         s = settings or ScfSettings()
         if s.occupations not in ("aufbau", "fermi_dirac"):
             raise ValueError("occupations: 'aufbau' or 'fermi_dirac'")
@@ -351,8 +366,15 @@ class GpuSolver:
         arr = nuclei_array(system.nuclei)
         cb = ABORT_FN(lambda _u: 1 if should_abort() else 0) if should_abort else ABORT_FN()
         self._abort_ref = cb
-        rc = lib().ks_solve(self._h, arr, len(system.nuclei), int(system.n_up), int(system.n_dn), ctypes.byref(cs),
-                            1 if warm else 0, cb, None, ctypes.byref(st))
+        if inner_abort is None and observe is None:
+            rc = lib().ks_solve(self._h, arr, len(system.nuclei), int(system.n_up), int(system.n_dn), ctypes.byref(cs),
+                                1 if warm else 0, cb, None, ctypes.byref(st))
+        else:
+            icb = ABORT_FN(lambda _u: 1 if inner_abort() else 0) if inner_abort else ABORT_FN()
+            ocb = OBSERVE_FN(lambda p, _u: observe({n: getattr(p.contents, n) for n, _ in Progress._fields_})) if observe else OBSERVE_FN()
+            self._observe_refs = (icb, ocb)
+            rc = lib().ks_solve_observed(self._h, arr, len(system.nuclei), int(system.n_up), int(system.n_dn), ctypes.byref(cs),
+                                         1 if warm else 0, cb, icb, ocb, None, ctypes.byref(st))
         if rc in (KS_NOT_CONVERGED, KS_STALLED):
             # QmError::ScfNotConverged(iterations, dRho) / ScfStalled { iterations, .. }: the counts ride on the exception
             err = _ERRORS[rc](lib().ks_last_error(self._h).decode(errors="replace"))

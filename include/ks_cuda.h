@@ -101,6 +101,18 @@ void ks_solver_destroy(void* solver);
    (GpuKs::check_vram, ks.rs:1303-1324). opts may be NULL; negative for invalid arguments. */
 long long ks_footprint_bytes(int n, int n_up, int n_dn, const ks_options* opts, int diis_history, int with_core);
 
+/* qm::ScfProgress (crates/qm/src/scf.rs:488-498): one SCF step as an observer sees it, after its dRho readback and
+   before the convergence test. energy is the Harris-Foulkes energy of the step's input density (F_HF = sum f eps
+   + double counting - kT S of the step's occupations); best_delta_rho, since_gain, window and stall_level are the
+   stall watch's. */
+typedef struct {
+    int iteration, max_iter;
+    double delta_rho, tol, energy, best_delta_rho;
+    int since_gain, window;
+    double stall_level;
+} ks_progress;
+typedef void (*ks_observe_fn)(const ks_progress* progress, void* user);
+
 /* One pseudised species: what the grid samples of the reference's qm::radial::filter::FilteredTable
    (crates/qm/src/radial/filter.rs:323-363) for one element at this grid's h. Every table is an even function
    tabulated at d = k du, k = 0 .. n-1 (the reference's du = h / 256), read by 4-point Lagrange with index -1
@@ -142,6 +154,14 @@ ks_status ks_apply_nonlocal(void* solver, const ks_nucleus* nuclei, int n_nuclei
    warm != 0 reuses the last converged state when its counts match. abort may be NULL. */
 ks_status ks_solve(void* solver, const ks_nucleus* nuclei, int n_nuclei, int n_up, int n_dn, const ks_settings* settings,
                    int warm, ks_abort_fn abort_fn, void* user, ks_stats* out);
+
+/* GpuSolver::solve_observed / solve_polled (crates/qm-gpu/src/scf.rs:1213-1235): ks_solve with a second cancellation
+   point and an observer. inner_abort (may be NULL) is also polled once per LOBPCG iteration of the calling thread's
+   eigensolve, so an abort lands within one iteration rather than one SCF step; it abandons the solve like abort_fn
+   (KS_ABORTED, the iterate parked as the next warm start). observe (may be NULL) gets one ks_progress per SCF step; it
+   changes no number of the solve. Both callbacks run on the calling thread and get `user`. */
+ks_status ks_solve_observed(void* solver, const ks_nucleus* nuclei, int n_nuclei, int n_up, int n_dn, const ks_settings* settings,
+                            int warm, ks_abort_fn abort_fn, ks_abort_fn inner_abort, ks_observe_fn observe, void* user, ks_stats* out);
 
 /* GpuSolver::forces (crates/qm-gpu/src/forces.rs:239): Hellmann-Feynman force on each nucleus
    (out3n[3*i + axis]) from the converged state, plus the point nuclear repulsion. */
