@@ -345,7 +345,10 @@ class GpuSolver:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the module's globals may already be gone; the process frees the GPU
+            pass
 
     def __enter__(self):
         return self

@@ -68,10 +68,18 @@ class Clocks:
         cmd = ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"]
         if self.uuid:
             cmd += ["-i", self.uuid]
+        self.first = []
         try:
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+        if self.proc:
+            # nvidia-smi's start-up holds driver locks for a moment; let it finish (its first sample) before the timed
+            # region, so that the host-driven solve is not stalled behind it
+            import select
+            ready, _, _ = select.select([self.proc.stdout], [], [], 10.0)
+            if ready:
+                self.first.append(self.proc.stdout.readline())
         return self
 
     def __exit__(self, *exc):
@@ -83,7 +91,7 @@ class Clocks:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.lines = [l for l in out.splitlines() if l.strip()]  # samples taken during the timed region
 
     def summary(self):
         sm, smax, reasons = [], None, set()
