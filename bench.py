@@ -42,8 +42,7 @@ CONFIG = {"workload": "H2O cold SCF + forces, 95^3 grid, h=0.25 Bohr, sigma=0.5 
           "grid": N, "h_bohr": H, "sigma_bohr": SIGMA, "bands_per_spin": N_UP + N_EXTRA, "l2": "flushed (256 MiB write) before each step"}
 
 
-def rank_info():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+from ks_replicas import max_over_ranks, rank_info, shard  # noqa: E402  (the replica plumbing of the package)
 
 
 def measured_peaks():
@@ -220,9 +219,8 @@ def bench_ours(args):
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+        import ks_replicas
+        ks_replicas.init("nccl", torch.device("cuda", local))
     dev = torch.device("cuda", local)
     uuid = None
     try:
@@ -283,12 +281,7 @@ def bench_ours(args):
     best = mixed if mixed is not None else plain
     t_local = statistics.mean(best["times"])
     e2e_local = statistics.mean(best["walls"])
-    if world > 1:
-        t = torch.tensor([t_local, e2e_local], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_max, e2e_max = float(t[0]), float(t[1])
-    else:
-        t_max, e2e_max = t_local, e2e_local
+    t_max, e2e_max = max_over_ranks([t_local, e2e_local], dev)
     roof = hpsi_roofline(torch, ks, peak, peak_source) if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -352,16 +345,32 @@ def bench_batch(args):
     sigma = 0.5, neutral, LSDA, 3 extra bands per spin, mixed form, tol 1e-6; `--workers` concurrent
     solves on the one GPU. Metric: geometries per second over the wall time of the whole batch
     (one warm-up pass of the first `--workers` molecules first)."""
+    import torch
     import ks_drivers as drv
-    jobs = drv.batch_workload(count=args.count)
+    import ks_replicas
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        ks_replicas.init("nccl", dev)
+    all_jobs = drv.batch_workload(count=args.count)
+    jobs = shard(all_jobs, rank, world)  # replicas: each GPU solves its share, no collective on the data path
     drv.solve_batch(jobs[: args.workers], workers=args.workers)
+    if world > 1:
+        torch.distributed.barrier()
     results, wall = drv.solve_batch(jobs, workers=args.workers)
     serial = None
     if args.serial:
         _, serial = drv.solve_batch(jobs, workers=1)
-    line = {"metric": "batch geometries/s (64 molecules, 48^3-96^3, to 1e-6)", "value": len(jobs) / wall, "unit": "geometries/s",
-            "n_gpus": 1, "higher_is_better": True, "wall_s": wall, "workers": args.workers, "count": len(jobs),
-            "scf_steps_total": int(sum(r["iterations"] for r in results)), "dtype": "f32", "data": "synthetic (seeded templates)",
+    wall, steps = max_over_ranks([wall, 0.0], dev)[0], sum(r["iterations"] for r in results)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": "batch geometries/s (64 molecules, 48^3-96^3, to 1e-6)", "value": len(all_jobs) / wall, "unit": "geometries/s",
+            "n_gpus": world, "higher_is_better": True, "wall_s": wall, "workers": args.workers, "count": len(all_jobs),
+            "scf_steps_rank0": int(steps), "dtype": "f32", "data": "synthetic (seeded templates)", "scaling": "strong",
             "config": {"workload": "batch of seeded molecules, per-molecule cubic grids U{48..96}, h=0.25, sigma=0.5, mixed form"},
             "serial_wall_s": serial, "timing": "wall clock around the batch (many solvers and streams)"}
     print(json.dumps(line), flush=True)
