@@ -67,18 +67,22 @@ class Clocks:
         cmd = ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"]
         if self.uuid:
             cmd += ["-i", self.uuid]
-        self.first = []
         try:
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
         if self.proc:
-            # nvidia-smi's start-up holds driver locks for a moment; let it finish (its first sample) before the timed
-            # region, so that the host-driven solve is not stalled behind it
+            # nvidia-smi's start-up holds driver locks for a while and stalls the host-driven solve's many small CUDA
+            # calls; let it settle (its first sample, then two more seconds) before the timed region, and drop what it
+            # printed so far: only samples taken during the timed region are kept
             import select
-            ready, _, _ = select.select([self.proc.stdout], [], [], 10.0)
-            if ready:
-                self.first.append(self.proc.stdout.readline())
+            fd = self.proc.stdout
+            if select.select([fd], [], [], 10.0)[0]:
+                fd.readline()
+            time.sleep(2.0)
+            while select.select([fd], [], [], 0.0)[0]:
+                if not fd.readline():
+                    break
         return self
 
     def __exit__(self, *exc):
