@@ -373,5 +373,16 @@ bool fd_witness(const double* ev, int k, int n, double mu, double kt) {
     return s.back() >= s[n - 1] + 0.1 && s.back() - mu >= 36.0 * kt;
 }
 
+int fd_witness_keep(const double* ev, int k, int n, double mu, double kt) {
+    if (n == 0 || k <= n) return k;
+    std::vector<double> s(ev, ev + k);
+    std::sort(s.begin(), s.end());
+    const double eps_n = s[n - 1];
+    auto passes = [&](int r) { return s[r] >= eps_n + 0.1 && s[r] - mu >= 36.0 * kt; };
+    for (int t = n; t < k; ++t)
+        if (passes(t)) return (t + 1 < k && passes(t + 1)) ? t + 2 : t + 1;
+    return k;
+}
+
 }  // namespace dense
 }  // namespace ks

@@ -39,6 +39,9 @@ bool diis_coefficients(int m, const Mat& gram, std::vector<double>& c);
 bool fermi_dirac(const double* evals, int k, int n, double kt, double* f, double& mu, double& entropy);
 // The highest level at least 0.1 Ha above the n-th lowest and 36 kT above mu (occupations.rs witness_reached).
 bool fd_witness(const double* evals, int k, int n, double mu, double kt);
+// After a passed witness, how many of the lowest levels to keep (occupations.rs:367-394 witness_keep, read on the levels
+// themselves): t + 1 for the lowest rank t >= n that is a witness, t + 2 when the level above it is one too; k when none.
+int fd_witness_keep(const double* evals, int k, int n, double mu, double kt);
 
 }  // namespace dense
 }  // namespace ks

@@ -97,6 +97,8 @@ constexpr double EIG_GUESS_FACTOR = 1.5;
 constexpr double PARTIAL_OCCUPATION_MIN = 1e-6;
 constexpr double GPU_PARTIAL_TOL = 1e-5;
 constexpr double LOOSE_F_FACTOR = 1e-2;
+// at most this many extra levels per channel grown for the Fermi-Dirac gap witness (crates/qm/src/scf.rs:295)
+constexpr int MAX_WITNESS_GROWTH = 32;
 constexpr double EIG_TOL_FRACTION = 0.0015;
 constexpr double EIG_TOL_MAX = 1e-3;
 constexpr double LAST_STEP_RESIDUAL_FACTOR = 3.0;
@@ -520,6 +522,23 @@ void Channel::create(const Layout& L, int kk) {
 }
 
 // ------------------------------------------------------------------ solver
+// The channel's block at newk columns: the lowest min(k, newk) columns of the current iterate are kept (in the first
+// arena), new ones are the reference's initial orbital with seed 1000 + 2 * column + spin (crates/qm/src/scf.rs:866).
+void Solver::resize_channel(int sp, int newk, const Nuc* dnuc, int nn) {
+    Channel& old = ch_[sp];
+    const int keep = std::min(old.k, newk);
+    Channel nc;
+    nc.create(L_, newk);
+    KS_CUDA(cudaMemcpyAsync(nc.A[0].at(0), old.X(), (size_t)keep * L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+    for (int i = keep; i < newk; ++i)
+        launch_initial_orbitals(L_, dnuc, nn, 1, 1000ULL + 2ULL * (unsigned long long)i + (unsigned long long)sp, 0, nc.A[0].at(i), s_);
+    nc.evals.assign(old.evals.begin(), old.evals.begin() + std::min<size_t>(keep, old.evals.size()));
+    while ((int)nc.evals.size() < newk) nc.evals.push_back(nc.evals.empty() ? -1.0 : nc.evals.back());
+    nc.cur = 0;
+    KS_CUDA(cudaStreamSynchronize(s_));  // the old block is freed below
+    ch_[sp] = std::move(nc);
+}
+
 // Mirrors the allocations of the constructor, Poisson::init, Reducer::init, Channel::create, the DIIS pool and the
 // ionic fields; each buffer is counted at cudaMalloc's 2 MiB granularity for large and 512 B for small requests.
 size_t Solver::footprint_bytes(int n, int n_up, int n_dn, const SolverOptions& o, int diis_history, bool pseudo_core) {
@@ -855,8 +874,12 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         const int nocc[2] = {n_up, n_dn};
         int kk[2];
         for (int sp = 0; sp < 2; ++sp) kk[sp] = nocc[sp] > 0 ? nocc[sp] + opt_.n_extra : 0;
-        const bool reuse = warm && have_warm_ && fd_state_ == fd && nocc_[0] == n_up && nocc_[1] == n_dn && ch_[0].k == kk[0] &&
-                           ch_[1].k == kk[1] && state_gen_ == ionic_gen();
+        bool reuse = warm && have_warm_ && fd_state_ == fd && nocc_[0] == n_up && nocc_[1] == n_dn && state_gen_ == ionic_gen();
+        // under Fermi-Dirac a warm block may have grown for its gap witness: it is reused at its size
+        for (int sp = 0; sp < 2 && reuse; ++sp)
+            if (fd && kk[sp] > 0 ? ch_[sp].k < kk[sp] : ch_[sp].k != kk[sp]) reuse = false;
+        if (reuse && fd)
+            for (int sp = 0; sp < 2; ++sp) kk[sp] = ch_[sp].k;
         // columns held to the eigen tolerance: N_sigma, or under Fermi-Dirac the block minus its loose tail (set each step)
         int tight[2] = {nocc[0], nocc[1]};
         double entropy = 0.0, mu[2] = {NAN, NAN};
@@ -1054,6 +1077,46 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 if (step_tol <= eig_lo) max_eig_res = std::max(max_eig_res, tight);
                 last_step_res = std::max(last_step_res, tight);
                 if (es.stop == 2) last_step_maxiter = true;
+            }
+            // Fermi-Dirac gap witness growth (crates/qm/src/scf.rs:810-877, solve_fd): while the block's highest level is
+            // no witness, its extra levels double (at most MAX_WITNESS_GROWTH, and 64 levels in all; a new vector is the
+            // reference's initial orbital with seed 1000 + 2 * index + spin) and the channel is solved again with every
+            // level held to the step's tolerance; once witnessed, the overshoot above the lowest witness is trimmed, never
+            // below the configured N_sigma + n_extra. The witness is read on the Ritz values.
+            for (int sp = 0; sp < 2 && fd; ++sp) {
+                if (nocc[sp] == 0) continue;
+                const int base = nocc[sp] + opt_.n_extra;
+                const int cap = std::min(MAX_WITNESS_GROWTH, 64 - nocc[sp]);
+                for (;;) {
+                    std::vector<double> f(kk[sp]);
+                    double m_sp = 0.0, s_sp = 0.0;
+                    if (!dense::fermi_dirac(ch_[sp].evals.data(), kk[sp], nocc[sp], s.kt, f.data(), m_sp, s_sp))
+                        throw NumericalError("Fermi-Dirac occupations refused (a non-finite level)");
+                    const int extras = kk[sp] - nocc[sp];
+                    if (dense::fd_witness(ch_[sp].evals.data(), kk[sp], nocc[sp], m_sp, s.kt)) {
+                        const int keep = std::max(base, dense::fd_witness_keep(ch_[sp].evals.data(), kk[sp], nocc[sp], m_sp, s.kt));
+                        if (keep < kk[sp]) {
+                            resize_channel(sp, keep, dnuc, nn);
+                            kk[sp] = keep;
+                            tight[sp] = std::min(tight[sp], keep);
+                        }
+                        break;
+                    }
+                    if (extras >= cap) break;  // the witness check at convergence reports the cap
+                    const int grown = std::min(std::max(2 * extras, extras + 1), cap);
+                    resize_channel(sp, nocc[sp] + grown, dnuc, nn);
+                    kk[sp] = nocc[sp] + grown;
+                    ++profile.witness_growths;
+                    KS_CUDA(cudaEventRecord(ev_fork_, s_));
+                    KS_CUDA(cudaStreamWaitEvent(lane_[sp]->s, ev_fork_, 0));
+                    const EigenStats es = lobpcg(ch_[sp], *lane_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, step_tol, EIGEN_MAX_ITER, kk[sp]);
+                    KS_CUDA(cudaEventRecord(lane_[sp]->ev_join, lane_[sp]->s));
+                    KS_CUDA(cudaStreamWaitEvent(s_, lane_[sp]->ev_join, 0));
+                    profile.eigen_iterations += es.iterations;
+                    eig_its += es.iterations;
+                    if (es.restores_exhausted) throw NumericalError("LOBPCG: a Ritz-vector formation failed again after its restores");
+                    last_step_res = std::max(last_step_res, es.max_residual);
+                }
             }
             profile.eigen_s += secs(te);
             // occupations of this step's levels (crates/qm/src/scf.rs:996-1013): Aufbau 1 on the N_sigma lowest (the block

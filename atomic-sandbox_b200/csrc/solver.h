@@ -244,6 +244,7 @@ public:
 
 private:
     void ensure_channel(int spin, int k);
+    void resize_channel(int spin, int newk, const Nuc* dnuc, int nn);
     void gram_checked(Reducer& red, int m, const float* S, int mt, const float* T);
     int readbacks_total() const { return red_.readbacks + lane_[0]->red.readbacks + lane_[1]->red.readbacks; }
     double wait_total() const { return red_.wait_s + lane_[0]->red.wait_s + lane_[1]->red.wait_s; }

@@ -54,7 +54,8 @@ class _Stats(ctypes.Structure):
 class _Profile(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("steps", "readbacks", "eigen_iterations", "poisson_iterations", "eigen_calls",
                                               "diis_resets")] + \
-               [(n, ctypes.c_double) for n in ("wall_s", "start_s", "poisson_s", "eigen_s", "host_dense_s", "sync_wait_s")]
+               [(n, ctypes.c_double) for n in ("wall_s", "start_s", "poisson_s", "eigen_s", "host_dense_s", "sync_wait_s")] + \
+               [("witness_growths", ctypes.c_int)]
 
 
 ABORT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)

@@ -83,6 +83,7 @@ typedef struct {
     double wall_s, start_s, poisson_s, eigen_s;
     double host_dense_s;  /* host time in the f64 Rayleigh-Ritz / DIIS algebra */
     double sync_wait_s;   /* host time blocked on device results (readbacks) */
+    int witness_growths;  /* Fermi-Dirac blocks grown for their gap witness (SolveProfile's witness growth count) */
 } ks_profile;
 
 /* Polled before every SCF step (GpuSolver::solve_with, crates/qm-gpu/src/scf.rs:1208): nonzero abandons the solve. */

@@ -43,3 +43,26 @@ def test_fermi_dirac_needs_extra_levels(ks):
     with ks.GpuSolver(33, 0.25) as so:
         with pytest.raises(ValueError, match="n_extra"):
             so.solve(ks.System([(0.0, 0.0, 0.0, 5)], 3, 2), ks.ScfSettings(occupations="fermi_dirac"))
+
+
+def test_witness_growth_reaches_the_fixed_block_answer(ks):
+    """With one extra level the B atom's up block (2s and the 2p triple) has no gap witness: the block grows by
+    doubling its extra levels (crates/qm/src/scf.rs:810-877) until its top level lies 0.1 Ha above level N and 36 kT
+    above mu, then keeps the overshoot trimmed. F, kT S and the forces equal the fixed-block oracle answer."""
+    case = REC["cases"]["B"]
+    nuc = [tuple(a) for a in case["nuclei"]]
+    settings = ks.ScfSettings(sigma=REC["sigma"], tol=REC["tol"], occupations="fermi_dirac", kt=REC["kt"])
+    with ks.GpuSolver(REC["grid"], REC["h"], n_extra=1) as so:
+        st = so.solve(ks.System(nuc, case["n_up"], case["n_dn"]), settings)
+        grown = so.profile()["witness_growths"]
+        fu, fd = so.occupations()
+        f = so.forces(nuc, REC["sigma"])
+        warm = so.solve(ks.System(nuc, case["n_up"], case["n_dn"]), settings, warm=True)
+    assert grown >= 1
+    assert len(fu) > case["n_up"] + 1
+    ref = case["stats"]
+    assert abs(st["energy"]["total"] - ref["total"]) < 1e-5, (st["energy"]["total"], ref["total"])
+    assert abs(st["energy"]["ts"] - ref["ts"]) < 1e-6
+    assert abs(fu.sum() - case["n_up"]) < 1e-9 and abs(fd.sum() - case["n_dn"]) < 1e-9
+    assert np.abs(f - np.array(case["forces"])).max() < 1e-4
+    assert warm["iterations"] <= 3 and abs(warm["energy"]["total"] - st["energy"]["total"]) < 1e-6, "the grown block is the warm start"
