@@ -1,8 +1,10 @@
 // capi.cu -- the extern "C" boundary (include/ks_cuda.h). Every entry point catches every
 // exception and turns it into a status; nothing here traps or aborts the host process.
 #include <atomic>
+#include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 #include "solver.h"
 
@@ -172,6 +174,72 @@ ks_status ks_vjp(void* solver, const ks_nucleus* nuclei, int n_nuclei, double si
         if (st != KS_OK) h->error = h->solver->error;
         return st;
     });
+}
+
+ks_status ks_solve_batch(ks_batch_job* jobs, int n_jobs, const ks_options* opts, int workers) {
+    if (n_jobs < 0 || (n_jobs > 0 && !jobs) || workers < 1 || workers > 64) {
+        g_create_error = "solve_batch: need jobs, n_jobs >= 0 and 1..64 workers";
+        return KS_INVALID;
+    }
+    SolverOptions o;
+    if (opts) {
+        o.gram_mode = opts->gram_mode;
+        o.n_extra = opts->n_extra;
+        o.init_mode = opts->init_mode;
+    }
+    if (o.n_extra < 0 || o.gram_mode < 0 || o.gram_mode > 1 || o.init_mode < 0 || o.init_mode > 1) {
+        g_create_error = "solve_batch: invalid options";
+        return KS_INVALID;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        g_create_error = "solve_batch: no CUDA device";
+        return KS_DEVICE;
+    }
+    std::atomic<int> next{0};
+    auto worker = [&] {
+        cudaSetDevice(dev);
+        std::unique_ptr<Solver> so;  // kept for the next job on the same grid
+        for (int j = next.fetch_add(1); j < n_jobs; j = next.fetch_add(1)) {
+            ks_batch_job& job = jobs[j];
+            std::memset(&job.stats, 0, sizeof(job.stats));
+            job.error[0] = 0;
+            auto set_error = [&](ks_status st, const std::string& msg) {
+                job.status = st;
+                std::snprintf(job.error, sizeof(job.error), "%s", msg.c_str());
+            };
+            const ks_settings& st = job.settings;
+            if (!valid_grid(job.n, job.h) || !job.nuclei || job.n_nuclei < 1 || !(st.sigma > 0) || !(st.tol > 0) || st.max_iter < 1 ||
+                !(st.eig_tol > 0)) {
+                set_error(KS_INVALID, "invalid job (grid, nuclei or settings)");
+                continue;
+            }
+            try {
+                if (!so || so->layout().n != job.n || so->layout().h != job.h) {
+                    so.reset();
+                    so.reset(new Solver(job.n, job.h, o));
+                }
+                ks_status r = so->solve(job.nuclei, job.n_nuclei, job.n_up, job.n_dn, st, false, nullptr, nullptr, &job.stats);
+                if (r == KS_OK && job.forces3n) r = so->forces(job.nuclei, job.n_nuclei, st.sigma, job.forces3n);
+                if (r != KS_OK) set_error(r, so->error);
+                else job.status = KS_OK;
+            } catch (const NumericalError& e) {
+                set_error(KS_NUMERICAL, e.what());
+                so.reset();
+            } catch (const std::invalid_argument& e) {
+                set_error(KS_INVALID, e.what());
+                so.reset();
+            } catch (const std::exception& e) {
+                set_error(KS_DEVICE, e.what());
+                so.reset();
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < std::min(workers, std::max(n_jobs, 1)); ++w) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    return KS_OK;
 }
 
 ks_status ks_state_counts(const void* solver, int* n_up, int* n_dn) {

@@ -71,6 +71,13 @@ class Progress(ctypes.Structure):
 OBSERVE_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(Progress), ctypes.c_void_p)
 
 
+class _BatchJob(ctypes.Structure):
+    """ks_batch_job (include/ks_cuda.h)."""
+    _fields_ = [("n", ctypes.c_int), ("h", ctypes.c_double), ("nuclei", ctypes.POINTER(Nucleus)), ("n_nuclei", ctypes.c_int),
+                ("n_up", ctypes.c_int), ("n_dn", ctypes.c_int), ("settings", _Settings), ("forces3n", ctypes.POINTER(ctypes.c_double)),
+                ("stats", _Stats), ("status", ctypes.c_int), ("error", ctypes.c_char * 160)]
+
+
 @dataclasses.dataclass
 class Projector:
     """One Kleinman-Bylander projector of a pseudised species: angular momentum l <= 2, E_KB (Ha), the radius of
@@ -183,7 +190,7 @@ EXPORTED = [
     "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
     "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations", "ks_sample_density", "ks_sampling_counters",
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
-    "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed",
+    "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
 ]
 
 
@@ -251,6 +258,7 @@ def lib():
         L.ks_solve_observed.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.POINTER(_Settings), ctypes.c_int, ABORT_FN, ABORT_FN, OBSERVE_FN, ctypes.c_void_p,
                                         ctypes.POINTER(_Stats)]
+        L.ks_solve_batch.argtypes = [ctypes.POINTER(_BatchJob), ctypes.c_int, ctypes.POINTER(_Options), ctypes.c_int]
         L.ks_footprint_bytes.restype = ctypes.c_longlong
         L.ks_footprint_bytes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Options), ctypes.c_int, ctypes.c_int]
         L.ks_density_with_core_to_volume.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, dp]
@@ -515,6 +523,46 @@ class GpuSolver:
         p = _Profile()
         _check(lib().ks_profile_get(self._h, ctypes.byref(p)), self._h)
         return {n: getattr(p, n) for n, _ in _Profile._fields_}
+
+
+def _stats_dict(st):
+    e = st.energy
+    return {
+        "iterations": st.iterations, "delta_rho": st.delta_rho,
+        "energy": {n: getattr(e, n) for n, _ in _Energy._fields_},
+        "boundary_density": st.boundary_density, "max_eigen_residual": st.max_eigen_residual,
+        "poisson_residual": st.poisson_residual, "poisson_iterations": st.poisson_iterations,
+        "electrons": list(st.electrons), "tol_used": st.tol_used, "n_warnings": st.n_warnings,
+        "entropy": st.entropy, "mu": list(st.mu), "partial": bool(st.partial),
+    }
+
+
+def solve_batch(jobs, workers=4, gram_mode=1, n_extra=3, init_mode=1, forces=True):
+    """Independent cold solves (and forces) of many geometries on the current GPU in the library's own thread pool
+    (ks_solve_batch). jobs: dicts with nuclei, n, h, n_up, n_dn and settings (ScfSettings). Returns one dict per job:
+    status (0 = KS_OK), error, stats (as GpuSolver.solve) and forces ((n, 3), or None)."""
+    arr = (_BatchJob * max(len(jobs), 1))()
+    keep = []
+    for i, job in enumerate(jobs):
+        s = job.get("settings") or ScfSettings()
+        nuc = nuclei_array(job["nuclei"])
+        f = np.zeros(3 * len(job["nuclei"]))
+        keep += [nuc, f]
+        a = arr[i]
+        a.n, a.h, a.nuclei, a.n_nuclei = int(job["n"]), float(job["h"]), nuc, len(job["nuclei"])
+        a.n_up, a.n_dn = int(job["n_up"]), int(job["n_dn"])
+        a.settings = _Settings(float(job["h"]) if s.sigma is None else s.sigma, s.tol, s.mixing, s.eig_tol, s.max_iter,
+                               s.diis_history, s.stall_window, 1 if s.occupations == "fermi_dirac" else 0, float(s.kt))
+        a.forces3n = _p(f) if forces else None
+    opts = _Options(int(gram_mode), int(n_extra), int(init_mode), 0)
+    _check(lib().ks_solve_batch(arr, len(jobs), ctypes.byref(opts), int(workers)))
+    out = []
+    for i, job in enumerate(jobs):
+        a = arr[i]
+        ok = a.status == KS_OK
+        out.append({"status": a.status, "error": a.error.decode(errors="replace"), "stats": _stats_dict(a.stats) if ok else None,
+                    "forces": keep[2 * i + 1].reshape(-1, 3).copy() if (ok and forces) else None})
+    return out
 
 
 def footprint_bytes(n, n_up, n_dn, n_extra=0, diis_history=6, with_core=False):

@@ -271,12 +271,25 @@ def velocity_verlet(solver, nuclei, n_up, n_dn, settings, dt_au, steps, velociti
 
 
 # ------------------------------------------------------------------ batches
-def solve_batch(jobs, settings_for=None, workers=4, gram_mode=1, n_extra=3):
+def solve_batch(jobs, settings_for=None, workers=4, gram_mode=1, n_extra=3, native=False):
     """Solves independent geometries concurrently on the current GPU: `workers` host threads, each
-    job on its own GpuSolver (own streams; the C ABI releases the GIL while it runs). jobs: dicts
-    with nuclei, n, h (and optional n_up / n_dn, default neutral lowest multiplicity). Returns
-    (results in job order, wall seconds); each result holds energy, iterations and forces."""
+    job on its own GpuSolver (own streams; the C ABI releases the GIL while it runs), or with native=True
+    the library's own thread pool (ks_solve_batch). jobs: dicts with nuclei, n, h (and optional n_up /
+    n_dn, default neutral lowest multiplicity). Returns (results in job order, wall seconds); each result
+    holds energy, iterations and forces."""
     settings_for = settings_for or (lambda job: ks.ScfSettings(sigma=0.5))
+    if native:
+        full = []
+        for job in jobs:
+            sys_ = ks.neutral_system(job["nuclei"]) if "n_up" not in job else ks.System(job["nuclei"], job["n_up"], job["n_dn"])
+            full.append(dict(job, n_up=sys_.n_up, n_dn=sys_.n_dn, settings=settings_for(job)))
+        t0 = time.perf_counter()
+        out = ks.solve_batch(full, workers=workers, gram_mode=gram_mode, n_extra=n_extra, init_mode=1)
+        wall = time.perf_counter() - t0
+        for r in out:
+            if r["status"] != 0:
+                raise ks.QmError(r["error"])
+        return [{"energy": r["stats"]["energy"]["total"], "iterations": r["stats"]["iterations"], "forces": r["forces"]} for r in out], wall
 
     def run(job):
         sys_ = ks.neutral_system(job["nuclei"]) if "n_up" not in job else ks.System(job["nuclei"], job["n_up"], job["n_dn"])

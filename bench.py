@@ -359,13 +359,13 @@ def bench_batch(args):
         ks_replicas.init("nccl", dev)
     all_jobs = drv.batch_workload(count=args.count)
     jobs = shard(all_jobs, rank, world)  # replicas: each GPU solves its share, no collective on the data path
-    drv.solve_batch(jobs[: args.workers], workers=args.workers)
+    drv.solve_batch(jobs[: args.workers], workers=args.workers, native=args.native)
     if world > 1:
         torch.distributed.barrier()
-    results, wall = drv.solve_batch(jobs, workers=args.workers)
+    results, wall = drv.solve_batch(jobs, workers=args.workers, native=args.native)
     serial = None
     if args.serial:
-        _, serial = drv.solve_batch(jobs, workers=1)
+        _, serial = drv.solve_batch(jobs, workers=1, native=args.native)
     wall, steps = max_over_ranks([wall, 0.0], dev)[0], sum(r["iterations"] for r in results)
     if world > 1:
         torch.distributed.barrier()
@@ -375,7 +375,8 @@ def bench_batch(args):
     line = {"metric": "batch geometries/s (64 molecules, 48^3-96^3, to 1e-6)", "value": len(all_jobs) / wall, "unit": "geometries/s",
             "n_gpus": world, "higher_is_better": True, "wall_s": wall, "workers": args.workers, "count": len(all_jobs),
             "scf_steps_rank0": int(steps), "dtype": "f32", "data": "synthetic (seeded templates)", "scaling": "strong",
-            "config": {"workload": "batch of seeded molecules, per-molecule cubic grids U{48..96}, h=0.25, sigma=0.5, mixed form"},
+            "config": {"workload": "batch of seeded molecules, per-molecule cubic grids U{48..96}, h=0.25, sigma=0.5, mixed form",
+                       "runtime": "library thread pool (ks_solve_batch)" if args.native else "Python threads over GpuSolver"},
             "serial_wall_s": serial, "timing": "wall clock around the batch (many solvers and streams)"}
     print(json.dumps(line), flush=True)
 
@@ -393,6 +394,7 @@ def main():
     ap.add_argument("--workload", default="h2o", choices=["h2o", "batch"], help="batch: the batched sample-generation workload")
     ap.add_argument("--workers", type=int, default=4, help="concurrent solves for --workload batch")
     ap.add_argument("--serial", action="store_true", help="also time the batch one molecule at a time")
+    ap.add_argument("--native", action="store_true", help="--workload batch through the library's thread pool (ks_solve_batch)")
     args = ap.parse_args()
     if args.workload == "batch":
         bench_batch(args)

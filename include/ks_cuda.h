@@ -178,6 +178,28 @@ ks_status ks_forces(void* solver, const ks_nucleus* nuclei, int n_nuclei, double
 ks_status ks_vjp(void* solver, const ks_nucleus* nuclei, int n_nuclei, double sigma, double e_bar, double* dE_dR3n,
                  double* dE_dsigma);
 
+/* One geometry of a batch: its grid, system and settings in; its statistics, forces and status out. */
+typedef struct {
+    int n;                     /* grid points per axis */
+    double h;                  /* spacing (Bohr) */
+    const ks_nucleus* nuclei;
+    int n_nuclei;
+    int n_up, n_dn;
+    ks_settings settings;
+    double* forces3n;          /* out (3 * n_nuclei doubles), or NULL for no forces */
+    ks_stats stats;            /* out */
+    int status;                /* out: the job's ks_status */
+    char error[160];           /* out: the job's message when status != KS_OK */
+} ks_batch_job;
+
+/* Independent cold solves (and forces) of many geometries on the current device: the batched sample generation of the
+   providers (one GpuSolver per grid, crates/providers/src/ks.rs) run by `workers` host threads, each with its own solver
+   and streams, so one geometry's kernels fill the GPU while another waits on a readback. A thread keeps its solver for
+   the next job on the same grid. Each job's result is that of a lone cold ks_solve + ks_forces (bit for bit, whatever
+   the scheduling). Returns KS_OK once every job has run (see each job's status), KS_INVALID for bad arguments.
+   No reference counterpart: the reference solves a batch one geometry at a time. */
+ks_status ks_solve_batch(ks_batch_job* jobs, int n_jobs, const ks_options* opts, int workers);
+
 /* The message of the last failure on this handle (or of ks_solver_create when solver is NULL). */
 const char* ks_last_error(const void* solver);
 
