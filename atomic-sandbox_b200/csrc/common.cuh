@@ -57,6 +57,9 @@ inline void check_cuda(cudaError_t e, const char* what, const char* file, int li
 // Every kernel launch of the library goes through this check, which also counts it
 // (ks_launch_count: the number of this library's kernels launched by the process).
 void count_launch();
+// A CUDA graph replay adds its kernel nodes; while the calling thread captures a graph, its launches are not counted.
+void count_launches(long long n);
+void set_capturing(bool on);
 #define KS_LAUNCH_CHECK() (::ks::count_launch(), ::ks::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }

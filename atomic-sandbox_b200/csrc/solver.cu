@@ -44,7 +44,12 @@ int sm_count() {
 }
 
 static std::atomic<long long> g_launches{0};
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+static thread_local bool t_capturing = false;
+void count_launch() {
+    if (!t_capturing) g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void set_capturing(bool on) { t_capturing = on; }
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 // Zeroes fresh device memory before any stream uses it. cudaMemset runs on the legacy default stream,
@@ -107,7 +112,7 @@ constexpr double STALL_LEVEL_PER_ELECTRON = 1e-3;
 // multigrid (crates/qm-gpu/src/multigrid.rs:62-72)
 constexpr int PRE_SWEEPS = 2, POST_SWEEPS = 2, COARSEST_SWEEPS = 12;
 constexpr double MG_OMEGA = 6.0 / 7.0;
-constexpr int FUSED_MAX_N = 24;
+constexpr int FUSED_MAX_N = 12;
 constexpr int CHECK_EVERY = 5;
 
 double jacobi_omega() {
@@ -412,6 +417,76 @@ void Poisson::cycle(int l, float* x, const float* b) {
 
 void Poisson::vcycle(const float* rhs, float* z) { cycle(0, z, rhs); }
 
+// One PCG iteration between two readbacks (crates/qm-gpu/src/poisson.rs:284-342): ap = L p with p.Ap, the v / r update,
+// z = M^-1 r by one V-cycle, r.z and r.r, the new direction. The scalars stay on the device (parity par).
+void Poisson::iteration(float* v, int par) {
+    double* scal = scal_.d();
+    StencilArgs lapd;
+    lapd.mode = ST_LAPLACIAN;
+    lapd.scale = (float)(1.0 / (L_.h * L_.h));
+    lapd.dot_partials = red_->partials();
+    const int ctas = launch_stencil(L_, p_.tmap, 1, lapd, ap_.at(0), s_);
+    launch_finish(red_->partials(), ctas, 1, -1.0, scal, s_);
+    launch_cg_update(L_.F, v, r_.at(0), p_.at(0), ap_.at(0), scal, 1 + 2 * par, s_);
+    vcycle(r_.at(0), z_.at(0));
+    const int nxt = 1 - par;
+    red_->dots({{r_.at(0), z_.at(0)}, {r_.at(0), r_.at(0)}}, 1, 1.0);
+    KS_CUDA(cudaMemcpyAsync(scal + 1 + 2 * nxt, red_->res() + 1, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+    launch_cg_direction(L_.F, p_.at(0), z_.at(0), scal, 1 + 2 * par, 1 + 2 * nxt, s_);
+    KS_CUDA(cudaMemcpyAsync(red_->res(), scal, sizeof(double), cudaMemcpyDeviceToDevice, s_));
+}
+
+// The iteration's ~40 small launches (the V-cycle's coarse levels are a few microseconds each) replayed as one CUDA
+// graph per (v, parity): captured on first use, then one cudaGraphLaunch per iteration, so the device runs them
+// back to back instead of waiting on the host's launch rate. The graph's kernels count as launches at every replay.
+void Poisson::run_iteration(float* v, int par) {
+    if (graph_v_ != v) {
+        release_graphs();
+        graph_v_ = v;
+    }
+    if (!graph_[par]) {
+        cudaGraph_t g = nullptr;
+        KS_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        set_capturing(true);
+        try {
+            iteration(v, par);
+        } catch (...) {
+            set_capturing(false);
+            cudaStreamEndCapture(s_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        set_capturing(false);
+        KS_CUDA(cudaStreamEndCapture(s_, &g));
+        size_t nodes = 0;
+        KS_CUDA(cudaGraphGetNodes(g, nullptr, &nodes));
+        std::vector<cudaGraphNode_t> list(nodes);
+        KS_CUDA(cudaGraphGetNodes(g, list.data(), &nodes));
+        int kernels = 0;
+        for (auto n : list) {
+            cudaGraphNodeType t;
+            KS_CUDA(cudaGraphNodeGetType(n, &t));
+            if (t == cudaGraphNodeTypeKernel) ++kernels;
+        }
+        const cudaError_t e = cudaGraphInstantiate(&graph_[par], g, 0);
+        cudaGraphDestroy(g);
+        KS_CUDA(e);
+        graph_kernels_[par] = kernels;
+    }
+    KS_CUDA(cudaGraphLaunch(graph_[par], s_));
+    count_launches(graph_kernels_[par]);
+}
+
+void Poisson::release_graphs() {
+    for (auto& g : graph_)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+Poisson::~Poisson() { release_graphs(); }
+
 void Poisson::moments(const float* rho, double* dst) {
     launch_moments(L_, rho, red_->partials(), red_->blocks(), s_);
     launch_finish(red_->partials(), red_->blocks(), 49, L_.h * L_.h * L_.h, dst, s_);
@@ -464,21 +539,11 @@ PoissonStats Poisson::solve(const float* rho, float* v, const CUtensorMap& v_map
     int it = 0, par = 0;
     double last_true = INFINITY;
     int stop = -1;
-    StencilArgs lapd = lap;
     while (residual > tol && it < max_iter) {
         if (!(rz > 0.0))
             throw NumericalError("Poisson: the multigrid preconditioner lost positive-definiteness (r.z = " + std::to_string(rz) + ")");
-        // ap = L p and p.Ap = -sum p (L p)
-        lapd.dot_partials = red_->partials();
-        int ctas = launch_stencil(L_, p_.tmap, 1, lapd, ap_.at(0), s_);
-        launch_finish(red_->partials(), ctas, 1, -1.0, scal, s_);
-        launch_cg_update(L_.F, v, r_.at(0), p_.at(0), ap_.at(0), scal, 1 + 2 * par, s_);
-        vcycle(r_.at(0), z_.at(0));
         const int nxt = 1 - par;
-        red_->dots({{r_.at(0), z_.at(0)}, {r_.at(0), r_.at(0)}}, 1, 1.0);
-        KS_CUDA(cudaMemcpyAsync(scal + 1 + 2 * nxt, red_->res() + 1, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-        launch_cg_direction(L_.F, p_.at(0), z_.at(0), scal, 1 + 2 * par, 1 + 2 * nxt, s_);
-        KS_CUDA(cudaMemcpyAsync(red_->res(), scal, sizeof(double), cudaMemcpyDeviceToDevice, s_));
+        run_iteration(v, par);
         h = red_->read(3);
         const double pap = h[0];
         rz = h[1];

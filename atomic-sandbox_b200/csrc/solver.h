@@ -136,6 +136,10 @@ struct PoissonStats { int iterations = 0; double residual = 0; int stop = 0; int
 // Multigrid-preconditioned CG Hartree solve (crates/qm-gpu/src/poisson.rs:111-343).
 class Poisson {
 public:
+    Poisson() = default;
+    Poisson(const Poisson&) = delete;
+    Poisson& operator=(const Poisson&) = delete;
+    ~Poisson();
     void init(const Layout& L, cudaStream_t s, Reducer* red);
     PoissonStats solve(const float* rho, float* v, const CUtensorMap& v_map, double tol, int max_iter);
     void moments(const float* rho, double* dst_dev);  // 49 f64, dV applied
@@ -145,6 +149,12 @@ private:
     void vcycle(const float* rhs, float* z);
     void cycle(int l, float* x, const float* b);
     void true_residual(const float* v, const CUtensorMap& v_map);
+    void iteration(float* v, int par);
+    void run_iteration(float* v, int par);
+    void release_graphs();
+    cudaGraphExec_t graph_[2] = {nullptr, nullptr};  // one PCG iteration per parity, for the v of graph_v_
+    int graph_kernels_[2] = {0, 0};
+    const float* graph_v_ = nullptr;
     Layout L_;
     cudaStream_t s_ = nullptr;
     Reducer* red_ = nullptr;
