@@ -242,6 +242,27 @@ ks_status ks_solve_batch(ks_batch_job* jobs, int n_jobs, const ks_options* opts,
     return KS_OK;
 }
 
+ks_status ks_set_density_extrapolation(void* solver, int on) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h) return KS_INVALID;
+    h->solver->set_density_extrapolation(on != 0);
+    return KS_OK;
+}
+
+ks_status ks_set_witness_cap(void* solver, int cap) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h) return KS_INVALID;
+    h->solver->set_witness_cap(cap);
+    return KS_OK;
+}
+
+ks_status ks_effective_eig_tol(const void* solver, double eig_tol, double* out) {
+    auto* h = static_cast<const Handle*>(solver);
+    if (!h || !out || !(eig_tol > 0)) return KS_INVALID;
+    *out = h->solver->effective_eig_tol(eig_tol);
+    return KS_OK;
+}
+
 ks_status ks_state_counts(const void* solver, int* n_up, int* n_dn) {
     auto* h = static_cast<const Handle*>(solver);
     if (!h || !h->solver->has_state()) return KS_NO_STATE;

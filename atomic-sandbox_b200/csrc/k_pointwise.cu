@@ -463,6 +463,17 @@ void launch_diis_mix(long long F, int m, const float* const* rho, const float* c
     KS_LAUNCH_CHECK();
 }
 
+// out = max(2 cur - prev, 0) (crates/qm-gpu/src/scf.rs:1146-1163, the density extrapolation in time)
+__global__ void extrapolate_kernel(long long F, const float* __restrict__ cur, const float* __restrict__ prev, float* __restrict__ out) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < F; e += (long long)gridDim.x * blockDim.x)
+        out[e] = fmaxf(2.0f * cur[e] - prev[e], 0.0f);
+}
+
+void launch_extrapolate(long long F, const float* cur, const float* prev, float* out, cudaStream_t s) {
+    extrapolate_kernel<<<stream_blocks(F), TPB, 0, s>>>(F, cur, prev, out);
+    KS_LAUNCH_CHECK();
+}
+
 void launch_scale(long long F, float* x, float a, cudaStream_t s) {
     scale_kernel<<<stream_blocks(F / 4), TPB, 0, s>>>(F / 4, reinterpret_cast<float4*>(x), a);
     KS_LAUNCH_CHECK();

@@ -55,6 +55,8 @@ void launch_density_residual(long long F, int k, const float* psi, const double*
 void launch_diis_mix(long long F, int m, const float* const* rho, const float* const* r, const float* c, const float* a,
                      float* out, cudaStream_t s);
 void launch_scale(long long F, float* x, float a, cudaStream_t s);
+// out = max(2 cur - prev, 0): the linear extrapolation in time of a density
+void launch_extrapolate(long long F, const float* cur, const float* prev, float* out, cudaStream_t s);
 // x *= target / *sum_dev when both are positive (the SCF's charge renormalisation, no host round trip)
 void launch_scale_ratio(long long F, float* x, const double* sum_dev, double target, cudaStream_t s);
 

@@ -102,8 +102,6 @@ constexpr double EIG_GUESS_FACTOR = 1.5;
 constexpr double PARTIAL_OCCUPATION_MIN = 1e-6;
 constexpr double GPU_PARTIAL_TOL = 1e-5;
 constexpr double LOOSE_F_FACTOR = 1e-2;
-// at most this many extra levels per channel grown for the Fermi-Dirac gap witness (crates/qm/src/scf.rs:295)
-constexpr int MAX_WITNESS_GROWTH = 32;
 constexpr double EIG_TOL_FRACTION = 0.0015;
 constexpr double EIG_TOL_MAX = 1e-3;
 constexpr double LAST_STEP_RESIDUAL_FACTOR = 3.0;
@@ -885,6 +883,8 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
     return es;
 }
 
+double Solver::effective_eig_tol(double eig_tol) const { return std::max(eig_tol, EIG_TOL_FLOOR_FACTOR * floor_); }
+
 ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,
                         void* user, ks_stats* out, ks_abort_fn inner_abort, ks_observe_fn observe) {
     auto t0 = clk::now();
@@ -969,10 +969,23 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             launch_deposit_charge(L_, dnuc, nn, 1.0, scale * fu, in_up_.at(0), s_);
             launch_deposit_charge(L_, dnuc, nn, 1.0, scale * fd, in_dn_.at(0), s_);
             launch_fill(vh_.at(0), 0.0f, L_.F, s_);
+        } else if (extrapolate_ && have_prev_) {
+            // rho_in = max(2 rho_t - rho_{t-1}, 0) from the last two converged outputs (crates/qm-gpu/src/scf.rs:1146-1163)
+            launch_extrapolate(L_.F, out_up_.at(0), prev_up_.at(0), in_up_.at(0), s_);
+            launch_extrapolate(L_.F, out_dn_.at(0), prev_dn_.at(0), in_dn_.at(0), s_);
+            profile.extrapolated = 1;
         } else {
             KS_CUDA(cudaMemcpyAsync(in_up_.at(0), out_up_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
             KS_CUDA(cudaMemcpyAsync(in_dn_.at(0), out_dn_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
         }
+        // rho_{t-1} for the next warm start: this solve's starting output, kept only if this solve is warm and converges
+        have_prev_ = false;
+        if (extrapolate_ && reuse) {
+            if (prev_up_.count == 0) { prev_up_.create(L_, 1); prev_dn_.create(L_, 1); }
+            KS_CUDA(cudaMemcpyAsync(prev_up_.at(0), out_up_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+            KS_CUDA(cudaMemcpyAsync(prev_dn_.at(0), out_dn_.at(0), L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+        }
+        const bool keep_prev = extrapolate_;
         nocc_[0] = n_up;
         nocc_[1] = n_dn;
         const float* pc = nullptr;
@@ -1144,14 +1157,14 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 if (es.stop == 2) last_step_maxiter = true;
             }
             // Fermi-Dirac gap witness growth (crates/qm/src/scf.rs:810-877, solve_fd): while the block's highest level is
-            // no witness, its extra levels double (at most MAX_WITNESS_GROWTH, and 64 levels in all; a new vector is the
+            // no witness, its extra levels double (at most the witness cap, 32 by default, and 64 levels in all; a new vector is the
             // reference's initial orbital with seed 1000 + 2 * index + spin) and the channel is solved again with every
             // level held to the step's tolerance; once witnessed, the overshoot above the lowest witness is trimmed, never
             // below the configured N_sigma + n_extra. The witness is read on the Ritz values.
             for (int sp = 0; sp < 2 && fd; ++sp) {
                 if (nocc[sp] == 0) continue;
                 const int base = nocc[sp] + opt_.n_extra;
-                const int cap = std::min(MAX_WITNESS_GROWTH, 64 - nocc[sp]);
+                const int cap = std::min(witness_cap_, 64 - nocc[sp]);
                 for (;;) {
                     std::vector<double> f(kk[sp]);
                     double m_sp = 0.0, s_sp = 0.0;
@@ -1363,7 +1376,8 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             for (int sp = 0; sp < 2; ++sp)
                 if (nocc[sp] > 0 && !dense::fd_witness(ch_[sp].evals.data(), kk[sp], nocc[sp], mu[sp], s.kt)) {
                     error = "no Fermi-Dirac gap witness in the block of " + std::to_string(kk[sp]) + " levels of spin " + std::to_string(sp) +
-                            " (its top level must lie 0.1 Ha above level N and 36 kT above mu): raise n_extra";
+                            " (its top level must lie 0.1 Ha above level N and 36 kT above mu) within the witness cap of " +
+                            std::to_string(witness_cap_) + " extra levels";
                     profile.wall_s = secs(t0);
                     return KS_NUMERICAL;
                 }
@@ -1447,6 +1461,9 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         converged_ = true;
         have_warm_ = true;
         fd_state_ = fd;
+        // prev holds this solve's starting rho_t: the next warm start extrapolates from it (a cold solve keeps none, so
+        // the chain restarts: the next warm start uses rho_t itself)
+        have_prev_ = keep_prev && reuse;
         profile.readbacks = readbacks_total() - rb0;
         profile.host_dense_s = lane_[0]->dense_s + lane_[1]->dense_s;
         profile.sync_wait_s = wait_total() - wait0;

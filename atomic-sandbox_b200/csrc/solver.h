@@ -224,6 +224,16 @@ public:
                     void* user, ks_stats* out, ks_abort_fn inner_abort = nullptr, ks_observe_fn observe = nullptr);
     ks_status forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n);
     ks_status vjp(const ks_nucleus* nuc, int nn, double sigma, double e_bar, double* dE_dR3n, double* dE_dsigma);
+    // rho_in of a warm start extrapolated linearly from the last two converged outputs (crates/qm-gpu/src/scf.rs:1146-1163)
+    void set_density_extrapolation(bool on) {
+        extrapolate_ = on;
+        if (!on) have_prev_ = false;
+    }
+    // at most `cap` extra Fermi-Dirac levels grown per channel for the gap witness, clamped to 1..32 (scf.rs:1122-1129)
+    void set_witness_cap(int cap) { witness_cap_ = std::max(1, std::min(cap, 32)); }
+    int witness_cap() const { return witness_cap_; }
+    // the LOBPCG tolerance the final SCF step converges to: max(eig_tol, 3 x the f32 residual floor) (scf.rs:1713-1715)
+    double effective_eig_tol(double eig_tol) const;
     // the ionic setup of the next solves (n = 0: all-electron); throws std::invalid_argument on bad tables
     void set_ionic(const ks_species* sp, int n) { ionic_.set(sp, n); }
     EigenStats lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked);
@@ -271,6 +281,9 @@ private:
     DevBuf nuc_d_;
     DevBuf sample_pts_, sample_out_, volume_;  // grow-only readout buffers
     Ionic ionic_;                              // the pseudopotential setup (inactive: all-electron)
+    bool extrapolate_ = false, have_prev_ = false;
+    Block prev_up_, prev_dn_;                  // rho_{t-1} of the density extrapolation
+    int witness_cap_ = 32;
     Ionic::Scratch nl_sc_;                     // projections on the solver's stream (energy, forces)
     Block pc_, xcu_, xcd_;                     // partial core of the geometry; v_xc scratch of the forces
     bool nl_on_ = false;                       // H psi includes V_NL (inside a solve under a setup)

@@ -55,7 +55,7 @@ class _Profile(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("steps", "readbacks", "eigen_iterations", "poisson_iterations", "eigen_calls",
                                               "diis_resets")] + \
                [(n, ctypes.c_double) for n in ("wall_s", "start_s", "poisson_s", "eigen_s", "host_dense_s", "sync_wait_s")] + \
-               [("witness_growths", ctypes.c_int)]
+               [("witness_growths", ctypes.c_int), ("extrapolated", ctypes.c_int)]
 
 
 ABORT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
@@ -191,6 +191,7 @@ EXPORTED = [
     "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations", "ks_sample_density", "ks_sampling_counters",
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
+    "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol",
 ]
 
 
@@ -258,6 +259,9 @@ def lib():
         L.ks_solve_observed.argtypes = [ctypes.c_void_p, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.POINTER(_Settings), ctypes.c_int, ABORT_FN, ABORT_FN, OBSERVE_FN, ctypes.c_void_p,
                                         ctypes.POINTER(_Stats)]
+        L.ks_set_density_extrapolation.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ks_set_witness_cap.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ks_effective_eig_tol.argtypes = [ctypes.c_void_p, ctypes.c_double, dp]
         L.ks_solve_batch.argtypes = [ctypes.POINTER(_BatchJob), ctypes.c_int, ctypes.POINTER(_Options), ctypes.c_int]
         L.ks_footprint_bytes.restype = ctypes.c_longlong
         L.ks_footprint_bytes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Options), ctypes.c_int, ctypes.c_int]
@@ -439,6 +443,20 @@ class GpuSolver:
         up, dn = np.empty(self.n ** 3), np.empty(self.n ** 3)
         _check(lib().ks_state_density(self._h, _p(up), _p(dn)), self._h)
         return up, dn
+
+    def set_density_extrapolation(self, on):
+        """Warm starts from max(2 rho_t - rho_{t-1}, 0) of the last two converged outputs (ks_set_density_extrapolation)."""
+        _check(lib().ks_set_density_extrapolation(self._h, 1 if on else 0), self._h)
+
+    def set_witness_cap(self, cap):
+        """At most `cap` (1..32) extra Fermi-Dirac levels per channel (ks_set_witness_cap)."""
+        _check(lib().ks_set_witness_cap(self._h, int(cap)), self._h)
+
+    def effective_eig_tol(self, eig_tol=1e-6):
+        """The LOBPCG tolerance of the final SCF step: max(eig_tol, 3 x the f32 residual floor) (ks_effective_eig_tol)."""
+        v = ctypes.c_double()
+        _check(lib().ks_effective_eig_tol(self._h, float(eig_tol), ctypes.byref(v)), self._h)
+        return v.value
 
     def set_ionic(self, species):
         """The ionic setup of the next solves (ks_set_ionic): a list of Species (pseudised Z), [] = all-electron."""

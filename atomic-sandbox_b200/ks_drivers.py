@@ -230,12 +230,16 @@ class GpuKs:
 
 
 # ------------------------------------------------------------------ molecular dynamics
-def velocity_verlet(solver, nuclei, n_up, n_dn, settings, dt_au, steps, velocities=None, sigma=None, retry_cold=True):
+def velocity_verlet(solver, nuclei, n_up, n_dn, settings, dt_au, steps, velocities=None, sigma=None, retry_cold=True,
+                    extrapolate=False):
     """Born-Oppenheimer MD, kick-drift-kick velocity Verlet (crates/sim/src/integrator.rs): one SCF
     solve per step, warm-started from the previous geometry; a warm solve that fails is retried
     cold, as the reference's provider does (crates/providers/src/ks.rs:590-601). Returns a list of
     per-step records: positions (Bohr), velocities, potential (the total KS energy), kinetic and
-    total energy (Ha), SCF iterations and whether the step needed the cold retry."""
+    total energy (Ha), SCF iterations and whether the step needed the cold retry. extrapolate starts every
+    warm solve from the linear extrapolation in time of the last two converged densities
+    (GpuSolver::set_density_extrapolation, crates/qm-gpu/src/scf.rs:1146-1163)."""
+    solver.set_density_extrapolation(bool(extrapolate))
     sigma = settings.sigma if sigma is None else sigma
     z = [int(a[3]) for a in nuclei]
     m = np.array([mass_au(q) for q in z])[:, None]
@@ -258,7 +262,7 @@ def velocity_verlet(solver, nuclei, n_up, n_dn, settings, dt_au, steps, velociti
         ke = 0.5 * float((m * v * v).sum())
         e_pot = st["energy"]["total"]
         traj.append({"positions": r.copy(), "velocities": v.copy(), "potential": e_pot, "kinetic": ke, "total": e_pot + ke,
-                     "iterations": st["iterations"], "cold_retry": retried})
+                     "iterations": st["iterations"], "cold_retry": retried, "extrapolated": bool(solver.profile()["extrapolated"])})
 
     record()
     for _ in range(steps):

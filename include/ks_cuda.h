@@ -85,6 +85,7 @@ typedef struct {
     double host_dense_s;  /* host time in the f64 Rayleigh-Ritz / DIIS algebra */
     double sync_wait_s;   /* host time blocked on device results (readbacks) */
     int witness_growths;  /* Fermi-Dirac blocks grown for their gap witness (SolveProfile's witness growth count) */
+    int extrapolated;     /* the warm start's input density was extrapolated (SolveProfile::extrapolated) */
 } ks_profile;
 
 /* Polled before every SCF step (GpuSolver::solve_with, crates/qm-gpu/src/scf.rs:1208): nonzero abandons the solve. */
@@ -199,6 +200,18 @@ typedef struct {
    the scheduling). Returns KS_OK once every job has run (see each job's status), KS_INVALID for bad arguments.
    No reference counterpart: the reference solves a batch one geometry at a time. */
 ks_status ks_solve_batch(ks_batch_job* jobs, int n_jobs, const ks_options* opts, int workers);
+
+/* GpuSolver::set_density_extrapolation (crates/qm-gpu/src/scf.rs:1146-1163): with on != 0 a warm solve starts from
+   rho_in = max(2 rho_t - rho_{t-1}, 0), the linear extrapolation in time of the last two converged output densities,
+   instead of rho_t (the caller's contract: equal time steps). rho_{t-1} is dropped by a cold solve, a solve that does not
+   converge (error or abandoned), a change of orbital counts and by turning extrapolation off; an MD caller resets the
+   chain after a discontinuous move by turning it off and on. Orbitals and V_H are warm-started as without it. */
+ks_status ks_set_density_extrapolation(void* solver, int on);
+/* GpuSolver::set_witness_cap (scf.rs:1122-1132): at most cap extra Fermi-Dirac levels per channel, clamped to 1..32. */
+ks_status ks_set_witness_cap(void* solver, int cap);
+/* GpuSolver::effective_eig_tol (scf.rs:1713-1715): the LOBPCG tolerance the SCF's final step converges to,
+   max(eig_tol, 3 x the f32 residual floor of this grid). */
+ks_status ks_effective_eig_tol(const void* solver, double eig_tol, double* out);
 
 /* The message of the last failure on this handle (or of ks_solver_create when solver is NULL). */
 const char* ks_last_error(const void* solver);
