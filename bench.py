@@ -276,9 +276,15 @@ def bench_ours(args):
         launches = (ks.launch_count() - launches0) / max(args.steps, 1)
         barrier()
         prof = solver.profile()
+        # outside the timed region: one observed solve (the observer changes no number) for the energy change of the
+        # last SCF step (its Harris-Foulkes energy against the step before), reported next to dRho
+        steps_seen = []
+        observed = solver.solve(system, settings, observe=steps_seen.append)
+        last_de = abs(steps_seen[-1]["energy"] - steps_seen[-2]["energy"]) if len(steps_seen) > 1 else None
+        same = observed["energy"]["total"] == stats["energy"]["total"]
         solver.close()
         return {"times": times, "walls": walls, "stats": stats, "forces": forces.tolist(), "clocks": clk.summary(), "profile": prof,
-                "rho_bytes": 2 * rho[0].size * 8, "launches": launches}
+                "rho_bytes": 2 * rho[0].size * 8, "launches": launches, "last_step_de": last_de, "observed_same": same}
 
     plain = run_form(0) if args.form in ("both", "plain") else None
     mixed = run_form(1) if args.form in ("both", "mixed") else None
@@ -311,7 +317,8 @@ def bench_ours(args):
                   "mixed_speedup": (statistics.mean(plain["times"]) / statistics.mean(mixed["times"])) if (plain and mixed) else None,
                   "reported_form": "mixed" if mixed is not None else "plain_fp32"},
         "accuracy": {"energy_ha": st["energy"]["total"], "scf_steps": st["iterations"], "delta_rho": st["delta_rho"],
-                     "oracle_fp64_energy_ha": oracle_e, "abs_dE_vs_fp64": abs(st["energy"]["total"] - oracle_e) if oracle_e else None},
+                     "oracle_fp64_energy_ha": oracle_e, "abs_dE_vs_fp64": abs(st["energy"]["total"] - oracle_e) if oracle_e else None,
+                     "last_step_dE_ha": best["last_step_de"], "observed_solve_bitwise_equal": best["observed_same"]},
         "profile": best["profile"],
         "e2e": {"value": e2e_max, "unit": "s", "h2d_bytes_per_step": 32 * len(NUCLEI), "d2h_bytes_per_step": best["rho_bytes"] + 24 * len(NUCLEI)},
         "gpu_launches": best["launches"],
