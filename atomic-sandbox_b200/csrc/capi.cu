@@ -296,12 +296,9 @@ ks_status ks_state_occupations(const void* solver, double* up, double* dn) {
 ks_status ks_state_density(const void* solver, double* rho_up, double* rho_dn) {
     auto* h = const_cast<Handle*>(static_cast<const Handle*>(solver));
     if (!h || !h->solver->has_state()) return KS_NO_STATE;
+    if (!rho_up || !rho_dn) return fail(h, KS_INVALID, "state_density: null output");
     return guarded(h, [&] {
-        const Layout& L = h->solver->layout();
-        Scratch sc(L.n, L.h);
-        KS_CUDA(cudaStreamSynchronize(h->solver->stream()));
-        sc.download_fields(h->solver->rho(0), 1, rho_up);
-        sc.download_fields(h->solver->rho(1), 1, rho_dn);
+        h->solver->density_f64(rho_up, rho_dn);
         return KS_OK;
     });
 }

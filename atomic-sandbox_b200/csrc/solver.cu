@@ -1659,6 +1659,18 @@ void Solver::sample_density(const double* pts3, int count, float* out) {
 }
 
 // crates/qm-gpu/src/scf.rs:1776-1779 (density_f32): the interior of rho_up + rho_dn as stored, f32
+// the two spin densities of the state as f64 n^3 arrays (ks_state_density): one unpack per spin into a grow-only device
+// buffer on the solver's stream and one copy each, without a per-call allocation
+void Solver::density_f64(double* up, double* dn) {
+    const size_t n3 = (size_t)L_.interior();
+    if (dens64_.bytes < 2 * n3 * sizeof(double)) dens64_.alloc(2 * n3 * sizeof(double));
+    launch_unpack(L_, 1, out_up_.at(0), dens64_.d(), s_);
+    launch_unpack(L_, 1, out_dn_.at(0), dens64_.d() + n3, s_);
+    KS_CUDA(cudaMemcpyAsync(up, dens64_.d(), n3 * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    KS_CUDA(cudaMemcpyAsync(dn, dens64_.d() + n3, n3 * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    KS_CUDA(cudaStreamSynchronize(s_));
+}
+
 void Solver::density_f32(float* host_n3) {
     const size_t bytes = (size_t)L_.interior() * sizeof(float);
     if (volume_.bytes < bytes) volume_.alloc(bytes);

@@ -252,6 +252,7 @@ public:
     // readouts of the converged state (crates/qm-gpu/src/sample.rs, scf.rs:1776-1842)
     void sample_density(const double* pts3, int count, float* out);
     void density_f32(float* host_n3);
+    void density_f64(double* up, double* dn);
     void density_to_volume(float* dense_dev, cudaStream_t s, bool with_core = false, double* max_out = nullptr);
     // out_v = V_NL x_v of the ionic setup at nuc (host f64 n^3 each); c = projections; returns the row count
     int apply_nonlocal(const ks_nucleus* nuc, int nn, int count, const double* x, double* out, double* c);
@@ -279,7 +280,7 @@ private:
     struct Entry { Block rho_up, rho_dn, r_up, r_dn; };
     std::vector<Entry> diis_pool_;
     DevBuf nuc_d_;
-    DevBuf sample_pts_, sample_out_, volume_;  // grow-only readout buffers
+    DevBuf sample_pts_, sample_out_, volume_, dens64_;  // grow-only readout buffers
     Ionic ionic_;                              // the pseudopotential setup (inactive: all-electron)
     bool extrapolate_ = false, have_prev_ = false;
     Block prev_up_, prev_dn_;                  // rho_{t-1} of the density extrapolation
