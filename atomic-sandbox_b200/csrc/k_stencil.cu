@@ -14,7 +14,8 @@
 // branches and no ghost storage. An 8-deep ring of planes keeps four planes of prefetch in flight.
 // Each of the 128 threads computes a 2 x 2 block of outputs (two x-neighbours in two adjacent
 // rows) with Blackwell's packed f32x2 arithmetic, keeps the nine z-values of its columns in a
-// register queue that the 9-way unrolled z-loop rotates by renaming (no moves), and reads 4.5
+// register queue that moves up one plane per step (a compact loop body: a 9-way unrolled rotation by
+// renaming overflowed the instruction cache, 'no instruction' being the top stall), and reads 4.5
 // shared-memory words per output. Stores and the V / R reads are coalesced 8-byte accesses.
 #include <algorithm>
 #include <cudaTypedefs.h>
@@ -33,6 +34,9 @@ constexpr int NS = 8;                               // ring depth (planes)
 constexpr int PLANE_FLOATS = HXW * HYW;             // 960
 constexpr unsigned PLANE_BYTES = PLANE_FLOATS * 4;  // 3840 = 30 * 128
 constexpr int THREADS = 128;                        // 16 x-pairs * 8 y-pairs
+// resident CTAs per SM: registers capped at 96 per thread (a few bytes of spill in two modes) for 20 warps per SM;
+// measured on the H2O 95^3 solve: 4 CTAs (126 registers) 213 ms, 5 CTAs 209 ms, 6 CTAs (80 registers) 216 ms
+constexpr int CTAS_PER_SM = 5;
 constexpr long long WAIT_LIMIT = 1LL << 22;         // bounded mbarrier waits (~seconds)
 
 constexpr float C1 = 1.6f, C2 = -0.2f, C3 = 0.025396825396825397f, C4 = -0.0017857142857142857f;
@@ -109,11 +113,10 @@ __device__ __forceinline__ u64 straddle(u64 a, u64 b) { return pack(hi_of(a), lo
 __device__ __forceinline__ u64 lds2(const float* p) { return *reinterpret_cast<const u64*>(p); }
 
 // Second differences of one row's two x-outputs at the centre plane c (ci = the thread's even x
-// in the staged plane), with the row's z-queue q (plane z+d at q[(J + 4 + d) % 9]):
+// in the staged plane), with the row's z-queue q (plane z+d at q[4 + d]):
 // sum_m c_m [dx_m + dy_m + dz_m], smallest coefficients first -- the scalar kernel's order.
-template <int J>
 __device__ __forceinline__ u64 lap_row(const float* c, int ci, const u64 (&q)[9]) {
-    const u64 f0 = q[(J + 4) % 9];
+    const u64 f0 = q[4];
     const u64 xm4 = lds2(c + ci - 4), xm2 = lds2(c + ci - 2), xp2 = lds2(c + ci + 2), xp4 = lds2(c + ci + 4);
     const u64 xp[5] = {0, straddle(f0, xp2), xp2, straddle(xp2, xp4), xp4};
     const u64 xm[5] = {0, straddle(xm2, f0), xm2, straddle(xm4, xm2), xm4};
@@ -122,7 +125,7 @@ __device__ __forceinline__ u64 lap_row(const float* c, int ci, const u64 (&q)[9]
     for (int m = 1; m <= 4; ++m) {
         const u64 dx = add2(sub2(xp[m], f0), sub2(xm[m], f0));
         const u64 dy = add2(sub2(lds2(c + ci + m * HXW), f0), sub2(lds2(c + ci - m * HXW), f0));
-        const u64 dz = add2(sub2(q[(J + 4 + m) % 9], f0), sub2(q[(J + 13 - m) % 9], f0));
+        const u64 dz = add2(sub2(q[4 + m], f0), sub2(q[4 - m], f0));
         d[m] = add2(add2(dx, dy), dz);
     }
     u64 acc = mul2(pack(C4, C4), d[4]);
@@ -139,20 +142,20 @@ struct Tile {
     bool okA, okB, ok2;  // rows A / B in range (and gx < n), gx + 1 < n
 };
 
-// One z-step (output plane z0 + s) with the queue rotation J = s % 9 fixed at compile time.
-template <int MODE, bool DOT, int J>
+// One z-step (output plane z0 + s): the new plane z0 + s + 4 enters the queues at q[8].
+template <int MODE, bool DOT>
 __device__ __forceinline__ void step(const Params& p, const Tile& t, float* ring, uint64_t* bar, u64 (&qa)[9], u64 (&qb)[9], int s,
                                      float lam, float* __restrict__ out, double& dot, const CUtensorMap* tmap, int x0, int y0) {
     const int qn = s + 8;
     mbar_wait(&bar[qn % NS], (unsigned)((qn / NS) & 1), p.err);
     const float* pn = ring + (qn % NS) * PLANE_FLOATS;
-    qa[(J + 8) % 9] = lds2(pn + t.ciA);
-    qb[(J + 8) % 9] = lds2(pn + t.ciA + HXW);
+    qa[8] = lds2(pn + t.ciA);
+    qb[8] = lds2(pn + t.ciA + HXW);
     const float* c = ring + ((s + 4) % NS) * PLANE_FLOATS;
     const u64 sc = pack(p.scale, p.scale);
-    const u64 la = mul2(lap_row<J>(c, t.ciA, qa), sc);
-    const u64 lb = mul2(lap_row<J>(c, t.ciA + HXW, qb), sc);
-    const u64 fa = qa[(J + 4) % 9], fb = qb[(J + 4) % 9];
+    const u64 la = mul2(lap_row(c, t.ciA, qa), sc);
+    const u64 lb = mul2(lap_row(c, t.ciA + HXW, qb), sc);
+    const u64 fa = qa[4], fb = qb[4];
     const long long rowA = ((long long)(t.z0 + s) * p.n + t.gy) * p.P + t.gx;
     const long long rowB = rowA + p.P;
     u64 oa = la, ob = lb;
@@ -204,7 +207,7 @@ __device__ __forceinline__ void step(const Params& p, const Tile& t, float* ring
 }
 
 template <int MODE, bool DOT>
-__global__ void __launch_bounds__(THREADS, 4) stencil_kernel(const __grid_constant__ CUtensorMap tmap, Params p, float* __restrict__ out) {
+__global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __grid_constant__ CUtensorMap tmap, Params p, float* __restrict__ out) {
     extern __shared__ __align__(1024) float ring[];  // NS planes of 40 x 24
     __shared__ __align__(8) uint64_t bar[NS];
 
@@ -258,26 +261,14 @@ __global__ void __launch_bounds__(THREADS, 4) stencil_kernel(const __grid_consta
     const float lam = (MODE == ST_JACOBI) ? (float)p.lambda[t.vec] : 0.0f;
     double dot = 0.0;
     int s = 0;
-    for (; s + 9 <= nz; s += 9) {
-        step<MODE, DOT, 0>(p, t, ring, bar, qa, qb, s + 0, lam, out, dot, &tmap, x0, y0);
-        step<MODE, DOT, 1>(p, t, ring, bar, qa, qb, s + 1, lam, out, dot, &tmap, x0, y0);
-        step<MODE, DOT, 2>(p, t, ring, bar, qa, qb, s + 2, lam, out, dot, &tmap, x0, y0);
-        step<MODE, DOT, 3>(p, t, ring, bar, qa, qb, s + 3, lam, out, dot, &tmap, x0, y0);
-        step<MODE, DOT, 4>(p, t, ring, bar, qa, qb, s + 4, lam, out, dot, &tmap, x0, y0);
-        step<MODE, DOT, 5>(p, t, ring, bar, qa, qb, s + 5, lam, out, dot, &tmap, x0, y0);
-        step<MODE, DOT, 6>(p, t, ring, bar, qa, qb, s + 6, lam, out, dot, &tmap, x0, y0);
-        step<MODE, DOT, 7>(p, t, ring, bar, qa, qb, s + 7, lam, out, dot, &tmap, x0, y0);
-        step<MODE, DOT, 8>(p, t, ring, bar, qa, qb, s + 8, lam, out, dot, &tmap, x0, y0);
+    for (; s < nz; ++s) {
+        step<MODE, DOT>(p, t, ring, bar, qa, qb, s, lam, out, dot, &tmap, x0, y0);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {  // the z-queues move up one plane: q[i] <- q[i + 1]
+            qa[i] = qa[i + 1];
+            qb[i] = qb[i + 1];
+        }
     }
-    // the tail: s % 9 == 0 here, so the rotation continues at J = 0
-    if (s < nz) step<MODE, DOT, 0>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
-    if (s < nz) step<MODE, DOT, 1>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
-    if (s < nz) step<MODE, DOT, 2>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
-    if (s < nz) step<MODE, DOT, 3>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
-    if (s < nz) step<MODE, DOT, 4>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
-    if (s < nz) step<MODE, DOT, 5>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
-    if (s < nz) step<MODE, DOT, 6>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
-    if (s < nz) step<MODE, DOT, 7>(p, t, ring, bar, qa, qb, s++, lam, out, dot, &tmap, x0, y0);
     if (DOT) {
         double sum = block_sum(dot);
         if (threadIdx.x == 0) p.dot_partials[blockIdx.x + (size_t)gridDim.x * blockIdx.y] = sum;
@@ -299,16 +290,16 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 struct Shape { int tiles_x, tiles_y, chunks, zc; };
 
 // The grid: (x, y) tiles x vectors x z-chunks. A CTA's time is about (its planes + prologue) steps
-// whatever else runs (the kernel is latency-bound at 4 CTAs per SM), and the launch takes
+// whatever else runs (the kernel is latency-bound at CTAS_PER_SM CTAs per SM), and the launch takes
 // ceil(CTAs / resident slots) such rounds, so the chunk count minimises waves x (zc + 8 halo planes
-// + ~4 prologue steps). At 95^3 this gives 4 chunks of 24 planes for 8 vectors (576 CTAs, one
-// wave) instead of a wave and a fifth, and one chunk for 64 vectors.
+// + ~4 prologue steps). At 95^3 with 5 CTAs per SM this gives 5 chunks of 19 planes for 8 vectors
+// (720 CTAs, one wave of 740 slots), and one chunk for 64 vectors.
 Shape shape_for(const Layout& L, int count) {
     Shape sh;
     sh.tiles_x = ceil_div(L.n, BX);
     sh.tiles_y = ceil_div(L.n, BY);
     const long long per_chunk = (long long)sh.tiles_x * sh.tiles_y * count;
-    const long long slots = 4LL * sm_count();
+    const long long slots = (long long)CTAS_PER_SM * sm_count();
     long long best = -1;
     for (int c = 1; c <= std::max(1, L.n / 8); ++c) {
         const int zc = ceil_div(L.n, c);
@@ -329,6 +320,8 @@ void launch_mode(const Shape& sh, int count, const CUtensorMap& tmap, const Para
     const int smem = NS * PLANE_BYTES;
     static const bool attr_set = [smem] {
         KS_CUDA(cudaFuncSetAttribute(stencil_kernel<MODE, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        // CTAS_PER_SM rings of 30 KB need the large shared-memory carveout
+        KS_CUDA(cudaFuncSetAttribute(stencil_kernel<MODE, DOT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         return true;
     }();
     (void)attr_set;
