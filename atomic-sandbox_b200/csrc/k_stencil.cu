@@ -291,9 +291,10 @@ struct Shape { int tiles_x, tiles_y, chunks, zc; };
 
 // The grid: (x, y) tiles x vectors x z-chunks. A CTA's time is about (its planes + prologue) steps
 // whatever else runs (the kernel is latency-bound at CTAS_PER_SM CTAs per SM), and the launch takes
-// ceil(CTAs / resident slots) such rounds, so the chunk count minimises waves x (zc + 8 halo planes
-// + ~4 prologue steps). At 95^3 with 5 CTAs per SM this gives 5 chunks of 19 planes for 8 vectors
-// (720 CTAs, one wave of 740 slots), and one chunk for 64 vectors.
+// ceil(CTAs / resident slots) such rounds, so the chunk count minimises waves x (zc + c) with c the
+// fixed cost of a chunk in plane steps (its 8 halo planes, partly hidden behind the other resident
+// CTAs; c = 8 measured best against 12 and 4). At 95^3 with 5 CTAs per SM this gives 5 chunks of 19
+// planes for 8 and 16 vectors (720 and 1440 CTAs) and 3 chunks of 32 planes for 48 and 64 vectors.
 Shape shape_for(const Layout& L, int count) {
     Shape sh;
     sh.tiles_x = ceil_div(L.n, BX);
@@ -305,7 +306,7 @@ Shape shape_for(const Layout& L, int count) {
         const int zc = ceil_div(L.n, c);
         const int cc = ceil_div(L.n, zc);
         const long long waves = (cc * per_chunk + slots - 1) / slots;
-        const long long cost = waves * (zc + 12);
+        const long long cost = waves * (zc + 8);
         if (best < 0 || cost < best) {
             best = cost;
             sh.zc = zc;
