@@ -40,6 +40,28 @@ __global__ void finish_kernel(const double* __restrict__ partials, int blocks, i
     }
 }
 
+// finish_kernel over two descriptors: warps [0, a.nvals) finish a, the next b.nvals warps finish b
+__global__ void finish_pair_kernel(FinishDesc a, FinishDesc b) {
+    int v = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const FinishDesc& d = v < a.nvals ? a : b;
+    if (v >= a.nvals) v -= a.nvals;
+    if (v >= d.nvals) return;
+    double sum = 0.0, comp = 0.0;
+    for (int blk = lane; blk < d.blocks; blk += 32) {
+        double x = d.partials[(size_t)blk * d.nvals + v];
+        double t = sum + x;
+        if (fabs(sum) >= fabs(x)) comp += (sum - t) + x; else comp += (x - t) + sum;
+        sum = t;
+    }
+    double total = warp_sum(sum + comp);
+    if (lane == 0) {
+        int o = v;
+        if (d.trows > 0) o = (v % d.tcols) * d.trows + v / d.tcols;
+        d.out[o] = total * d.scale;
+    }
+}
+
 __global__ void finish_max_kernel(const double* __restrict__ partials, int blocks, double* __restrict__ out) {
     double m = 0.0;
     for (int b = threadIdx.x; b < blocks; b += blockDim.x) m = fmax(m, partials[b]);
@@ -269,6 +291,11 @@ int reduce_blocks(long long F) {
 
 void launch_finish(const double* partials, int blocks, int nvals, double scale, double* out, cudaStream_t s) {
     finish_kernel<<<ceil_div((long long)nvals * 32, 256), 256, 0, s>>>(partials, blocks, nvals, scale, out, 0, 0);
+    KS_LAUNCH_CHECK();
+}
+
+void launch_finish_pair(const FinishDesc& a, const FinishDesc& b, cudaStream_t s) {
+    finish_pair_kernel<<<ceil_div((long long)(a.nvals + b.nvals) * 32, 256), 256, 0, s>>>(a, b);
     KS_LAUNCH_CHECK();
 }
 

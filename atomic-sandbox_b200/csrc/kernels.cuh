@@ -85,6 +85,16 @@ int stencil_ctas(const Layout& L, int count);
 void launch_finish(const double* partials, int blocks, int nvals, double scale, double* out, cudaStream_t s);
 // the same for a rows x cols matrix of values, written transposed (out[c*rows + r])
 void launch_finish_transposed(const double* partials, int blocks, int rows, int cols, double scale, double* out, cudaStream_t s);
+// Two finishes in one launch, each value summed exactly as launch_finish / launch_finish_transposed would (bitwise):
+// trows > 0 writes value r*tcols + c to out[c*trows + r].
+struct FinishDesc {
+    const double* partials = nullptr;
+    int blocks = 0, nvals = 0;
+    double scale = 1.0;
+    double* out = nullptr;
+    int trows = 0, tcols = 0;
+};
+void launch_finish_pair(const FinishDesc& a, const FinishDesc& b, cudaStream_t s);
 // G = S^T [S | T] on the tensor cores (k_gram_tc.cu): partials [gram_tc_blocks(m, mt)][(m + mt) x m] of the
 // transpose D = [S | T]^T S; m <= 64, round8(m) + mt <= 128.
 int gram_tc_blocks(int m, int mt);

@@ -269,6 +269,7 @@ void Lane::init(const Layout& L) {
     KS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     KS_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     red.init(L, s, 1 << 20);
+    norm_part.alloc((size_t)red.blocks() * 64 * sizeof(double));
 }
 
 double* Lane::upload_buffer(size_t doubles) {
@@ -305,7 +306,7 @@ void Reducer::dots(const std::vector<std::pair<const float*, const float*>>& pai
     }
 }
 
-void Reducer::gram(int m, const float* S, int mt, const float* T, int off, double scale) {
+void Reducer::gram(int m, const float* S, int mt, const float* T, int off, double scale, const FinishDesc* extra) {
     if (gram_mode == 1) {
         // tensor cores: partials of D = [S | T]^T S, finished transposed into G = S^T [S | T]
         if (m > 64 || ((m + 7) & ~7) + mt > 128) throw std::invalid_argument("tensor-core Gram: block too large (m <= 64, round8(m) + mt <= 128)");
@@ -313,13 +314,35 @@ void Reducer::gram(int m, const float* S, int mt, const float* T, int off, doubl
         const size_t need = (size_t)blocks * m * (m + mt);
         if (need * sizeof(double) > partials_.bytes) partials_.alloc(need * sizeof(double));
         launch_gram_tc(L_.F, m, S, mt, T, partials_.d(), s_);
-        launch_finish_transposed(partials_.d(), blocks, m + mt, m, scale, res_.d() + off, s_);
+        if (extra) {
+            FinishDesc g;
+            g.partials = partials_.d();
+            g.blocks = blocks;
+            g.nvals = (m + mt) * m;
+            g.scale = scale;
+            g.out = res_.d() + off;
+            g.trows = m + mt;
+            g.tcols = m;
+            launch_finish_pair(g, *extra, s_);
+        } else {
+            launch_finish_transposed(partials_.d(), blocks, m + mt, m, scale, res_.d() + off, s_);
+        }
         return;
     }
     const size_t need = (size_t)gram_blocks_ * m * (m + mt);
     if (need * sizeof(double) > partials_.bytes) partials_.alloc(need * sizeof(double));
     launch_gram(L_.F, m, S, mt, T, partials_.d(), gram_blocks_, s_);
-    launch_finish(partials_.d(), gram_blocks_, m * (m + mt), scale, res_.d() + off, s_);
+    if (extra) {
+        FinishDesc g;
+        g.partials = partials_.d();
+        g.blocks = gram_blocks_;
+        g.nvals = m * (m + mt);
+        g.scale = scale;
+        g.out = res_.d() + off;
+        launch_finish_pair(g, *extra, s_);
+    } else {
+        launch_finish(partials_.d(), gram_blocks_, m * (m + mt), scale, res_.d() + off, s_);
+    }
 }
 
 const double* Reducer::read(int count) {
@@ -659,9 +682,9 @@ void Solver::ensure_channel(int spin, int k) {
     }
 }
 
-void Solver::gram_checked(Reducer& red, int m, const float* S, int mt, const float* T) {
+void Solver::gram_checked(Reducer& red, int m, const float* S, int mt, const float* T, const FinishDesc* extra) {
     red.gram_mode = opt_.gram_mode;
-    red.gram(m, S, mt, T, 0, L_.h * L_.h * L_.h);  // the L2 product <a, b> = h^3 sum a b
+    red.gram(m, S, mt, T, 0, L_.h * L_.h * L_.h, extra);  // the L2 product <a, b> = h^3 sum a b
 }
 
 EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked) {
@@ -745,12 +768,12 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         if (inner_flag_.load()) throw AbortInside();
         Block& S = ch.A[ch.cur];
         // 1. R = HX - theta X with the first Jacobi sweep fused (into Q), then 3 damped sweeps Q -> W -> Q -> W
-        double* norm_partials = lane.red.partials();
         const int nb = lane.red.blocks();
+        if (lane.norm_part.bytes < (size_t)nb * k * sizeof(double)) lane.norm_part.alloc((size_t)nb * k * sizeof(double));
+        double* norm_partials = lane.norm_part.d();  // finished in the Gram's finish launch below
         launch_residual_precond(L_, k, ch.HX.at(0), ch.X(), theta_d, V, lambda_d, diag_t, ch.T.at(0), ch.Q.at(0), norm_partials, nb, lane.s);
         const int m = 2 * k + np;
         const int off_norm = m * 2 * m;
-        launch_finish(norm_partials, nb, k, L_.h * L_.h * L_.h, lane.red.res() + off_norm, lane.s);
         StencilArgs jac;
         jac.mode = ST_JACOBI;
         jac.scale = ham_scale;
@@ -768,7 +791,13 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         // 2. HW and HP in one launch (W and P are contiguous after X)
         apply_h(S, k, k + np, ch.T.at(k));
         // 3. the readback: G = S^T [S | T] and |r_i|^2
-        gram_checked(lane.red, m, S.at(0), m, ch.T.at(0));
+        FinishDesc norms;
+        norms.partials = norm_partials;
+        norms.blocks = nb;
+        norms.nvals = k;
+        norms.scale = L_.h * L_.h * L_.h;
+        norms.out = lane.red.res() + off_norm;
+        gram_checked(lane.red, m, S.at(0), m, ch.T.at(0), &norms);
         const double* g = lane.red.read(off_norm + k);
         const int mc = 2 * m;
         std::vector<double> A((size_t)m * m), B((size_t)m * m);

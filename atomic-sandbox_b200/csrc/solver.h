@@ -52,7 +52,7 @@ public:
     // sum_p a_p b_p * scale for every pair, written to res()[off + i]
     void dots(const std::vector<std::pair<const float*, const float*>>& pairs, int off, double scale);
     // G = scale * S^T [S | T], written to res()[off...] row-major m x (m + mt)
-    void gram(int m, const float* S, int mt, const float* T, int off, double scale = 1.0);
+    void gram(int m, const float* S, int mt, const float* T, int off, double scale = 1.0, const FinishDesc* extra = nullptr);
     double* res() const { return res_.d(); }
     double* partials() const { return partials_.d(); }
     int blocks() const { return blocks_; }
@@ -199,6 +199,7 @@ struct Lane {
     size_t up_cap = 0;
     double dense_s = 0;  // host time in the Rayleigh-Ritz algebra (profile)
     Ionic::Scratch nl;   // the nonlocal operator's projections on this lane's stream
+    DevBuf norm_part;    // per-CTA |r_i|^2 partials of the residual kernel, finished with the Gram
     Lane() = default;
     Lane(const Lane&) = delete;
     Lane& operator=(const Lane&) = delete;
@@ -266,7 +267,7 @@ public:
 private:
     void ensure_channel(int spin, int k);
     void resize_channel(int spin, int newk, const Nuc* dnuc, int nn);
-    void gram_checked(Reducer& red, int m, const float* S, int mt, const float* T);
+    void gram_checked(Reducer& red, int m, const float* S, int mt, const float* T, const FinishDesc* extra = nullptr);
     int readbacks_total() const { return red_.readbacks + lane_[0]->red.readbacks + lane_[1]->red.readbacks; }
     double wait_total() const { return red_.wait_s + lane_[0]->red.wait_s + lane_[1]->red.wait_s; }
     Layout L_;
