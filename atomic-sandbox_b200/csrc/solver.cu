@@ -75,7 +75,6 @@ int* device_error_flag() {
 
 namespace {
 
-constexpr double PI = 3.14159265358979323846;
 const double COEFF0 = -205.0 / 72.0;
 const double COEFF[5] = {-205.0 / 72.0, 8.0 / 5.0, -1.0 / 5.0, 8.0 / 315.0, -1.0 / 560.0};
 
@@ -863,7 +862,6 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         std::vector<double> th, C;
         double alpha = rayleigh_ritz(m, A, B, k, th, C);
         es.alpha_worst = std::max(es.alpha_worst, alpha);
-        int mm = m;
         if (!(alpha <= std::max(ALPHA_MAX, ALPHA_RESIDUAL_FRACTION * stop_res / floor_)) && np > 0) {
             ++es.fallbacks;
             const int m2 = 2 * k;
@@ -875,9 +873,7 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
             C.assign((size_t)m * k, 0.0);
             for (int c = 0; c < k; ++c)
                 for (int i = 0; i < m2; ++i) C[i + (size_t)m * c] = C2[i + (size_t)m2 * c];
-            mm = m2;
         }
-        (void)mm;
         // 5. X_new = S C, P_new = X_new - X (X^T X)^-1 X^T X_new = S C_p
         std::vector<double> bxx((size_t)k * k), rhs((size_t)k * k, 0.0);
         for (int i = 0; i < k; ++i)
