@@ -1,6 +1,6 @@
 // ks_oracle.cpp -- CPU f64 oracle of the Kohn-Sham SCF hot path.
 //
-// TEST INFRASTRUCTURE ONLY (the checker, never the product). A restatement, in plain C++17,
+// TEST INFRASTRUCTURE ONLY (the reference of the tests, never the product). A restatement, in plain C++17,
 // of the reference's f64 CPU solver, crate `qm`:
 //   grid + Neumaier sums      crates/qm/src/grid.rs:1-99
 //   8th-order stencil         crates/qm/src/stencil.rs:21-51

@@ -3,8 +3,8 @@
  *
  * TEST INFRASTRUCTURE ONLY. The oracle is a single-threaded (optionally OpenMP)
  * f64 restatement of the reference's CPU Kohn-Sham solver, crate `qm`
- * (crates/qm/src/{grid,stencil,xc,nuclear,poisson,eigen,scf,forces}.rs). It is the
- * checker of the CUDA solver: only tests/, __graft_entry__.smoke() and bench.py's
+ * (crates/qm/src/{grid,stencil,xc,nuclear,poisson,eigen,scf,forces}.rs). The CUDA
+ * solver is tested against it: only tests/, __graft_entry__.smoke() and bench.py's
  * cpu_baseline / reference arm may load it. The product never calls it.
  *
  * Grid layout of every array here: the reference's `qm::Grid`, idx = i + n*(j + n*k),
