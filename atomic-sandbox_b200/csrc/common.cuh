@@ -12,6 +12,7 @@
 // stride F, which makes one 4-D tensor map (n, n, n, count) cover a whole block.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -64,10 +65,25 @@ void set_capturing(bool on);
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-// Number of SMs of the current device (148 on B200), cached per process.
+// Number of SMs of the current device (148 on B200), cached per device.
 int sm_count();
 // A device int that kernels with bounded waits set to nonzero when a wait gives up; the host reads
-// and clears it after each solve step (allocated once per process).
+// and clears it after each solve step (allocated once per device).
 int* device_error_flag();
+
+// Runs set() once per device for one call site (`done` holds a bit per device index): a kernel's
+// function attributes (its dynamic shared-memory limit, the carveout) belong to the context of the
+// device they were set on, so a solver on a second device of the same process sets them again.
+// Two threads may both run set() the first time; setting an attribute twice is harmless.
+template <class Set>
+void once_per_device(std::atomic<unsigned long long>& done, Set&& set) {
+    int dev = 0;
+    KS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw DeviceError("device index out of range");
+    const unsigned long long bit = 1ull << dev;
+    if (done.load(std::memory_order_acquire) & bit) return;
+    set();
+    done.fetch_or(bit, std::memory_order_acq_rel);
+}
 
 }  // namespace ks

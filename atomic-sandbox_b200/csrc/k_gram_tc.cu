@@ -397,12 +397,11 @@ void launch_gram_tc(long long F, int m, const float* S, int mt, const float* T, 
     if (p.R < 2) throw std::invalid_argument("gram_tc: tile ring does not fit");
     p.err = device_error_flag();
     const int smem = fixed + 2 * p.R * p.tbytes;
-    static const bool attr = [] {
+    static std::atomic<unsigned long long> attr_set{0};
+    once_per_device(attr_set, [] {
         KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BUDGET));
         KS_CUDA(cudaFuncSetAttribute(gram_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BUDGET));
-        return true;
-    }();
-    (void)attr;
+    });
     if (m8 <= 32) gram_tc_kernel<32><<<sm_count(), THREADS, smem, s>>>(ms, mtm, p, partials);
     else gram_tc_kernel<64><<<sm_count(), THREADS, smem, s>>>(ms, mtm, p, partials);
     KS_LAUNCH_CHECK();

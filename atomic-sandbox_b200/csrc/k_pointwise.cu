@@ -459,11 +459,10 @@ void launch_block_lincomb(long long F, int m, const float* S, int q, const doubl
     if (q <= 0) return;
     if (m > 64) throw std::invalid_argument("block_lincomb: at most 64 input fields");
     long long F4 = F / 4;
-    static const bool attr = [] {  // 64 fields x LCB float4 of dynamic shared memory at most
+    static std::atomic<unsigned long long> attr_set{0};
+    once_per_device(attr_set, [] {  // 64 fields x LCB float4 of dynamic shared memory at most
         KS_CUDA(cudaFuncSetAttribute(block_lincomb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * LCB * 16));
-        return true;
-    }();
-    (void)attr;
+    });
     dim3 grid((unsigned)((F4 + LCB - 1) / LCB), ceil_div(q, QG));
     block_lincomb_kernel<<<grid, LCB, (size_t)m * LCB * 16, s>>>(F4, m, reinterpret_cast<const ulonglong2*>(S), q, C,
                                                                  reinterpret_cast<ulonglong2*>(out), split, gap, device_error_flag());

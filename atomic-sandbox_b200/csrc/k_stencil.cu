@@ -319,13 +319,12 @@ Shape shape_for(const Layout& L, int count) {
 template <int MODE, bool DOT>
 void launch_mode(const Shape& sh, int count, const CUtensorMap& tmap, const Params& p, float* out, cudaStream_t s) {
     const int smem = NS * PLANE_BYTES;
-    static const bool attr_set = [smem] {
+    static std::atomic<unsigned long long> attr_set{0};
+    once_per_device(attr_set, [smem] {
         KS_CUDA(cudaFuncSetAttribute(stencil_kernel<MODE, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         // CTAS_PER_SM rings of 30 KB need the large shared-memory carveout
         KS_CUDA(cudaFuncSetAttribute(stencil_kernel<MODE, DOT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        return true;
-    }();
-    (void)attr_set;
+    });
     dim3 grid(sh.tiles_x * sh.tiles_y * sh.chunks, count);
     stencil_kernel<MODE, DOT><<<grid, THREADS, smem, s>>>(tmap, p, out);
     KS_LAUNCH_CHECK();
