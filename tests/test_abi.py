@@ -48,3 +48,38 @@ def test_spin_split_matches_reference_rules(ks):
     assert ks.spin_split(3) == (2, 1)
     assert ks.spin_split(2, 3) == (2, 0)
     assert ks.spin_split(0) == (0, 0)
+
+
+def _count_params(sig):
+    sig = sig.strip()
+    if sig in ("", "void"):
+        return 0
+    depth, n = 0, 1
+    for ch in sig:
+        if ch in "(<[":
+            depth += 1
+        elif ch in ")>]":
+            depth -= 1
+        elif ch == "," and depth == 0:
+            n += 1
+    return n
+
+
+def test_rust_binding_declares_every_symbol():
+    """INTEGRATION.md's Rust extern block declares every entry point of the header, each with the header's
+    parameter count."""
+    header = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    block = doc[doc.index('extern "C" {'):]
+    block = block[:block.index("\n}\n")]
+    seen, wrong = 0, []
+    for m in re.finditer(r"\b(ks_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", header):
+        name, args = m.group(1), m.group(2)
+        r = re.search(r"pub fn " + name + r"\((.*?)\)\s*(->|;)", block, flags=re.S)
+        if not r:
+            wrong.append((name, "not declared"))
+        elif _count_params(args) != _count_params(r.group(1)):
+            wrong.append((name, _count_params(args), _count_params(r.group(1))))
+        seen += 1
+    assert seen == len(declared()), (seen, len(declared()))
+    assert not wrong, wrong
