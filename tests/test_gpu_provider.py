@@ -1,6 +1,5 @@
 """The provider's semantics on the GPU (crates/providers/src/ks.rs GpuKs): the footprint estimate against the device
 memory a solve really takes, warm evaluations on one grid, the rebuild on a grid change and a pseudised scene."""
-import numpy as np
 import pytest
 
 import synthetic_species as ss

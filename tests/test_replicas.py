@@ -5,7 +5,6 @@ import os
 import socket
 import sys
 
-import pytest
 import torch.multiprocessing as mp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
