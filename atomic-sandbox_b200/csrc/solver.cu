@@ -512,7 +512,7 @@ void Poisson::moments(const float* rho, double* dst) {
     launch_finish(red_->partials(), red_->blocks(), 49, L_.h * L_.h * L_.h, dst, s_);
 }
 
-void Poisson::true_residual(const float* v, const CUtensorMap& v_map) {
+void Poisson::true_residual(const CUtensorMap& v_map) {
     StencilArgs a;
     a.mode = ST_LAPLACIAN;
     a.scale = (float)(1.0 / (L_.h * L_.h));
@@ -573,7 +573,7 @@ PoissonStats Poisson::solve(const float* rho, float* v, const CUtensorMap& v_map
         ++it;
         residual = std::sqrt(rr / b_norm2);
         if (it % CHECK_EVERY == 0 && residual > tol) {
-            true_residual(v, v_map);
+            true_residual(v_map);
             double tr = std::sqrt(red_->read(1)[0] / b_norm2);
             if (!std::isfinite(tr)) throw NumericalError("Poisson: non-finite true residual");
             // crates/qm-gpu/src/poisson.rs:188-190
@@ -583,7 +583,7 @@ PoissonStats Poisson::solve(const float* rho, float* v, const CUtensorMap& v_map
         }
     }
     if (stop < 0) stop = residual <= tol ? 0 : 3;
-    true_residual(v, v_map);
+    true_residual(v_map);
     double tr = std::sqrt(red_->read(1)[0] / b_norm2);
     if (!std::isfinite(tr)) throw NumericalError("Poisson: non-finite true residual");
     st.iterations = it;

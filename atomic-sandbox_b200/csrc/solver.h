@@ -148,7 +148,7 @@ private:
     struct Level { MgLevel lv; DevBuf x, b, res, tmp; };
     void vcycle(const float* rhs, float* z);
     void cycle(int l, float* x, const float* b);
-    void true_residual(const float* v, const CUtensorMap& v_map);
+    void true_residual(const CUtensorMap& v_map);  // r = b + L v into ap_, |r|^2 reduced (v is v_map's field)
     void iteration(float* v, int par);
     void run_iteration(float* v, int par);
     void release_graphs();
