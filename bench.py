@@ -167,7 +167,7 @@ def bench_reference(args):
     value = statistics.mean(vals)
     line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (fixed geometry)", "config": CONFIG, "impl": "reference",
+            "data": "synthetic (fixed geometry)", "config": dict(CONFIG, parallelism=f"replicas x{world}"), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": last["sample"]},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": time.perf_counter() - t_start}

@@ -1,0 +1,50 @@
+"""bench.py's reference arm on the CPU: the JSON line's keys and meaning (the oracle port timed on host cores, the same
+metric, unit, direction and config as the CUDA arm), alone and under torchrun, where rank 0 alone prints and the other
+ranks exit 0 without work. CPU only: the arm never touches a GPU."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+
+def _lines(out):
+    return [json.loads(x) for x in out.splitlines() if x.startswith("{")]
+
+
+def _check(line, world):
+    import bench
+    assert line["impl"] == "reference"
+    assert line["metric"] == bench.METRIC and line["unit"] == "s" and line["higher_is_better"] is False
+    assert line["config"] == dict(bench.CONFIG, parallelism=f"replicas x{world}")
+    assert line["value"] > 0 and line["ms_per_step"] == 1000.0 * line["value"]
+    cpu = line["cpu_baseline"]
+    assert cpu["kind"] == "port" and cpu["cores"] >= 1 and cpu["value"] == line["value"] and "oracle" in cpu["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert line["n_gpus"] == world and line["steps"] == 1 and line["warmup"] == 0
+
+
+def test_reference_arm_line():
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0"], cwd=ROOT,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _lines(r.stdout)
+    assert len(lines) == 1
+    _check(lines[0], 1)
+
+
+def test_reference_arm_under_torchrun_prints_once():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+           "--master-port", str(port), "bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"]
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _lines(r.stdout)
+    assert len(lines) == 1, r.stdout[-2000:]
+    _check(lines[0], 2)
