@@ -151,6 +151,32 @@ def cpu_sample(threads, sample_scale=1.0):
     return value, {"t_lobpcg_it_s": t_lob, "t_cg_it_s": t_cg, "sample": sample}
 
 
+def cpu_baseline_entry():
+    """The bench line's cpu_baseline: the oracle on all host threads (the headline CPU figure), the same sample on one
+    thread (the reference's CPU solver runs on one), and the per-stage CPU times behind both: a LOBPCG iteration
+    (k = 5), a Jacobi-CG Poisson iteration and one f64 H psi apply of one 95^3 vector."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import ks_oracle as O
+    threads = os.cpu_count() or 1
+    value, det = cpu_sample(threads)
+    value_1t, det_1t = cpu_sample(1)
+    f = np.random.default_rng(5).uniform(-1.0, 1.0, N ** 3)
+    v = O.nuclear_potential(N, H, NUCLEI, SIGMA)
+    O.hamiltonian(N, H, f, v)
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.hamiltonian(N, H, f, v)
+    t_hpsi = (time.perf_counter() - t0) / reps
+    O.set_threads(threads)
+    return {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": det["sample"],
+            "single_thread": {"value": value_1t, "unit": "s", "cores": 1, "sample": det_1t["sample"]},
+            "stage_s": {"lobpcg_iteration_k5": det["t_lobpcg_it_s"], "poisson_cg_iteration": det["t_cg_it_s"],
+                        "lobpcg_iteration_k5_1t": det_1t["t_lobpcg_it_s"], "poisson_cg_iteration_1t": det_1t["t_cg_it_s"],
+                        "hpsi_one_vector_1t": t_hpsi}}
+
+
 def bench_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -295,8 +321,7 @@ def bench_ours(args):
     roof = hpsi_roofline(torch, ks, peak, peak_source) if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, det = cpu_sample(os.cpu_count() or 1)
-        cpu = {"value": v, "unit": "s", "cores": os.cpu_count() or 1, "kind": "port", "sample": det["sample"]}
+        cpu = cpu_baseline_entry()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

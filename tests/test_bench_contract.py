@@ -48,3 +48,17 @@ def test_reference_arm_under_torchrun_prints_once():
     lines = _lines(r.stdout)
     assert len(lines) == 1, r.stdout[-2000:]
     _check(lines[0], 2)
+
+
+def test_cpu_baseline_entry():
+    """The CUDA arm's cpu_baseline (computed on the CPU): the all-threads figure, the single-thread one and the
+    per-stage times, all positive, with the single-thread sample on one core."""
+    import bench
+    cpu = bench.cpu_baseline_entry()
+    assert cpu["kind"] == "port" and cpu["unit"] == "s" and cpu["cores"] == (os.cpu_count() or 1) and cpu["value"] > 0
+    one = cpu["single_thread"]
+    assert one["cores"] == 1 and one["value"] > 0 and "oracle" in one["sample"]
+    assert set(cpu["stage_s"]) == {"lobpcg_iteration_k5", "poisson_cg_iteration", "lobpcg_iteration_k5_1t",
+                                   "poisson_cg_iteration_1t", "hpsi_one_vector_1t"}
+    assert all(t > 0 for t in cpu["stage_s"].values())
+    json.dumps(cpu)
