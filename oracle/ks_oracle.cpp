@@ -50,6 +50,18 @@ void par_for(long n, F body) {
     for (auto& th : pool) th.join();
 }
 
+// Runs body(i) for i in [0, n) on up to g_threads std::threads, task i on thread i % threads: for a few
+// large independent tasks (each one a serial reduction, such as a Neumaier dot), so again the results do
+// not depend on the thread count.
+template <class F>
+void par_tasks(long n, F body) {
+    const int t = (int)std::min<long>(g_threads, n);
+    if (t <= 1) { for (long i = 0; i < n; ++i) body(i); return; }
+    std::vector<std::thread> pool;
+    for (int w = 0; w < t; ++w) pool.emplace_back([=, &body] { for (long i = w; i < n; i += t) body(i); });
+    for (auto& th : pool) th.join();
+}
+
 using Vec = std::vector<double>;
 
 // ---------------------------------------------------------------- grid (crates/qm/src/grid.rs)
@@ -355,28 +367,33 @@ struct Poisson {
         double q[N_MOM];
         moments(rho, q);
         size_t N = g.len();
-        for (size_t i = 0; i < N; ++i) b[i] = 4.0 * PI * rho[i];
+        par_for((long)N, [&](long i) { b[i] = 4.0 * PI * rho[i]; });
         add_boundary_term(q, b.data());
         apply_a(v.data(), ap.data());
-        for (size_t i = 0; i < N; ++i) r[i] = b[i] - ap[i];
-        double inv_diag = -(g.h * g.h) / (3.0 * COEFF[0]);
+        const double inv_diag = -(g.h * g.h) / (3.0 * COEFF[0]);
+        par_for((long)N, [&](long i) { r[i] = b[i] - ap[i]; z[i] = inv_diag * r[i]; });
         double b_norm = std::fmax(std::sqrt(gdot(g, b, b)), 1e-300);
-        for (size_t i = 0; i < N; ++i) z[i] = inv_diag * r[i];
         p = z;
-        double rz = gdot(g, r, z);
+        double dots[2];  // r.z and r.r: independent serial sums, one task each
+        par_tasks(2, [&](long t) { dots[t] = t == 0 ? gdot(g, r, z) : gdot(g, r, r); });
+        double rz = dots[0];
         int it = 0;
-        residual = std::sqrt(gdot(g, r, r)) / b_norm;
+        residual = std::sqrt(dots[1]) / b_norm;
         while (residual > tol && it < max_iter) {
             apply_a(p.data(), ap.data());
             double pap = gdot(g, p, ap);
             double alpha = rz / pap;
-            for (size_t i = 0; i < N; ++i) { v[i] += alpha * p[i]; r[i] -= alpha * ap[i]; }
-            for (size_t i = 0; i < N; ++i) z[i] = inv_diag * r[i];
-            double rz_new = gdot(g, r, z);
+            par_for((long)N, [&](long i) {
+                v[i] += alpha * p[i];
+                r[i] -= alpha * ap[i];
+                z[i] = inv_diag * r[i];
+            });
+            par_tasks(2, [&](long t) { dots[t] = t == 0 ? gdot(g, r, z) : gdot(g, r, r); });
+            double rz_new = dots[0];
             double beta = rz_new / rz;
             rz = rz_new;
-            for (size_t i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
-            residual = std::sqrt(gdot(g, r, r)) / b_norm;
+            par_for((long)N, [&](long i) { p[i] = z[i] + beta * p[i]; });
+            residual = std::sqrt(dots[1]) / b_norm;  // p's update leaves r as it was
             ++it;
         }
         return it;
@@ -651,11 +668,11 @@ struct Precond {
         double diag_t = -1.5 * COEFF[0] / (g.h * g.h);
         size_t N = g.len();
         inv_d.resize(N);
-        for (size_t i = 0; i < N; ++i) inv_d[i] = 1.0 / std::fmax(diag_t + v[i] - lambda, 0.1);
+        par_for((long)N, [&](long i) { inv_d[i] = 1.0 / std::fmax(diag_t + v[i] - lambda, 0.1); });
     }
     void apply(const double* r, double* w) const {
         size_t N = g.len();
-        for (size_t i = 0; i < N; ++i) w[i] = r[i] * inv_d[i];
+        par_for((long)N, [&](long i) { w[i] = r[i] * inv_d[i]; });
         Vec hw(N);
         for (int s = 1; s < 4; ++s) {   // JACOBI_SWEEPS = 4
             hamiltonian(g, v, w, hw.data());
@@ -670,12 +687,12 @@ void orthonormalise(const Grid& g, std::vector<Vec>& s) {
     size_t N = g.len();
     for (auto& v : s) {
         for (auto& q : kept) {
-            double c = gdot(g, q, v);
-            for (size_t i = 0; i < N; ++i) v[i] -= c * q[i];
+            const double c = gdot(g, q, v);
+            par_for((long)N, [&](long i) { v[i] -= c * q[i]; });
         }
-        double nrm = std::sqrt(gdot(g, v, v));
+        const double nrm = std::sqrt(gdot(g, v, v));
         if (nrm > 1e-12) {
-            for (size_t i = 0; i < N; ++i) v[i] /= nrm;
+            par_for((long)N, [&](long i) { v[i] /= nrm; });
             kept.push_back(std::move(v));
         }
     }
@@ -695,12 +712,13 @@ int lobpcg(const Grid& g, const double* v, std::vector<Vec>& x, Vec& evals, cons
     int iterations = 0;
     max_residual = std::numeric_limits<double>::infinity();
     for (;;) {
-        for (int i = 0; i < k; ++i) { ham(g, v, nl, xs[i].data(), hx[i].data()); evals[i] = gdot(g, xs[i], hx[i]); }
+        for (int i = 0; i < k; ++i) ham(g, v, nl, xs[i].data(), hx[i].data());
+        par_tasks(k, [&](long i) { evals[i] = gdot(g, xs[i], hx[i]); });
         std::vector<Vec> w;
         double max_res = 0.0;
         Vec r(N);
         for (int i = 0; i < k; ++i) {
-            for (size_t j = 0; j < N; ++j) r[j] = hx[i][j] - evals[i] * xs[i][j];
+            par_for((long)N, [&](long j) { r[j] = hx[i][j] - evals[i] * xs[i][j]; });
             double ri = std::sqrt(gdot(g, r, r));
             max_res = std::fmax(max_res, ri);
             if (std::isnan(ri)) max_res = ri;
@@ -720,28 +738,36 @@ int lobpcg(const Grid& g, const double* v, std::vector<Vec>& x, Vec& evals, cons
         std::vector<Vec> hs(m, Vec(N));
         for (int i = 0; i < m; ++i) ham(g, v, nl, s[i].data(), hs[i].data());
         Vec a((size_t)m * m);
+        std::vector<std::pair<int, int>> pairs;
         for (int i = 0; i < m; ++i)
-            for (int j = 0; j <= i; ++j) {
-                double val = gdot(g, s[i], hs[j]);
-                a[(size_t)i * m + j] = val;
-                a[(size_t)j * m + i] = val;
-            }
+            for (int j = 0; j <= i; ++j) pairs.emplace_back(i, j);
+        par_tasks((long)pairs.size(), [&](long t) {  // each entry one serial Neumaier dot
+            const int i = pairs[t].first, j = pairs[t].second;
+            const double val = gdot(g, s[i], hs[j]);
+            a[(size_t)i * m + j] = val;
+            a[(size_t)j * m + i] = val;
+        });
         Vec ev(m), evec((size_t)m * m);
         jacobi_sym_eigen(m, a, ev.data(), evec.data());
         std::vector<int> order(m);
         for (int i = 0; i < m; ++i) order[i] = i;
         std::stable_sort(order.begin(), order.end(), [&](int i, int j) { return ev[i] < ev[j]; });
         std::vector<Vec> new_x(k, Vec(N, 0.0)), new_p(k, Vec(N, 0.0));
-        for (int col = 0; col < k; ++col) {
-            const double* c = evec.data() + (size_t)m * order[col];
-            for (int si = 0; si < m; ++si) {
-                double coef = c[si];
-                if (coef == 0.0) continue;
-                for (size_t j = 0; j < N; ++j) new_x[col][j] += coef * s[si][j];
-                if (si >= k)
-                    for (size_t j = 0; j < N; ++j) new_p[col][j] += coef * s[si][j];
+        // per point, each output sums its terms in input order (si ascending) from 0, as a column-by-column pass does
+        par_for((long)N, [&](long j) {
+            for (int col = 0; col < k; ++col) {
+                const double* c = evec.data() + (size_t)m * order[col];
+                double sx = new_x[col][j], sp = new_p[col][j];
+                for (int si = 0; si < m; ++si) {
+                    const double coef = c[si];
+                    if (coef == 0.0) continue;
+                    sx += coef * s[si][j];
+                    if (si >= k) sp += coef * s[si][j];
+                }
+                new_x[col][j] = sx;
+                new_p[col][j] = sp;
             }
-        }
+        });
         xs = std::move(new_x);
         orthonormalise(g, xs);
         if ((int)xs.size() != k) return -2;
