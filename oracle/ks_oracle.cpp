@@ -128,11 +128,30 @@ void kinetic(const Grid& g, const double* f, double* out) {
     const size_t N = g.len();
     par_for((long)N, [&](long i) { out[i] *= -0.5; });
 }
-// eigen.rs:117-122 LocalHamiltonian::apply
+// eigen.rs:117-122 LocalHamiltonian::apply: kinetic(x) then y += V x, in one pass with the same roundings per point
+// (the Laplacian scaled by 1/h^2, then by -1/2, then V x added)
 void hamiltonian(const Grid& g, const double* v, const double* x, double* y) {
-    kinetic(g, x, y);
-    const size_t N = g.len();
-    par_for((long)N, [&](long i) { y[i] += v[i] * x[i]; });
+    const int n = g.n;
+    const double inv_h2 = 1.0 / (g.h * g.h);
+    const size_t strides[3] = {1, (size_t)n, (size_t)n * n};
+    par_for(n, [&](long k) {
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                size_t id = g.idx(i, j, (int)k);
+                double acc = 3.0 * COEFF[0] * x[id];
+                int pos[3] = {i, j, (int)k};
+                for (int axis = 0; axis < 3; ++axis)
+                    for (int m = 1; m <= 4; ++m) {
+                        double c = COEFF[m];
+                        if (pos[axis] + m < n) acc += c * x[id + m * strides[axis]];
+                        if (pos[axis] >= m) acc += c * x[id - m * strides[axis]];
+                    }
+                double out = acc * inv_h2;
+                out *= -0.5;
+                out += v[id] * x[id];
+                y[id] = out;
+            }
+    });
 }
 
 // ---------------------------------------------------------------- xc (xc.rs:88-207)
