@@ -6,6 +6,7 @@
 #include <string>
 #include <thread>
 #include <vector>
+#include "dense.h"
 #include "solver.h"
 
 using namespace ks;
@@ -590,6 +591,29 @@ ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gr
         std::memcpy(out, g, sizeof(double) * m * (m + mt));
         return KS_OK;
     });
+}
+
+ks_status ks_rayleigh_ritz(int m, const double* a, const double* b, int nk, double* theta, double* c, double* alpha) {
+    if (m < 1 || nk < 1 || nk > m || !a || !b || !theta || !c) return fail(nullptr, KS_INVALID, "invalid arguments");
+    return guarded(nullptr, [&] {
+        const std::vector<double> A(a, a + (size_t)m * m), B(b, b + (size_t)m * m);
+        std::vector<double> th, C;
+        const double amp = rayleigh_ritz(m, A, B, nk, th, C);
+        std::memcpy(theta, th.data(), sizeof(double) * nk);
+        std::memcpy(c, C.data(), sizeof(double) * (size_t)m * nk);
+        if (alpha) *alpha = amp;
+        return KS_OK;
+    });
+}
+
+ks_status ks_fermi_dirac(const double* evals, int k, int n, double kt, double* f, double* mu, double* entropy) {
+    if (k < 0 || n < 0 || (k > 0 && (!evals || !f)) || !mu || !entropy) return fail(nullptr, KS_INVALID, "invalid arguments");
+    double m_ = 0.0, s_ = 0.0;
+    if (!dense::fermi_dirac(evals, k, n, kt, f, m_, s_))
+        return fail(nullptr, KS_INVALID, "fermi_dirac: refused (fewer than n + 1 levels, a non-finite level or kT)");
+    *mu = m_;
+    *entropy = s_;
+    return KS_OK;
 }
 
 ks_status ks_lobpcg(int n, double h, const double* v, int k, double* x, double* evals, double tol, int max_iter, int gram_mode,

@@ -191,7 +191,7 @@ EXPORTED = [
     "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations", "ks_sample_density", "ks_sampling_counters",
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
-    "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol",
+    "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
 ]
 
 
@@ -238,6 +238,8 @@ def lib():
         L.ks_lobpcg.argtypes = [ctypes.c_int, ctypes.c_double, dp, ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                 dp, ip]
         L.ks_multipole_moments.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
+        L.ks_rayleigh_ritz.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp]
+        L.ks_fermi_dirac.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
         L.ks_field_pitch.argtypes = [ctypes.c_int]
         L.ks_launch_count.restype = ctypes.c_longlong
         L.ks_launch_count.argtypes = []
@@ -637,6 +639,29 @@ def multipole_moments(n, h, rho):
     q = np.empty(49)
     _check(lib().ks_multipole_moments(n, h, _p(_f64(rho, n ** 3)), _p(q)))
     return q
+
+
+def rayleigh_ritz(a, b, nk):
+    """The LOBPCG Rayleigh-Ritz step on the host (crates/qm-gpu/src/eigen.rs:515-542): the lowest nk pairs of
+    A c = theta B c. Returns (theta ascending, C as an m x nk array of B-orthonormal columns, alpha)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    m = a.shape[0]
+    if a.shape != (m, m) or b.shape != (m, m):
+        raise ValueError("rayleigh_ritz: A and B must be square and of one size")
+    theta, c, alpha = np.empty(nk), np.empty(m * nk), ctypes.c_double()
+    _check(lib().ks_rayleigh_ritz(m, _p(a), _p(b), int(nk), _p(theta), _p(c), ctypes.byref(alpha)))
+    return theta, c.reshape(nk, m).T.copy(), alpha.value
+
+
+def fermi_dirac(evals, n, kt):
+    """Fermi-Dirac occupations of one channel (crates/qm/src/occupations.rs fermi_dirac), as the solver computes
+    them: (f, mu, S). ValueError on the reference's refusals."""
+    ev = _f64(evals)
+    f = np.empty(max(ev.size, 1))
+    mu, s = ctypes.c_double(), ctypes.c_double()
+    _check(lib().ks_fermi_dirac(_p(ev), ev.size, int(n), float(kt), _p(f), ctypes.byref(mu), ctypes.byref(s)))
+    return f[:ev.size], mu.value, s.value
 
 
 def gram(n, s, t, gram_mode=0):

@@ -279,6 +279,18 @@ ks_status ks_lobpcg(int n, double h, const double* v, int k, double* x, double* 
 /* multipole moments Q_lm = sum rho R_lm dV (crates/qm-gpu/src/poisson.rs:237-244) */
 ks_status ks_multipole_moments(int n, double h, const double* rho, double* q49);
 
+/* ---- host-only parity hooks: the solver's f64 host algebra (no device is touched) ---- */
+/* rayleigh_ritz (crates/qm-gpu/src/eigen.rs:515-542; its test rayleigh_ritz_pairs_survive_a_bad_symmetric_eigen,
+   :1188-1201): the lowest nk pairs of A c = theta B c for symmetric m x m A and B (row-major, B with a positive
+   diagonal); theta ascending, c column-major m x nk (B-orthonormal coefficient vectors), alpha (may be NULL) the
+   coefficient amplification max_i |T y_i|. KS_NUMERICAL on a non-positive diagonal of B or on rank loss (fewer than
+   nk directions above the drop tolerance). */
+ks_status ks_rayleigh_ritz(int m, const double* a, const double* b, int nk, double* theta, double* c, double* alpha);
+/* fermi_dirac (crates/qm/src/occupations.rs): occupations f (in evals' order) of k levels holding n electrons at kt
+   (Ha), the chemical potential mu (NaN for n = 0) and the entropy S. KS_INVALID on the reference's refusals (fewer
+   than n + 1 levels, a non-finite level or kT). */
+ks_status ks_fermi_dirac(const double* evals, int k, int n, double kt, double* f, double* mu, double* entropy);
+
 /* ---- device-pointer entry points for callers that keep fields on the GPU (bench, integrations) ----
    Fields are in the pitched layout: element (i, j, k) at (k*n + j)*P + i, P = ks_field_pitch(n),
    F = n*n*P floats per field, blocks of fields contiguous with stride F; pad columns hold 0. */

@@ -1,0 +1,70 @@
+"""The solver's f64 host algebra through its host-only C-ABI hooks (no device is touched), against the reference's own
+known answers: the Rayleigh-Ritz step on the 23 x 23 problem dumped from a failing reference run
+(tests/golden/rr_i1_{a,b}.txt; crates/qm-gpu/src/eigen.rs:1188-1201 rayleigh_ritz_pairs_survive_a_bad_symmetric_eigen),
+and the Fermi-Dirac occupation rule (crates/qm/src/occupations.rs:474-612), which must also agree with the oracle's
+restatement. CPU only."""
+import os
+
+import numpy as np
+import pytest
+
+import fd_known_answers
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _rr_problem():
+    return (np.loadtxt(os.path.join(GOLDEN, "rr_i1_a.txt")), np.loadtxt(os.path.join(GOLDEN, "rr_i1_b.txt")))
+
+
+def test_rayleigh_ritz_survives_the_bad_symmetric_eigen(ks):
+    """The reference's assertions: every returned coefficient vector's Rayleigh quotient equals its Ritz value to
+    1e-9 and theta_0 = -0.8686699 to 1e-6 (the mispaired decomposition gave +0.7195). Also: theta ascending, the
+    columns B-orthonormal to 1e-9, and the Ritz values those of the full generalised problem (scipy) to 1e-9."""
+    from scipy.linalg import eigh
+    a, b = _rr_problem()
+    assert a.shape == b.shape and a.shape[0] == a.shape[1]
+    theta, c, alpha = ks.rayleigh_ritz(a, b, 8)
+    for k in range(8):
+        ck = c[:, k]
+        ray = (ck @ a @ ck) / (ck @ b @ ck)
+        assert abs(ray - theta[k]) < 1e-9, (k, ray, theta[k])
+    assert abs(theta[0] + 0.8686699) < 1e-6, theta
+    assert np.all(np.diff(theta) >= 0)
+    assert np.max(np.abs(c.T @ b @ c - np.eye(8))) < 1e-9
+    assert np.max(np.abs(theta - eigh(a, b, eigvals_only=True)[:8])) < 1e-9
+    assert alpha >= 1.0 - 1e-12
+
+
+def test_rayleigh_ritz_refusals(ks):
+    """A non-positive norm on B's diagonal and a subspace that lost rank are numerical errors (eigen.rs:522-531);
+    bad sizes are argument errors."""
+    a, b = _rr_problem()
+    bad = b.copy()
+    bad[3, 3] = 0.0
+    with pytest.raises(ks.Numerical):
+        ks.rayleigh_ritz(a, bad, 8)
+    m = 6
+    s = np.random.default_rng(1).standard_normal((m, 3))
+    with pytest.raises(ks.Numerical):  # rank 3 < nk = 4
+        ks.rayleigh_ritz(np.eye(m), s @ s.T + 1e-30 * np.eye(m), 4)
+    with pytest.raises(ValueError):
+        ks.rayleigh_ritz(a, b, a.shape[0] + 1)
+
+
+def test_fermi_dirac_known_answers_of_the_solver(ks):
+    fd_known_answers.check(ks.fermi_dirac)
+
+
+def test_fermi_dirac_matches_the_oracle(ks, oracle):
+    """The solver's rule and the oracle's restatement on 300 random spectra (spreads from 1e-6 to 20 Ha, kT from 1e-4
+    to 0.05 Ha): f and S to 1e-14, mu to 1e-12 absolute."""
+    rng = np.random.default_rng(0xFD)
+    for _ in range(300):
+        k = 2 + int(rng.integers(30))
+        n = 1 + int(rng.integers(k - 1))
+        kt = 1e-4 * 500 ** rng.uniform()
+        evals = -(1e-6 * 2e7 ** rng.uniform()) * rng.uniform(size=k)
+        f1, mu1, s1 = ks.fermi_dirac(evals, n, kt)
+        f2, mu2, s2 = oracle.fermi_dirac(evals, n, kt)
+        assert np.max(np.abs(f1 - f2)) <= 1e-14 and abs(s1 - s2) <= 1e-14 and abs(mu1 - mu2) <= 1e-12, (k, n, kt)
