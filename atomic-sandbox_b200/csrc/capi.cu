@@ -616,6 +616,13 @@ ks_status ks_fermi_dirac(const double* evals, int k, int n, double kt, double* f
     return KS_OK;
 }
 
+ks_status ks_fd_witness(const double* evals, int k, int n, double mu, double kt, int* reached, int* keep) {
+    if (k < 0 || n < 0 || (k > 0 && !evals) || !reached || !keep) return fail(nullptr, KS_INVALID, "invalid arguments");
+    *reached = dense::fd_witness(evals, k, n, mu, kt) ? 1 : 0;
+    *keep = dense::fd_witness_keep(evals, k, n, mu, kt);
+    return KS_OK;
+}
+
 ks_status ks_lobpcg(int n, double h, const double* v, int k, double* x, double* evals, double tol, int max_iter, int gram_mode,
                     double* max_residual, int* iterations) {
     if (!valid_grid(n, h) || !v || k < 1 || !x || !evals || gram_mode < 0 || gram_mode > 1) return fail(nullptr, KS_INVALID, "invalid arguments");

@@ -192,6 +192,7 @@ EXPORTED = [
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
     "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
+    "ks_fd_witness",
 ]
 
 
@@ -240,6 +241,7 @@ def lib():
         L.ks_multipole_moments.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
         L.ks_rayleigh_ritz.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp]
         L.ks_fermi_dirac.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
+        L.ks_fd_witness.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
         L.ks_field_pitch.argtypes = [ctypes.c_int]
         L.ks_launch_count.restype = ctypes.c_longlong
         L.ks_launch_count.argtypes = []
@@ -662,6 +664,15 @@ def fermi_dirac(evals, n, kt):
     mu, s = ctypes.c_double(), ctypes.c_double()
     _check(lib().ks_fermi_dirac(_p(ev), ev.size, int(n), float(kt), _p(f), ctypes.byref(mu), ctypes.byref(s)))
     return f[:ev.size], mu.value, s.value
+
+
+def fd_witness(evals, n, mu, kt):
+    """The solver's gap witness of a Fermi-Dirac block read on its levels (crates/qm/src/occupations.rs
+    witness_reached, witness_keep): (reached, keep)."""
+    ev = _f64(evals)
+    reached, keep = ctypes.c_int(), ctypes.c_int()
+    _check(lib().ks_fd_witness(_p(ev), ev.size, int(n), float(mu), float(kt), ctypes.byref(reached), ctypes.byref(keep)))
+    return bool(reached.value), keep.value
 
 
 def gram(n, s, t, gram_mode=0):

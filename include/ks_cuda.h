@@ -290,6 +290,11 @@ ks_status ks_rayleigh_ritz(int m, const double* a, const double* b, int nk, doub
    (Ha), the chemical potential mu (NaN for n = 0) and the entropy S. KS_INVALID on the reference's refusals (fewer
    than n + 1 levels, a non-finite level or kT). */
 ks_status ks_fermi_dirac(const double* evals, int k, int n, double kt, double* f, double* mu, double* entropy);
+/* The gap witness of a Fermi-Dirac block, read on its k levels (any order) for n electrons at mu and kt:
+   reached = witness_reached (crates/qm/src/occupations.rs:283-292: the top level 0.1 Ha above the n-th lowest and
+   36 kT above mu; always for n = 0), keep = witness_keep on the levels themselves (occupations.rs:372-394: t + 1 for
+   the lowest rank t >= n that passes both arms, t + 2 when rank t + 1 passes too, k when none does or n = 0). */
+ks_status ks_fd_witness(const double* evals, int k, int n, double mu, double kt, int* reached, int* keep);
 
 /* ---- device-pointer entry points for callers that keep fields on the GPU (bench, integrations) ----
    Fields are in the pitched layout: element (i, j, k) at (k*n + j)*P + i, P = ks_field_pitch(n),

@@ -68,3 +68,21 @@ def test_fermi_dirac_matches_the_oracle(ks, oracle):
         f1, mu1, s1 = ks.fermi_dirac(evals, n, kt)
         f2, mu2, s2 = oracle.fermi_dirac(evals, n, kt)
         assert np.max(np.abs(f1 - f2)) <= 1e-14 and abs(s1 - s2) <= 1e-14 and abs(mu1 - mu2) <= 1e-12, (k, n, kt)
+
+
+def test_witness_known_answers(ks):
+    """The reference's witness tests on levels with zero residuals (crates/qm/src/occupations.rs:615-631
+    witness_both_arms; :686-707 witness_keep_trims_the_overshoot, its zero-residual cases), on the solver's rule."""
+    lvl = lambda top: [-0.3, top, -0.5]  # eps_(2) = -0.3, in any order
+    assert not ks.fd_witness(lvl(-0.3 + 0.099), 2, -0.4, 5e-3)[0]   # the gap arm fails
+    assert not ks.fd_witness(lvl(-0.1), 2, -0.1 - 0.105, 3e-3)[0]   # the tail arm fails: 0.105 < 36 kT = 0.108
+    assert ks.fd_witness(lvl(-0.1), 2, -0.1 - 0.2, 3e-3)[0]         # both met
+    assert not ks.fd_witness([-0.5, -0.3], 2, -0.9, 3e-3)[0]        # no level above the n-th
+    assert ks.fd_witness([], 0, 0.0, 3e-3)[0]                       # an empty channel needs none
+    kt, mu = 5e-3, -0.4
+    evals = [-0.5, -0.3, -0.25, -0.1, -0.05, 0.0, 0.3]
+    reached, keep = ks.fd_witness(evals, 1, mu, kt)
+    assert reached and keep == 5      # the witness -0.1 at rank 3 and the passing spare -0.05
+    assert ks.fd_witness(evals[:keep], 1, mu, kt)[0]  # what is kept passes on its own
+    assert ks.fd_witness(evals, 0, mu, kt)[1] == 7    # an empty channel keeps its block
+    assert ks.fd_witness([0.3, -0.5, -0.05, -0.1, 0.0, -0.25, -0.3], 1, mu, kt)[1] == 5  # order does not matter
