@@ -14,6 +14,7 @@ missing or cannot be loaded raises at load time -- there is no CPU fallback.
 """
 import ctypes
 import dataclasses
+import math
 import os
 import subprocess
 
@@ -349,6 +350,11 @@ class GpuSolver:
     GRAM_FP32, GRAM_TENSOR = 0, 1
 
     def __init__(self, n, h, gram_mode=0, n_extra=0, init_mode=0):
+        # the library's own argument checks (ks_solver_create), raised as argument errors before any device work
+        if not (5 <= int(n) <= 1024 and float(h) > 0 and math.isfinite(float(h))):
+            raise ValueError(f"grid: need 5 <= n <= 1024 and h > 0 (got n = {n}, h = {h})")
+        if gram_mode not in (0, 1) or int(n_extra) < 0 or init_mode not in (0, 1):
+            raise ValueError(f"invalid options: gram_mode {gram_mode}, n_extra {n_extra}, init_mode {init_mode}")
         opts = _Options(gram_mode, n_extra, init_mode, 0)
         self._h = lib().ks_solver_create(int(n), float(h), ctypes.byref(opts))
         if not self._h:
