@@ -689,6 +689,10 @@ void Solver::gram_checked(Reducer& red, int m, const float* S, int mt, const flo
 EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked) {
     EigenStats es;
     const int k = ch.k;
+    // LOBPCG_TRACE in the environment, set to any value, prints the reference's per-iteration lines to stderr
+    // (crates/qm-gpu/src/eigen.rs:707, :800, :853, :941); the two spin channels' lines carry their spin
+    static const bool trace = std::getenv("LOBPCG_TRACE") != nullptr;
+    const char* tag = &ch == &ch_[0] ? "[up]" : &ch == &ch_[1] ? "[dn]" : "";
     const int rb0 = lane.red.readbacks;
     const double omega = jacobi_omega();
     const double diag_t = -1.5 * COEFF0 / (L_.h * L_.h);
@@ -832,6 +836,9 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
                 slack += RITZ_FORM_SLACK * (1.0 + std::fabs(theta[i])) + RITZ_FORM_RES * res[i];
             }
             bool bad = !(rise <= slack);
+            if (bad && trace)
+                std::fprintf(stderr, "lobpcg%s it %d: a Ritz vector does not match its Ritz value (rise %.3e, slack %.3e); the step is redone without P\n",
+                             tag, iterations, rise, slack);
             if (bad && es.restores >= MAX_FORM_RESTORES) es.restores_exhausted = true;
             if (bad && es.restores < MAX_FORM_RESTORES) {
                 ++es.restores;
@@ -854,6 +861,12 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
             es.iterations = iterations;
             es.max_residual = max_res;
             es.stop = stop;
+            if (trace) {
+                std::fprintf(stderr, "lobpcg%s exit: iterations %d, max residual %.3e, stop %d, restores %d, fallbacks %d, evals", tag,
+                             iterations, max_res, stop, es.restores, es.fallbacks);
+                for (int i = 0; i < k; ++i) std::fprintf(stderr, " %.10f", lambda[i]);
+                std::fprintf(stderr, "\n");
+            }
             break;
         }
         ++iterations;
@@ -862,6 +875,7 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         std::vector<double> th, C;
         double alpha = rayleigh_ritz(m, A, B, k, th, C);
         es.alpha_worst = std::max(es.alpha_worst, alpha);
+        if (trace) std::fprintf(stderr, "lobpcg%s it %d: max_res %.2e alpha %.2f m %d\n", tag, iterations, max_res, alpha, m);
         if (!(alpha <= std::max(ALPHA_MAX, ALPHA_RESIDUAL_FRACTION * stop_res / floor_)) && np > 0) {
             ++es.fallbacks;
             const int m2 = 2 * k;
@@ -1049,11 +1063,9 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             for (auto& r : gram) r.erase(r.begin());
         };
 
-        // KS_TRACE=1 in the environment prints one line per SCF step to stderr (the reference's trace switch)
-        static const bool trace = [] {
-            const char* t = std::getenv("KS_TRACE");
-            return t && *t && *t != '0';
-        }();
+        // SCF_TRACE in the environment, set to any value, prints one line per SCF step to stderr (the reference's switch,
+        // crates/qm-gpu/src/scf.rs:1281)
+        static const bool trace = std::getenv("SCF_TRACE") != nullptr;
         int iterations = 0;
         double delta_rho = INFINITY, test_tol = s.tol;
         double q_out[2] = {0, 0};
