@@ -12,6 +12,7 @@
 // stride F, which makes one 4-D tensor map (n, n, n, count) cover a whole block.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
@@ -70,6 +71,16 @@ int sm_count();
 // A device int that kernels with bounded waits set to nonzero when a wait gives up; the host reads
 // and clears it after each solve step (allocated once per device).
 int* device_error_flag();
+
+// An NVTX range over a scope: one phase of the solve (a solve, an SCF step, an eigensolve, a Poisson solve, the
+// forces) as a profiler shows it, and what ncu --nvtx filters on. The ranges are per host thread, so the down channel's
+// eigensolve on its own thread nests correctly; with no tool attached a range costs a function call.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Runs set() once per device for one call site (`done` holds a bit per device index): a kernel's
 // function attributes (its dynamic shared-memory limit, the carveout) belong to the context of the

@@ -526,6 +526,7 @@ void Poisson::true_residual(const CUtensorMap& v_map) {
 }
 
 PoissonStats Poisson::solve(const float* rho, float* v, const CUtensorMap& v_map, double tol, int max_iter) {
+    NvtxRange range("ks poisson");
     PoissonStats st;
     const int rb0 = red_->readbacks;
     double* scal = scal_.d();
@@ -687,6 +688,7 @@ void Solver::gram_checked(Reducer& red, int m, const float* S, int mt, const flo
 }
 
 EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked) {
+    NvtxRange range("ks lobpcg");
     EigenStats es;
     const int k = ch.k;
     // LOBPCG_TRACE in the environment, set to any value, prints the reference's per-iteration lines to stderr
@@ -926,6 +928,7 @@ double Solver::effective_eig_tol(double eig_tol) const { return std::max(eig_tol
 
 ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,
                         void* user, ks_stats* out, ks_abort_fn inner_abort, ks_observe_fn observe) {
+    NvtxRange range("ks solve");
     auto t0 = clk::now();
     inner_fn_ = inner_abort;
     inner_user_ = user;
@@ -1094,6 +1097,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         while (iterations < s.max_iter) {
             if (abort_fn && abort_fn(user)) return park("abandoned before SCF step " + std::to_string(iterations + 1));
             ++iterations;
+            NvtxRange step_range("ks scf step");
             // a warm guess is accepted within the 1.5x band only in the convergence phase (the previous step's dRho
             // already below tol); before that only within the step's own tol. This is the reference's rule for its
             // Fermi-Dirac channels (crates/qm-gpu/src/scf.rs module doc, "The guess band only in the convergence
@@ -1520,6 +1524,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
 }
 
 ks_status Solver::forces(const ks_nucleus* nuc, int nn, double sigma, double* out3n) {
+    NvtxRange range("ks forces");
     if (!converged_) { error = "no converged state"; return KS_NO_STATE; }
     if (nn <= 0 || nn > 32 || !nuc || !out3n) { error = "invalid arguments"; return KS_INVALID; }
     if (state_gen_ != 0) return ionic_forces(nuc, nn, sigma, out3n);
