@@ -19,6 +19,7 @@
 // rounding; the eigensolver's rotations inside degenerate clusters may differ (density-invariant).
 #include "ks_oracle.h"
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -700,21 +701,35 @@ struct Precond {
     }
 };
 
-// modified Gram-Schmidt in Grid::dot; drops norm < 1e-12 (eigen.rs:243-255)
+// modified Gram-Schmidt in Grid::dot; drops norm < 1e-12 (eigen.rs:243-255). Each vector's projections run in order,
+// a dot against its current value and then the update, exactly as one loop over the vectors does, so the result is
+// bitwise that of one thread. Across vectors they run as a wavefront on g_threads threads: vector s projects out
+// vector j as soon as j is final (kept or dropped). Threads take the vectors round-robin in increasing order, so the
+// lowest unfinished vector always has every earlier vector final and a thread working on it: no thread waits forever.
 void orthonormalise(const Grid& g, std::vector<Vec>& s) {
-    std::vector<Vec> kept;
-    size_t N = g.len();
-    for (auto& v : s) {
-        for (auto& q : kept) {
+    const int m = (int)s.size();
+    const size_t N = g.len();
+    std::vector<std::atomic<int>> state(m);  // 0 in progress, 1 kept, 2 dropped
+    for (auto& x : state) x.store(0, std::memory_order_relaxed);
+    par_tasks(m, [&](long idx) {
+        Vec& v = s[idx];
+        for (long j = 0; j < idx; ++j) {
+            int st;
+            while ((st = state[j].load(std::memory_order_acquire)) == 0) std::this_thread::yield();
+            if (st != 1) continue;
+            const Vec& q = s[j];
             const double c = gdot(g, q, v);
-            par_for((long)N, [&](long i) { v[i] -= c * q[i]; });
+            for (size_t i = 0; i < N; ++i) v[i] -= c * q[i];
         }
         const double nrm = std::sqrt(gdot(g, v, v));
-        if (nrm > 1e-12) {
-            par_for((long)N, [&](long i) { v[i] /= nrm; });
-            kept.push_back(std::move(v));
-        }
-    }
+        const bool keep = nrm > 1e-12;
+        if (keep)
+            for (size_t i = 0; i < N; ++i) v[i] /= nrm;
+        state[idx].store(keep ? 1 : 2, std::memory_order_release);
+    });
+    std::vector<Vec> kept;
+    for (int i = 0; i < m; ++i)
+        if (state[i].load(std::memory_order_relaxed) == 1) kept.push_back(std::move(s[i]));
     s = std::move(kept);
 }
 
