@@ -200,6 +200,21 @@ def bench_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def profiled_traffic(count, prof=os.path.join(ROOT, "profiles", "stencil_hpsi_95.md")):
+    """DRAM bytes (read + write) of one H psi launch of `count` vectors, from the committed ncu summary of a smaller
+    launch (its `dram_bytes_per_launch` over its `count` vectors), scaled by the vectors: the traffic grows with them
+    (every vector is streamed once). None when the summary is missing or unreadable."""
+    import re
+    if not os.path.exists(prof):
+        return None
+    with open(prof) as f:
+        text = f.read()
+    mb, mc = re.search(r"dram_bytes_per_launch: (\d+)", text), re.search(r"count: (\d+)", text)
+    if not (mb and mc) or int(mc.group(1)) <= 0:
+        return None
+    return int(mb.group(1)) * count / int(mc.group(1))
+
+
 def hpsi_roofline(torch, ks, peak, source, count=64):
     """H psi on a 64-vector block of 95^3 fields (0.44 GB, 3.5x L2): CUDA events on the launching
     stream around 20 back-to-back launches after 3 warm-ups. Algorithmic bytes per launch: psi read
@@ -228,15 +243,7 @@ def hpsi_roofline(torch, ks, peak, source, count=64):
     t = e0.elapsed_time(e1) / 1000.0 / reps
     algo = (8.0 * count + 4.0) * N ** 3
     achieved = algo / t / 1e9
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "stencil_hpsi_95.md")
-    if os.path.exists(prof):
-        import re
-        with open(prof) as f:
-            text = f.read()
-        mb, mc = re.search(r"dram_bytes_per_launch: (\d+)", text), re.search(r"count: (\d+)", text)
-        if mb and mc:
-            traffic = int(mb.group(1)) * count / int(mc.group(1))
+    traffic = profiled_traffic(count)
     del psi, v, out
     return {"bound": "hbm", "kernel": f"stencil_kernel (H psi, {count} x 95^3 block)", "achieved": achieved, "peak": peak,
             "peak_source": source, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,

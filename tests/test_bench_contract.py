@@ -62,3 +62,14 @@ def test_cpu_baseline_entry():
                                    "poisson_cg_iteration_1t", "hpsi_one_vector_1t"}
     assert all(t > 0 for t in cpu["stage_s"].values())
     json.dumps(cpu)
+
+
+def test_profiled_traffic_scales_the_committed_capture():
+    """The roofline's traffic: the committed ncu capture (profiles/stencil_hpsi_95.md, 48 vectors) scaled to the
+    bench's 64-vector launch, and within 5 % of the algorithmic (8k + 4) N^3 bytes (0.98: no re-reads; some of the
+    output is still in L2 at the kernel's end); None without a summary."""
+    import bench
+    t = bench.profiled_traffic(64)
+    algo = (8 * 64 + 4) * 95 ** 3
+    assert t is not None and abs(t / algo - 1.0) < 0.05, (t, algo)
+    assert bench.profiled_traffic(64, prof="/nonexistent/summary.md") is None
