@@ -45,6 +45,9 @@ constexpr int RMAX = 16;                     // ring depth cap
 constexpr int KT = 32;                       // points per stage (one 128-byte swizzle row)
 constexpr int ROWS = 128;                    // MMA M: rows of [S | T] padded
 constexpr int TILE_BYTES = ROWS * KT * 4;    // 16 KB
+// Every TMA load's x coordinate is a multiple of KT points, so KT * 4 bytes must be a multiple of 16 (the TMA rule,
+// whose violation faults the GPU), and the 128-byte swizzle wants rows of exactly 128 bytes.
+static_assert((KT * 4) % 16 == 0 && KT * 4 == 128, "TMA x coordinates and swizzle rows need KT * 4 == 128 bytes");
 constexpr int THREADS = 480;                 // 8 epilogue, 4 split, 1 TMA, 2 MMA warps
 constexpr int FLUSH = 8;                     // stages summed in f32 before an f64 add
 constexpr int NBUF_MAX = 8;                  // hi*hi accumulator buffers in flight (TMEM permitting)

@@ -34,8 +34,17 @@ constexpr int NS = 8;                               // ring depth (planes)
 constexpr int PLANE_FLOATS = HXW * HYW;             // 960
 constexpr unsigned PLANE_BYTES = PLANE_FLOATS * 4;  // 3840 = 30 * 128
 constexpr int THREADS = 128;                        // 16 x-pairs * 8 y-pairs
-// resident CTAs per SM: registers capped at 96 per thread (a few bytes of spill in two modes) for 20 warps per SM;
-// measured on the H2O 95^3 solve: 4 CTAs (126 registers) 213 ms, 5 CTAs 209 ms, 6 CTAs (80 registers) 216 ms
+// The TMA rules the plane loads rely on, checked here because a violation faults the GPU instead of returning an
+// error: the box's inner extent is a multiple of 16 bytes; a load's x coordinate, x0 - 4 with x0 a multiple of BX,
+// times 4 bytes is a multiple of 16 (negative x is allowed for loads and reads the zero fill); each ring plane starts
+// on a 128-byte boundary. The z-queue issues plane s + 12 into the buffer plane s + 4 left, which needs NS = 8.
+static_assert((HXW * 4) % 16 == 0, "TMA box inner extent must be a multiple of 16 bytes");
+static_assert((BX * 4) % 16 == 0 && (4 * 4) % 16 == 0, "TMA x coordinate x0 - 4 must be a multiple of 16 bytes");
+static_assert(PLANE_BYTES % 128 == 0, "ring planes must start on 128-byte boundaries");
+static_assert(NS == 8, "plane s + 12 reuses the buffer of plane s + 4 only with an 8-deep ring");
+static_assert(THREADS == (BX / 2) * (BY / 2), "one thread per 2 x 2 block of outputs");
+// resident CTAs per SM: registers capped at 96 per thread (no spills) for 20 warps per SM; measured on the H2O 95^3
+// solve: 4 CTAs (126 registers) 213 ms, 5 CTAs 209 ms, 6 CTAs (80 registers) 216 ms
 constexpr int CTAS_PER_SM = 5;
 constexpr long long WAIT_LIMIT = 1LL << 22;         // bounded mbarrier waits (~seconds)
 
