@@ -458,6 +458,9 @@ void launch_lincomb(long long F, int count, float* y, const Terms& t, cudaStream
 void launch_block_lincomb(long long F, int m, const float* S, int q, const double* C, float* out, int split, int gap, cudaStream_t s) {
     if (q <= 0) return;
     if (m > 64) throw std::invalid_argument("block_lincomb: at most 64 input fields");
+    // the bulk copies need 16-byte aligned sources and sizes: whole float4 rows of 16-byte aligned fields
+    if (F % 4 != 0 || reinterpret_cast<uintptr_t>(S) % 16 != 0 || reinterpret_cast<uintptr_t>(out) % 16 != 0)
+        throw std::invalid_argument("block_lincomb: fields must be 16-byte aligned with F a multiple of 4 floats");
     long long F4 = F / 4;
     static std::atomic<unsigned long long> attr_set{0};
     once_per_device(attr_set, [] {  // 64 fields x LCB float4 of dynamic shared memory at most
