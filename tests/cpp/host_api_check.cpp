@@ -1,8 +1,10 @@
-// host_api_check.cpp -- checks of the C++ mirror (include/ks_solver.hpp) that need no GPU: argument errors as
+// host_api_check.cpp -- checks of the C++ mirror (include/ks_solver.hpp). Without a GPU: argument errors as
 // InvalidArgument, the solver's host algebra against the reference's own known answers, and, with --no-device on a
-// machine without a CUDA device, the loud failure of a valid solver (Device, no CPU fallback).
+// machine without a CUDA device, the loud failure of a valid solver (Device, no CPU fallback). With --scf on a GPU:
+// the H2 33^3 SCF and forces through qm_gpu::GpuSolver against the reference's pins, and the solver's contract
+// (warm start, abort, coincident nuclei, the cap on SCF steps).
 //
-//   host_api_check <dir holding rr_i1_a.txt and rr_i1_b.txt> [--no-device]
+//   host_api_check <dir holding rr_i1_a.txt and rr_i1_b.txt> [--no-device | --scf]
 //
 // Prints one "ok <check>" line per check and exits 0, or prints "FAIL <check>: <why>" and exits 1.
 #include <cmath>
@@ -112,6 +114,32 @@ void check_arguments() {
     expect(f33 > 0 && f65 > f33, "footprint_bytes grows with the grid");
 }
 
+// The 33^3 Aufbau pins of the reference (crates/qm/src/scf.rs:1276-1279): H2 at (+-0.7, 0, 0), h = sigma = 0.25,
+// tol 1e-6: E = -0.952449176828 Ha and F_x0 = +0.128755968665 Ha/Bohr, here to 1e-5 Ha and 1e-4 Ha/Bohr.
+void check_scf() {
+    using namespace qm_gpu;
+    GpuSolver so(33, 0.25);
+    const System h2{{{{0.7, 0.0, 0.0}, 1}, {{-0.7, 0.0, 0.0}, 1}}, 1, 1};
+    ScfSettings st;
+    st.sigma = 0.25;
+    const ScfStats cold = so.solve(h2, st);
+    expect(std::fabs(cold.energy.total + 0.9524491768275237) < 1e-5, "solve: the H2 33^3 energy pin", std::to_string(cold.energy.total));
+    const std::vector<Vec3> f = so.forces(h2.nuclei, st.sigma);
+    expect(f.size() == 2 && std::fabs(f[0][0] - 0.12875596866453332) < 1e-4, "forces: the H2 33^3 force pin", std::to_string(f[0][0]));
+    const auto ev = so.evals();
+    expect(ev.first.size() == 1 && ev.second.size() == 1 && ev.first[0] == ev.second[0], "evals: one level per spin, equal");
+    const ScfStats warm = so.solve(h2, st, true);
+    expect(warm.iterations < cold.iterations, "solve: a warm start takes fewer steps");
+    expect(throws<Aborted>([&] { so.solve_with(h2, st, false, [] { return true; }); }), "solve_with: should_abort abandons the solve");
+    ScfSettings capped = st;
+    capped.max_iter = 2;
+    GpuSolver fresh(33, 0.25);
+    expect(throws<ScfNotConverged>([&] { fresh.solve(h2, capped); }), "solve: two steps is ScfNotConverged");
+    const System same{{{{0.1, 0.0, 0.0}, 1}, {{0.1, 0.0, 0.0}, 1}}, 1, 1};
+    expect(throws<CoincidentNuclei>([&] { fresh.solve(same, st); }), "solve: coincident nuclei");
+    expect(throws<NoState>([&] { fresh.forces(h2.nuclei, st.sigma); }), "forces: no state after a failed solve");
+}
+
 void check_no_device() {
     expect(throws<qm_gpu::Device>([] { qm_gpu::GpuSolver(33, 0.25, {1, 3, 1}); }), "GpuSolver: no CUDA device is a Device error");
 }
@@ -120,16 +148,18 @@ void check_no_device() {
 
 int main(int argc, char** argv) {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: %s <golden dir> [--no-device]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s <golden dir> [--no-device | --scf]\n", argv[0]);
         return 2;
     }
     const std::string dir = argv[1];
     const bool no_device = argc > 2 && std::string(argv[2]) == "--no-device";
+    const bool scf = argc > 2 && std::string(argv[2]) == "--scf";
     try {
         check_arguments();
         check_rayleigh_ritz(dir);
         check_occupations();
         if (no_device) check_no_device();
+        if (scf) check_scf();
     } catch (const std::exception& e) {
         std::printf("FAIL unexpected exception: %s\n", e.what());
         return 1;
