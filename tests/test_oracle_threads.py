@@ -30,3 +30,26 @@ def test_results_are_bitwise_independent_of_threads(oracle):
     for x, y in zip(a, b):
         assert np.array_equal(np.asarray(x), np.asarray(y))
     assert repr(sorted(sa.items())) == repr(sorted(sb.items()))
+
+
+def test_pseudo_path_is_bitwise_independent_of_threads(oracle):
+    """The pseudised-ion path (V_loc, the partial core, the Kleinman-Bylander operator, its SCF and the five force
+    terms) on 1 and 4 threads, bit for bit."""
+    import synthetic_species as ss
+    n, h, sigma = 25, 0.35, 0.5
+    sp = [ss.oxygen_like(h)]
+    out = []
+    for threads in (1, 4):
+        oracle.set_threads(threads)
+        try:
+            x = np.random.default_rng(3).uniform(-0.5, 0.5, (2, n ** 3))
+            nl, c = oracle.nonlocal_apply(n, h, NUC, sp, x)
+            v_loc = oracle.ionic_local_potential(n, h, NUC, sigma, sp)
+            st, stats = oracle.scf_ionic(n, h, NUC, 4, 4, sp, sigma=sigma, tol=1e-4)
+            f = oracle.forces_ionic(st, NUC, sigma, sp)
+            out.append(([nl, c, v_loc, st.evals()[0], st.evals()[1], f], repr(sorted(stats.items()))))
+        finally:
+            oracle.set_threads(min(8, os.cpu_count() or 1))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+    assert out[0][1] == out[1][1]
