@@ -29,6 +29,10 @@ ks_status fail(Handle* h, ks_status st, const std::string& msg) {
 template <class F>
 ks_status guarded(Handle* h, F body) {
     try {
+        // a solver's calls raise and read that solver's own wait-timeout flag (other calls keep the thread's current
+        // flag, the device's shared one unless a scope is active: host-only hooks then touch no device)
+        std::unique_ptr<ErrorFlagScope> flag_scope;
+        if (h && h->solver) flag_scope.reset(new ErrorFlagScope(h->solver->err_flag()));
         return body();
     } catch (const NumericalError& e) {
         return fail(h, KS_NUMERICAL, e.what());
@@ -41,12 +45,21 @@ ks_status guarded(Handle* h, F body) {
     }
 }
 
-// A throwaway context for the grid-kernel entry points: layout, stream, reducer.
+// A throwaway context for the grid-kernel entry points: layout, stream and its own wait-timeout flag, installed as
+// the thread's current flag for the hook's lifetime and checked when results come back.
 struct Scratch {
     Layout L;
     cudaStream_t s = nullptr;
-    explicit Scratch(int n, double h) : L(Layout::make(n, h)) { KS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    DevBuf flag;
+    std::unique_ptr<ErrorFlagScope> scope;
+    explicit Scratch(int n, double h) : L(Layout::make(n, h)) {
+        KS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        flag.alloc(256);
+        zero_device(flag.p, flag.bytes);
+        scope.reset(new ErrorFlagScope(static_cast<int*>(flag.p)));
+    }
     ~Scratch() {
+        scope.reset();
         if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
     }
     void upload_fields(const double* host, int count, Block& dst) {
@@ -59,7 +72,7 @@ struct Scratch {
         DevBuf tmp((size_t)L.interior() * std::max(count, 1) * sizeof(double));
         launch_unpack(L, count, src, tmp.d(), s);
         KS_CUDA(cudaMemcpyAsync(host, tmp.p, (size_t)L.interior() * count * sizeof(double), cudaMemcpyDeviceToHost, s));
-        KS_CUDA(cudaStreamSynchronize(s));
+        check_device_flag(s);
     }
 };
 
@@ -220,6 +233,7 @@ ks_status ks_solve_batch(ks_batch_job* jobs, int n_jobs, const ks_options* opts,
                     so.reset();
                     so.reset(new Solver(job.n, job.h, o));
                 }
+                ErrorFlagScope flag_scope(so->err_flag());
                 ks_status r = so->solve(job.nuclei, job.n_nuclei, job.n_up, job.n_dn, st, false, nullptr, nullptr, &job.stats);
                 if (r == KS_OK && job.forces3n) r = so->forces(job.nuclei, job.n_nuclei, st.sigma, job.forces3n);
                 if (r != KS_OK) set_error(r, so->error);
@@ -676,6 +690,13 @@ ks_status ks_hpsi_device(void* stream, int n, double h, int count, const float* 
         a.scale = (float)(-0.5 / (h * h));
         a.V = v;
         launch_stencil(L, map, count, a, out, static_cast<cudaStream_t>(stream));
+        return KS_OK;
+    });
+}
+
+ks_status ks_device_status(void* stream) {
+    return guarded(nullptr, [&] {
+        check_device_flag(static_cast<cudaStream_t>(stream));
         return KS_OK;
     });
 }

@@ -68,9 +68,26 @@ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 // Number of SMs of the current device (148 on B200), cached per device.
 int sm_count();
-// A device int that kernels with bounded waits set to nonzero when a wait gives up; the host reads
-// and clears it after each solve step (allocated once per device).
+// The device int that kernels with bounded waits set to nonzero when a wait gives up, as the calling host thread
+// sees it at launch time: the flag an ErrorFlagScope installed on this thread (a solver's own for the duration of
+// its calls, a kernel hook's own), else the device's shared flag, which the device-pointer entry points use and
+// ks_device_status reads. A solver's flag is reset at the start of each solve and read with each readback, so a
+// timeout is reported by the call whose kernels raised it and by no other solver.
 int* device_error_flag();
+class ErrorFlagScope {
+public:
+    explicit ErrorFlagScope(int* flag);
+    ~ErrorFlagScope();
+    ErrorFlagScope(const ErrorFlagScope&) = delete;
+    ErrorFlagScope& operator=(const ErrorFlagScope&) = delete;
+
+private:
+    int* prev_;
+};
+// Synchronises s, reads the calling thread's current flag and clears it; throws DeviceError when a wait gave up.
+void check_device_flag(cudaStream_t s);
+// Zeroes fresh device memory and waits for it (cudaMemset on the legacy stream).
+void zero_device(void* p, size_t bytes);
 
 // An NVTX range over a scope: one phase of the solve (a solve, an SCF step, an eigensolve, a Poisson solve, the
 // forces) as a profiler shows it, and what ncu --nvtx filters on. The ranges are per host thread, so the down channel's

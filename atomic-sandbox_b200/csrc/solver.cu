@@ -60,7 +60,7 @@ void zero_device(void* p, size_t bytes) {
     KS_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
 }
 
-int* device_error_flag() {
+static int* shared_error_flag() {
     static int* flags[64] = {nullptr};
     int dev = 0;
     KS_CUDA(cudaGetDevice(&dev));
@@ -71,6 +71,25 @@ int* device_error_flag() {
         zero_device(flags[dev], sizeof(int));
     }
     return flags[dev];
+}
+
+static thread_local int* t_error_flag = nullptr;
+
+int* device_error_flag() { return t_error_flag ? t_error_flag : shared_error_flag(); }
+
+ErrorFlagScope::ErrorFlagScope(int* flag) : prev_(t_error_flag) { t_error_flag = flag; }
+ErrorFlagScope::~ErrorFlagScope() { t_error_flag = prev_; }
+
+void check_device_flag(cudaStream_t s) {
+    int* flag = device_error_flag();
+    int host = 0;
+    KS_CUDA(cudaMemcpyAsync(&host, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    KS_CUDA(cudaStreamSynchronize(s));
+    if (host) {
+        KS_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
+        KS_CUDA(cudaStreamSynchronize(s));
+        throw DeviceError("a kernel's bounded wait gave up (a bulk or TMA copy did not complete)");
+    }
 }
 
 namespace {
@@ -655,6 +674,8 @@ Solver::Solver(int n, double h, const SolverOptions& o) : L_(Layout::make(n, h))
     KS_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
     KS_CUDA(cudaGetDevice(&dev_));
     KS_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+    err_.alloc(256);
+    zero_device(err_.p, err_.bytes);
     red_.init(L_, s_, 1 << 20);
     for (auto& l : lane_) {
         l.reset(new Lane());
@@ -940,6 +961,10 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
     } clear_inner{this};
     std::memset(out, 0, sizeof(*out));
     profile = ks_profile{};
+    // the solver's own wait-timeout flag: kernels of this solve raise it, its readbacks read it, and a timeout left by an
+    // earlier call is not blamed on this one
+    ErrorFlagScope flag_scope(err_flag());
+    KS_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), s_));
     const int rb0 = readbacks_total();
     const double wait0 = wait_total();
     for (auto& l : lane_) l->dense_s = 0.0;
@@ -1147,6 +1172,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 const bool both = nocc[0] > 0 && nocc[1] > 0;
                 if (both)
                     worker = std::thread([&] {
+                        ErrorFlagScope worker_flag(err_flag());
                         try {
                             KS_CUDA(cudaSetDevice(dev_));
                             run(1);

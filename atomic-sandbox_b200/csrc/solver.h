@@ -263,6 +263,8 @@ public:
     ks_profile profile{};
     Poisson& poisson() { return poisson_; }
     Reducer& reducer() { return red_; }
+    // this solver's wait-timeout flag (device int); its calls install it as the thread's current flag (ErrorFlagScope)
+    int* err_flag() const { return static_cast<int*>(err_.p); }
 
 private:
     void ensure_channel(int spin, int k);
@@ -307,6 +309,7 @@ private:
     bool fd_state_ = false;        // the state was converged under Fermi-Dirac
     DevBuf occ_d_;                 // device copy of the occupations (2 x 64 doubles), density weights
     cudaEvent_t ev_fork_ = nullptr;
+    DevBuf err_;                   // the solver's own wait-timeout flag
     int dev_ = 0;
     double floor_;
 };

@@ -193,7 +193,7 @@ EXPORTED = [
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
     "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
-    "ks_fd_witness",
+    "ks_fd_witness", "ks_device_status",
 ]
 
 
@@ -248,6 +248,7 @@ def lib():
         L.ks_launch_count.argtypes = []
         L.ks_solver_stream.restype = ctypes.c_void_p
         L.ks_solver_stream.argtypes = [ctypes.c_void_p]
+        L.ks_device_status.argtypes = [ctypes.c_void_p]
         L.ks_hpsi_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p]
         L.ks_gram_device_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
@@ -721,3 +722,9 @@ def hpsi_device(stream, n, h, count, psi_ptr, v_ptr, out_ptr):
     """H psi on device pointers in the pitched layout (ks_hpsi_device)."""
     _check(lib().ks_hpsi_device(ctypes.c_void_p(stream), int(n), float(h), int(count), ctypes.c_void_p(psi_ptr),
                                 ctypes.c_void_p(v_ptr), ctypes.c_void_p(out_ptr)))
+
+
+def device_status(stream):
+    """Synchronises `stream` and raises Device when a kernel of the device-pointer entry points gave up a bounded
+    wait since the last check (ks_device_status); the flag is cleared."""
+    _check(lib().ks_device_status(ctypes.c_void_p(stream)))

@@ -304,8 +304,17 @@ int ks_field_pitch(int n);
 void* ks_solver_stream(void* solver);
 /* How many of this library's kernels the process has launched so far (instrumentation). */
 long long ks_launch_count(void);
-/* out_v = -1/2 lap psi_v + V psi_v, v = 0..count-1, enqueued on `stream` (a cudaStream_t, NULL = legacy). */
+/* out_v = -1/2 lap psi_v + V psi_v, v = 0..count-1, enqueued on `stream` (a cudaStream_t, NULL = legacy).
+   Like every device-pointer entry point it returns before its kernel runs, so its status covers the arguments and
+   the launch only; a bounded wait of the kernel that gave up is reported by ks_device_status. */
 ks_status ks_hpsi_device(void* stream, int n, double h, int count, const float* psi, const float* v, float* out);
+/* Wait-timeout status of the device-pointer entry points (ks_hpsi_device, ks_gram_device_noalloc). Their kernels
+   wait on TMA and bulk copies with bounded spins; a wait that gives up raises the current device's shared timeout
+   flag and leaves that launch's output undefined. This call synchronises `stream` (a cudaStream_t, NULL = legacy),
+   reads the flag, clears it, and returns KS_DEVICE (message in ks_last_error(NULL)) when it was raised, else KS_OK.
+   Solvers keep their own flags and report a timeout from the call that hit it. No counterpart in the reference,
+   whose wgpu path has no device-side waits. */
+ks_status ks_device_status(void* stream);
 
 /* G = S^T [S | T] with the CUDA-core Gram (the gram_mode 0 form of ks_gram, bit-for-bit the same result) for
    callers that must not allocate device memory: a host framework whose caching allocator owns the GPU's memory

@@ -66,10 +66,10 @@ def _count_params(sig):
 
 
 def test_rust_binding_declares_every_symbol():
-    """INTEGRATION.md's Rust extern block declares every entry point of the header, each with the header's
-    parameter count."""
+    """The Rust sys crate (rust/qm-b200-sys/src/lib.rs) declares every entry point of the header in its extern block,
+    each with the header's parameter count."""
     header = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    doc = open(os.path.join(ROOT, "rust", "qm-b200-sys", "src", "lib.rs")).read()
     block = doc[doc.index('extern "C" {'):]
     block = block[:block.index("\n}\n")]
     seen, wrong = 0, []
