@@ -436,11 +436,65 @@ ks_status ks_state_orbitals(const void* solver, int spin, double* out) {
     });
 }
 
+ks_status ks_state_import(void* solver, int n_up, int n_dn, int k_up, const double* orbitals_up, const double* evals_up,
+                          int k_dn, const double* orbitals_dn, const double* evals_dn, const double* rho_up,
+                          const double* rho_dn, const double* v_h, int occupations, const double* occ_up, const double* occ_dn) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h) return KS_INVALID;
+    if (occupations < 0 || occupations > 1) return fail(h, KS_INVALID, "state_import: occupations must be 0 or 1");
+    return guarded(h, [&] {
+        const int k[2] = {k_up, k_dn};
+        const double* const orb[2] = {orbitals_up, orbitals_dn};
+        const double* const ev[2] = {evals_up, evals_dn};
+        const double* const occ[2] = {occ_up, occ_dn};
+        h->solver->import_state(n_up, n_dn, k, orb, ev, occ, rho_up, rho_dn, v_h, occupations == 1);
+        return KS_OK;
+    });
+}
+
+ks_status ks_test_poison_parked_density(void* solver) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h) return KS_INVALID;
+    return guarded(h, [&] {
+        h->solver->poison_parked_density();
+        return KS_OK;
+    });
+}
+
+ks_status ks_test_fail_readbacks(void* solver, int skip, int count) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h || skip < 0 || count < 0) return KS_INVALID;
+    h->solver->fail_readbacks(skip, count);
+    return KS_OK;
+}
+
 ks_status ks_profile_get(const void* solver, ks_profile* out) {
     auto* h = static_cast<const Handle*>(solver);
     if (!h || !out) return KS_INVALID;
     *out = h->solver->profile;
     return KS_OK;
+}
+
+ks_status ks_set_kernel_timing(void* solver, int on) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h) return KS_INVALID;
+    return guarded(h, [&] {
+        h->solver->timer().enable(on != 0);
+        return KS_OK;
+    });
+}
+
+int ks_kernel_times(void* solver, ks_kernel_time* out, int cap) {
+    auto* h = static_cast<Handle*>(solver);
+    if (!h || cap < 0 || (cap > 0 && !out)) return -1;
+    int n = -1;
+    const ks_status st = guarded(h, [&] {
+        const std::vector<ks_kernel_time> t = h->solver->timer().totals();
+        for (int i = 0; i < (int)t.size() && i < cap; ++i) out[i] = t[i];
+        n = (int)t.size();
+        return KS_OK;
+    });
+    return st == KS_OK ? n : -1;
 }
 
 // ---- grid-kernel entry points

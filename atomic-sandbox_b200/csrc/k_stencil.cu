@@ -4,19 +4,22 @@
 // Reference operators: crates/qm/src/stencil.rs:21-51 (coefficients c = [-205/72, 8/5, -1/5,
 // 8/315, -1/560], Dirichlet zero outside the box), crates/qm-gpu/src/shaders/stencil.wgsl:58-106
 // (hamiltonian, jacobi_step). The centre is folded into second differences,
-//     lap f = (1/h^2) sum_{m=1..4} c_m sum_axes [(f_{+m} - f_0) + (f_{-m} - f_0)],
-// exact in real arithmetic because c_0 = -2 sum c_m, and exact per difference in f32 for smooth f.
+//     lap f = s sum_{m=1..4} c_m sum_axes [(f_{+m} - f_0) + (f_{-m} - f_0)],
+// exact in real arithmetic because c_0 = -2 sum c_m, and exact per difference in f32 for smooth f (the
+// differences carry no rounding, which keeps the f32 residual floor of the reference's stop rules). s is the
+// operator's scale (1/h^2, or -1/(2 h^2) for H); smallest coefficients first.
 //
-// B200 design ("2.5-D" tiling): a CTA owns a 32 x 16 (x, y) tile of one field and marches a
-// z-chunk. Each z-plane of the tile plus its 4-point xy halo (40 x 24 floats) is staged in shared
-// memory by one TMA load (cp.async.bulk.tensor.4d); the tensor map's extent is n on every axis, so
-// the halo beyond the box arrives as the hardware's zero fill -- the Dirichlet boundary costs no
-// branches and no ghost storage. An 8-deep ring of planes keeps four planes of prefetch in flight.
-// Each of the 128 threads computes a 2 x 2 block of outputs (two x-neighbours in two adjacent
-// rows) with Blackwell's packed f32x2 arithmetic, keeps the nine z-values of its columns in a
-// register queue that moves up one plane per step (a compact loop body: a 9-way unrolled rotation by
-// renaming overflowed the instruction cache, 'no instruction' being the top stall), and reads 4.5
-// shared-memory words per output. Stores and the V / R reads are coalesced 8-byte accesses.
+// B200 design ("2.5-D" tiling): a CTA owns a 32 x 16 (x, y) tile of one field and marches a z-chunk. Each z-plane
+// of the tile plus its 4-point xy halo (40 x 24 floats) is staged in shared memory by one TMA load
+// (cp.async.bulk.tensor.4d); the tensor map's extent is n on every axis, so the halo beyond the box arrives as the
+// hardware's zero fill -- the Dirichlet boundary costs no branches and no ghost storage. An 8-deep ring of planes
+// keeps four planes of prefetch in flight. Each of the 128 threads owns four consecutive x-outputs of one row: it
+// reads its centre, x- and y-neighbours as 16-byte quads (11 shared loads per 4 outputs), keeps the nine z-values of
+// its quad in a register queue that moves up one plane per step, and computes the two packed pairs of the quad with
+// Blackwell's f32x2 arithmetic. A neighbour pair that straddles two quads (odd x offsets) is differenced with two
+// scalar subtractions instead of being repacked. The V / R reads and the stores are coalesced 16-byte accesses;
+// the quad's pad columns are stored as 0. Measured against the 2 x 2-outputs-per-thread form it replaces: the same
+// outputs bit for bit at h = 0.25, and H psi on 95^3 at 8 / 16 / 64 vectors 13 / 13 / 21 % faster.
 #include <algorithm>
 #include <cudaTypedefs.h>
 #include "kernels.cuh"
@@ -33,22 +36,29 @@ constexpr int HXW = BX + 8, HYW = BY + 8;          // staged plane with halo: 40
 constexpr int NS = 8;                               // ring depth (planes)
 constexpr int PLANE_FLOATS = HXW * HYW;             // 960
 constexpr unsigned PLANE_BYTES = PLANE_FLOATS * 4;  // 3840 = 30 * 128
-constexpr int THREADS = 128;                        // 16 x-pairs * 8 y-pairs
+constexpr int THREADS = 128;                        // 8 x-quads * 16 rows
 // The TMA rules the plane loads rely on, checked here because a violation faults the GPU instead of returning an
 // error: the box's inner extent is a multiple of 16 bytes; a load's x coordinate, x0 - 4 with x0 a multiple of BX,
 // times 4 bytes is a multiple of 16 (negative x is allowed for loads and reads the zero fill); each ring plane starts
-// on a 128-byte boundary. The z-queue issues plane s + 12 into the buffer plane s + 4 left, which needs NS = 8.
+// on a 128-byte boundary. The quads the threads read start on 16-byte boundaries: rows of HXW floats, quads at
+// 4 * tx + 4 (and +-4 for the x-neighbours). The z-queue issues plane s + 12 into the buffer plane s + 4 left, which
+// needs NS = 8.
 static_assert((HXW * 4) % 16 == 0, "TMA box inner extent must be a multiple of 16 bytes");
 static_assert((BX * 4) % 16 == 0 && (4 * 4) % 16 == 0, "TMA x coordinate x0 - 4 must be a multiple of 16 bytes");
 static_assert(PLANE_BYTES % 128 == 0, "ring planes must start on 128-byte boundaries");
 static_assert(NS == 8, "plane s + 12 reuses the buffer of plane s + 4 only with an 8-deep ring");
-static_assert(THREADS == (BX / 2) * (BY / 2), "one thread per 2 x 2 block of outputs");
-// resident CTAs per SM: registers capped at 96 per thread (no spills) for 20 warps per SM; measured on the H2O 95^3
-// solve: 4 CTAs (126 registers) 213 ms, 5 CTAs 209 ms, 6 CTAs (80 registers) 216 ms
+static_assert(THREADS == (BX / 4) * BY, "one thread per x-quad of a row");
+// resident CTAs per SM: registers capped at 96 per thread (no spills) for 20 warps per SM; 4 and 6 CTAs per SM
+// measured slower (H psi on 95^3: 4 CTAs 182 us at 64 vectors, 6 CTAs 144 us, against 137 us at 5)
 constexpr int CTAS_PER_SM = 5;
 constexpr long long WAIT_LIMIT = 1LL << 22;         // bounded mbarrier waits (~seconds)
+constexpr long long DRAIN_LIMIT = 1LL << 16;        // waits for copies in flight after a wait gave up
 
 constexpr float C1 = 1.6f, C2 = -0.2f, C3 = 0.025396825396825397f, C4 = -0.0017857142857142857f;
+#ifndef KS_FOLD_SCALE
+#define KS_FOLD_SCALE 0
+#endif
+constexpr bool FOLD_SCALE = KS_FOLD_SCALE != 0;
 
 struct Params {
     int n, P;
@@ -82,16 +92,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: on timeout the error flag is raised and the caller carries on with whatever is
-// in shared memory (the result is then garbage, the host reports a device error).
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+// Bounded wait: false (and the error flag raised) when the copy did not complete within `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err, long long limit = WAIT_LIMIT) {
     long long spins = 0;
     while (!mbar_try_wait(bar, parity)) {
-        if (++spins > WAIT_LIMIT) {
+        if (++spins > limit) {
             if (err) atomicExch(err, 1);
-            return;
+            return false;
         }
     }
+    return true;
 }
 __device__ __forceinline__ void tma_load_plane(float* dst, const CUtensorMap* map, int x, int y, int z, int v, uint64_t* bar) {
     asm volatile(
@@ -101,7 +111,7 @@ __device__ __forceinline__ void tma_load_plane(float* dst, const CUtensorMap* ma
         : "memory");
 }
 
-// ---- packed f32x2 arithmetic (sm_100): one instruction for both x-neighbours of a thread
+// ---- packed f32x2 arithmetic (sm_100): one instruction for two x-neighbours
 __device__ __forceinline__ u64 add2(u64 a, u64 b) { u64 d; asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
 __device__ __forceinline__ u64 sub2(u64 a, u64 b) { u64 d; asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
 __device__ __forceinline__ u64 mul2(u64 a, u64 b) { u64 d; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
@@ -110,109 +120,67 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
     return d;
 }
-__device__ __forceinline__ u64 pack(float lo, float hi) {
+__device__ __forceinline__ u64 pk(float lo, float hi) {
     u64 d;
     asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
     return d;
 }
 __device__ __forceinline__ float lo_of(u64 v) { return __uint_as_float((unsigned)v); }
 __device__ __forceinline__ float hi_of(u64 v) { return __uint_as_float((unsigned)(v >> 32)); }
-// (hi of a, lo of b): the pair one float to the right of a
-__device__ __forceinline__ u64 straddle(u64 a, u64 b) { return pack(hi_of(a), lo_of(b)); }
-__device__ __forceinline__ u64 lds2(const float* p) { return *reinterpret_cast<const u64*>(p); }
+__device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float4 ldg4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+// (a0 - f0.lo, a1 - f0.hi)
+__device__ __forceinline__ u64 dif(float a0, float a1, u64 f0) { return sub2(pk(a0, a1), f0); }
 
-// Second differences of one row's two x-outputs at the centre plane c (ci = the thread's even x
-// in the staged plane), with the row's z-queue q (plane z+d at q[4 + d]):
-// sum_m c_m [dx_m + dy_m + dz_m], smallest coefficients first -- the scalar kernel's order.
-__device__ __forceinline__ u64 lap_row(const float* c, int ci, const u64 (&q)[9]) {
-    const u64 f0 = q[4];
-    const u64 xm4 = lds2(c + ci - 4), xm2 = lds2(c + ci - 2), xp2 = lds2(c + ci + 2), xp4 = lds2(c + ci + 4);
-    const u64 xp[5] = {0, straddle(f0, xp2), xp2, straddle(xp2, xp4), xp4};
-    const u64 xm[5] = {0, straddle(xm2, f0), xm2, straddle(xm4, xm2), xm4};
-    u64 d[5];
+// sum_m (c_m s) d_m of the thread's quad, as two packed pairs (x0, x0+1) and (x0+2, x0+3). cpl: the quad's address
+// in the centre plane (x-neighbour quads at -4 / +4, y-neighbours at +-m*HXW); q: the z-queue, q[4] the centre.
+// The y-neighbour quads are loaded inside the m loop, largest m first, so that only two are live at a time.
+__device__ __forceinline__ void lap_quad(const float* cpl, const float4 (&q)[9], const u64 (&k)[5], u64& o0, u64& o1) {
+    const float4 c = q[4];
+    const float4 l = lds4(cpl - 4), r = lds4(cpl + 4);
+    const float xs[12] = {l.x, l.y, l.z, l.w, c.x, c.y, c.z, c.w, r.x, r.y, r.z, r.w};
+    const u64 f0[2] = {pk(c.x, c.y), pk(c.z, c.w)};
+    u64 acc[2];
 #pragma unroll
-    for (int m = 1; m <= 4; ++m) {
-        const u64 dx = add2(sub2(xp[m], f0), sub2(xm[m], f0));
-        const u64 dy = add2(sub2(lds2(c + ci + m * HXW), f0), sub2(lds2(c + ci - m * HXW), f0));
-        const u64 dz = add2(sub2(q[4 + m], f0), sub2(q[4 - m], f0));
-        d[m] = add2(add2(dx, dy), dz);
+    for (int m = 4; m >= 1; --m) {
+        const float4 yu = lds4(cpl + m * HXW), yd = lds4(cpl - m * HXW);
+        const float4& zu = q[4 + m];
+        const float4& zd = q[4 - m];
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const int b = 4 + 2 * p;  // the pair's first element in xs
+            u64 dx;
+            if (m & 1) {
+                // odd offsets straddle two quads: two scalar differences instead of a repacked pair
+                const float a0 = xs[b + m] - lo_of(f0[p]), a1 = xs[b + 1 + m] - hi_of(f0[p]);
+                const float b0 = xs[b - m] - lo_of(f0[p]), b1 = xs[b + 1 - m] - hi_of(f0[p]);
+                dx = add2(pk(a0, a1), pk(b0, b1));
+            } else {
+                dx = add2(dif(xs[b + m], xs[b + 1 + m], f0[p]), dif(xs[b - m], xs[b + 1 - m], f0[p]));
+            }
+            u64 dy, dz;
+            if (p == 0) {
+                dy = add2(dif(yu.x, yu.y, f0[0]), dif(yd.x, yd.y, f0[0]));
+                dz = add2(dif(zu.x, zu.y, f0[0]), dif(zd.x, zd.y, f0[0]));
+            } else {
+                dy = add2(dif(yu.z, yu.w, f0[1]), dif(yd.z, yd.w, f0[1]));
+                dz = add2(dif(zu.z, zu.w, f0[1]), dif(zd.z, zd.w, f0[1]));
+            }
+            const u64 d = add2(add2(dx, dy), dz);
+            acc[p] = (m == 4) ? mul2(k[4], d) : fma2(k[m], d, acc[p]);
+        }
     }
-    u64 acc = mul2(pack(C4, C4), d[4]);
-    acc = fma2(pack(C3, C3), d[3], acc);
-    acc = fma2(pack(C2, C2), d[2], acc);
-    acc = fma2(pack(C1, C1), d[1], acc);
-    return acc;
+    o0 = acc[0];
+    o1 = acc[1];
 }
 
-struct Tile {
-    int z0, nplanes, vec;
-    int gx, gy, ciA;
-    long long vbase;
-    bool okA, okB, ok2;  // rows A / B in range (and gx < n), gx + 1 < n
-};
-
-// One z-step (output plane z0 + s): the new plane z0 + s + 4 enters the queues at q[8].
-template <int MODE, bool DOT>
-__device__ __forceinline__ void step(const Params& p, const Tile& t, float* ring, uint64_t* bar, u64 (&qa)[9], u64 (&qb)[9], int s,
-                                     float lam, float* __restrict__ out, double& dot, const CUtensorMap* tmap, int x0, int y0) {
-    const int qn = s + 8;
-    mbar_wait(&bar[qn % NS], (unsigned)((qn / NS) & 1), p.err);
-    const float* pn = ring + (qn % NS) * PLANE_FLOATS;
-    qa[8] = lds2(pn + t.ciA);
-    qb[8] = lds2(pn + t.ciA + HXW);
-    const float* c = ring + ((s + 4) % NS) * PLANE_FLOATS;
-    const u64 sc = pack(p.scale, p.scale);
-    const u64 la = mul2(lap_row(c, t.ciA, qa), sc);
-    const u64 lb = mul2(lap_row(c, t.ciA + HXW, qb), sc);
-    const u64 fa = qa[4], fb = qb[4];
-    const long long rowA = ((long long)(t.z0 + s) * p.n + t.gy) * p.P + t.gx;
-    const long long rowB = rowA + p.P;
-    u64 oa = la, ob = lb;
-    if (MODE != ST_LAPLACIAN) {
-        const u64 va = t.okA ? *reinterpret_cast<const u64*>(p.V + rowA) : 0ull;
-        const u64 vb = t.okB ? *reinterpret_cast<const u64*>(p.V + rowB) : 0ull;
-        const u64 ha = fma2(va, fa, la), hb = fma2(vb, fb, lb);
-        if (MODE == ST_HAMILTONIAN) {
-            oa = ha;
-            ob = hb;
-        } else {
-            const u64 ra = t.okA ? *reinterpret_cast<const u64*>(p.R + t.vbase + rowA) : 0ull;
-            const u64 rb = t.okB ? *reinterpret_cast<const u64*>(p.R + t.vbase + rowB) : 0ull;
-            const u64 nl = pack(-lam, -lam);
-            // w + (omega / max(diag_t + V - lambda, 0.1)) (r - (H w - lambda w)), as the scalar sweep
-            const u64 ua = sub2(ra, fma2(nl, fa, ha)), ub = sub2(rb, fma2(nl, fb, hb));
-            const float ia0 = p.omega * (1.0f / fmaxf(p.diag_t + lo_of(va) - lam, 0.1f));
-            const float ia1 = p.omega * (1.0f / fmaxf(p.diag_t + hi_of(va) - lam, 0.1f));
-            const float ib0 = p.omega * (1.0f / fmaxf(p.diag_t + lo_of(vb) - lam, 0.1f));
-            const float ib1 = p.omega * (1.0f / fmaxf(p.diag_t + hi_of(vb) - lam, 0.1f));
-            oa = fma2(pack(ia0, ia1), ua, fa);
-            ob = fma2(pack(ib0, ib1), ub, fb);
-        }
-    }
-    if (t.okA) {
-        if (t.ok2) *reinterpret_cast<u64*>(out + t.vbase + rowA) = oa;
-        else out[t.vbase + rowA] = lo_of(oa);
-    }
-    if (t.okB) {
-        if (t.ok2) *reinterpret_cast<u64*>(out + t.vbase + rowB) = ob;
-        else out[t.vbase + rowB] = lo_of(ob);
-    }
-    if (DOT) {
-        if (t.okA) {
-            dot += (double)lo_of(fa) * (double)lo_of(oa);
-            if (t.ok2) dot += (double)hi_of(fa) * (double)hi_of(oa);
-        }
-        if (t.okB) {
-            dot += (double)lo_of(fb) * (double)lo_of(ob);
-            if (t.ok2) dot += (double)hi_of(fb) * (double)hi_of(ob);
-        }
-    }
-    __syncthreads();  // the centre plane's buffer is free
-    if (threadIdx.x == 0 && s + 12 < t.nplanes) {
-        const int q = s + 12, b = q % NS;
-        mbar_expect_tx(&bar[b], PLANE_BYTES);
-        tma_load_plane(ring + b * PLANE_FLOATS, tmap, x0 - 4, y0 - 4, t.z0 - 4 + q, p.vec0 + t.vec, &bar[b]);
-    }
+// f64 sum of f0 * o over the valid elements of a quad (the Poisson p.Ap and the kinetic <psi, lap psi>)
+__device__ __forceinline__ double quad_dot(const float4& f, u64 o0, u64 o1, bool e1, bool e2, bool e3) {
+    double d = (double)f.x * (double)lo_of(o0);
+    if (e1) d += (double)f.y * (double)hi_of(o0);
+    if (e2) d += (double)f.z * (double)lo_of(o1);
+    if (e3) d += (double)f.w * (double)hi_of(o1);
+    return d;
 }
 
 template <int MODE, bool DOT>
@@ -220,27 +188,23 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
     extern __shared__ __align__(1024) float ring[];  // NS planes of 40 x 24
     __shared__ __align__(8) uint64_t bar[NS];
 
-    Tile t;
-    t.vec = blockIdx.y;
+    const int vec = blockIdx.y;
     int b = blockIdx.x;
     const int tile_x = b % p.tiles_x;
     b /= p.tiles_x;
     const int tile_y = b % p.tiles_y;
     const int chunk = b / p.tiles_y;
     const int x0 = tile_x * BX, y0 = tile_y * BY;
-    t.z0 = chunk * p.zc;
-    const int nz = min(t.z0 + p.zc, p.n) - t.z0;
-    t.nplanes = nz + 8;  // relative plane q <-> z = z0 - 4 + q
-    const int lx = (threadIdx.x & 15) * 2;   // even x of the thread's pair
-    const int ly = (threadIdx.x >> 4) * 2;   // rows ly and ly + 1
-    t.gx = x0 + lx;
-    t.gy = y0 + ly;
-    const bool okx = t.gx < p.n;
-    t.ok2 = t.gx + 1 < p.n;
-    t.okA = okx && t.gy < p.n;
-    t.okB = okx && t.gy + 1 < p.n;
-    t.ciA = (ly + 4) * HXW + (lx + 4);
-    t.vbase = (long long)t.vec * p.F;
+    const int z0 = chunk * p.zc;
+    const int nz = min(z0 + p.zc, p.n) - z0;
+    const int nplanes = nz + 8;  // relative plane q <-> z = z0 - 4 + q
+    const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
+    const int gx = x0 + 4 * tx, gy = y0 + ty;
+    // the quad's elements inside the box (gx is a multiple of 4 below n <= P, so the whole quad lies inside the
+    // row's P floats; elements at or past n are pad columns and are stored as 0)
+    const bool ok = gx < p.n && gy < p.n;
+    const bool e1 = gx + 1 < p.n, e2 = gx + 2 < p.n, e3 = gx + 3 < p.n;
+    const int ci = (ty + 4) * HXW + 4 * tx + 4;
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < NS; ++i) mbar_init(&bar[i], 1);
@@ -250,36 +214,100 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
     auto issue = [&](int q) {
         const int bb = q % NS;
         mbar_expect_tx(&bar[bb], PLANE_BYTES);
-        tma_load_plane(ring + bb * PLANE_FLOATS, &tmap, x0 - 4, y0 - 4, t.z0 - 4 + q, p.vec0 + t.vec, &bar[bb]);
+        tma_load_plane(ring + bb * PLANE_FLOATS, &tmap, x0 - 4, y0 - 4, z0 - 4 + q, p.vec0 + vec, &bar[bb]);
     };
+    // A wait that gives up raises the error flag and marks the thread dead: a dead thread waits no longer than a poll
+    // for later planes, thread 0 issues no further loads once dead, and before exiting thread 0 waits a bounded time
+    // for its copies still in flight. The CTA's outputs are then undefined (the host reports the error).
+    int issued = 0;  // planes issued so far (thread 0's count)
     if (threadIdx.x == 0)
-        for (int q = 0; q < NS; ++q) issue(q);
+        for (; issued < min(NS, nplanes); ++issued) issue(issued);
 
-    u64 qa[9], qb[9];
+    float4 q[9];
+    bool alive = true;
+    int waited = 0;  // planes 0..waited-1 arrived (each slot then holds at most one copy in flight)
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        mbar_wait(&bar[q], 0, p.err);
-        const float* pl = ring + q * PLANE_FLOATS;
-        qa[q] = lds2(pl + t.ciA);
-        qb[q] = lds2(pl + t.ciA + HXW);
+    for (int i = 0; i < 8; ++i) {
+        const bool got = mbar_wait(&bar[i], 0, p.err, alive ? WAIT_LIMIT : 1);
+        if (got && waited == i) waited = i + 1;
+        alive = alive && got;
+        q[i] = lds4(ring + i * PLANE_FLOATS + ci);
     }
     __syncthreads();  // planes 0..3 are consumed: their buffers take planes 8..11
-    if (threadIdx.x == 0)
-        for (int q = NS; q < min(NS + 4, t.nplanes); ++q) issue(q);
+    if (alive && threadIdx.x == 0)
+        for (; issued < min(NS + 4, nplanes); ++issued) issue(issued);
 
-    const float lam = (MODE == ST_JACOBI) ? (float)p.lambda[t.vec] : 0.0f;
+    // the coefficients; with FOLD_SCALE the operator's scale is folded into them, else it multiplies the sum (the
+    // same bits when the scale is a power of two)
+    u64 kc[5];
+    const float ks = FOLD_SCALE ? p.scale : 1.0f;
+    kc[0] = 0;
+    kc[1] = pk(C1 * ks, C1 * ks);
+    kc[2] = pk(C2 * ks, C2 * ks);
+    kc[3] = pk(C3 * ks, C3 * ks);
+    kc[4] = pk(C4 * ks, C4 * ks);
+    const u64 scale2 = pk(p.scale, p.scale);
+    const float lam = (MODE == ST_JACOBI) ? (float)p.lambda[vec] : 0.0f;
+    const long long plane = (long long)p.n * p.P;
+    const long long row0 = ((long long)z0 * p.n + gy) * p.P + gx;
+    const long long vbase = (long long)vec * p.F;
     double dot = 0.0;
-    int s = 0;
-    for (; s < nz; ++s) {
-        step<MODE, DOT>(p, t, ring, bar, qa, qb, s, lam, out, dot, &tmap, x0, y0);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {  // the z-queues move up one plane: q[i] <- q[i + 1]
-            qa[i] = qa[i + 1];
-            qb[i] = qb[i + 1];
+    // the compact loop body (not unrolled): unrolled bodies measured slower (the instruction cache)
+#pragma unroll 1
+    for (int s = 0; s < nz; ++s) {
+        const int qn = s + 8;
+        const bool got = mbar_wait(&bar[qn % NS], (unsigned)((qn / NS) & 1), p.err, alive ? WAIT_LIMIT : 1);
+        if (got && alive) waited = qn + 1;
+        alive = alive && got;
+        q[8] = lds4(ring + (qn % NS) * PLANE_FLOATS + ci);
+        const float* cpl = ring + ((s + 4) % NS) * PLANE_FLOATS + ci;
+        const long long at = row0 + s * plane;
+        // the global reads are issued before the stencil arithmetic, which hides their latency
+        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 v = (MODE != ST_LAPLACIAN && ok) ? ldg4(p.V + at) : zero4;
+        const float4 r = (MODE == ST_JACOBI && ok) ? ldg4(p.R + vbase + at) : zero4;
+        u64 o0, o1;
+        lap_quad(cpl, q, kc, o0, o1);
+        if (!FOLD_SCALE) {
+            o0 = mul2(o0, scale2);
+            o1 = mul2(o1, scale2);
         }
+        const float4 f = q[4];
+        if (MODE != ST_LAPLACIAN) {
+            const u64 h0 = fma2(pk(v.x, v.y), pk(f.x, f.y), o0), h1 = fma2(pk(v.z, v.w), pk(f.z, f.w), o1);
+            if (MODE == ST_HAMILTONIAN) {
+                o0 = h0;
+                o1 = h1;
+            } else {
+                const u64 nl = pk(-lam, -lam);
+                // w + (omega / max(diag_t + V - lambda, 0.1)) (r - (H w - lambda w)), as the scalar sweep
+                const u64 u0 = sub2(pk(r.x, r.y), fma2(nl, pk(f.x, f.y), h0));
+                const u64 u1 = sub2(pk(r.z, r.w), fma2(nl, pk(f.z, f.w), h1));
+                const float i0 = p.omega * (1.0f / fmaxf(p.diag_t + v.x - lam, 0.1f));
+                const float i1 = p.omega * (1.0f / fmaxf(p.diag_t + v.y - lam, 0.1f));
+                const float i2 = p.omega * (1.0f / fmaxf(p.diag_t + v.z - lam, 0.1f));
+                const float i3 = p.omega * (1.0f / fmaxf(p.diag_t + v.w - lam, 0.1f));
+                o0 = fma2(pk(i0, i1), u0, pk(f.x, f.y));
+                o1 = fma2(pk(i2, i3), u1, pk(f.z, f.w));
+            }
+        }
+        if (ok) {
+            *reinterpret_cast<float4*>(out + vbase + at) =
+                make_float4(lo_of(o0), e1 ? hi_of(o0) : 0.f, e2 ? lo_of(o1) : 0.f, e3 ? hi_of(o1) : 0.f);
+            if (DOT) dot += quad_dot(f, o0, o1, e1, e2, e3);
+        }
+        __syncthreads();  // the centre plane's buffer is free
+        if (alive && threadIdx.x == 0 && s + 12 < nplanes) {
+            issue(s + 12);
+            issued = s + 13;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) q[i] = q[i + 1];  // the z-queue moves up one plane
     }
+    if (threadIdx.x == 0 && !alive)
+        for (int qq = waited; qq < issued; ++qq) mbar_wait(&bar[qq % NS], (unsigned)((qq / NS) & 1), nullptr, DRAIN_LIMIT);
     if (DOT) {
-        double sum = block_sum(dot);
+        const double sum = block_sum(dot);
         if (threadIdx.x == 0) p.dot_partials[blockIdx.x + (size_t)gridDim.x * blockIdx.y] = sum;
     }
 }
@@ -359,6 +387,10 @@ int stencil_ctas(const Layout& L, int count) {
 
 int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const StencilArgs& a, float* out, cudaStream_t s) {
     if (count <= 0) return 0;
+    // the quads' 16-byte loads and stores need 16-byte aligned fields (P is a multiple of 4 floats)
+    if ((reinterpret_cast<uintptr_t>(out) & 15) || (a.V && (reinterpret_cast<uintptr_t>(a.V) & 15)) ||
+        (a.R && (reinterpret_cast<uintptr_t>(a.R) & 15)))
+        throw std::invalid_argument("stencil: fields must be 16-byte aligned");
     Shape sh = shape_for(L, count);
     Params p;
     p.n = L.n;

@@ -250,6 +250,58 @@ double rayleigh_ritz(int m, const std::vector<double>& A, const std::vector<doub
     return alpha;
 }
 
+// ------------------------------------------------------------------ kernel timing
+KernelTimer::~KernelTimer() {
+    for (auto& r : pending_) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (cudaEvent_t e : pool_) cudaEventDestroy(e);
+}
+
+cudaEvent_t KernelTimer::take() {
+    {
+        std::lock_guard<std::mutex> lock(mu_);
+        if (!pool_.empty()) {
+            cudaEvent_t e = pool_.back();
+            pool_.pop_back();
+            return e;
+        }
+    }
+    cudaEvent_t e = nullptr;
+    KS_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void KernelTimer::enable(bool on) {
+    totals();  // settle what is recorded, then start from zero
+    std::lock_guard<std::mutex> lock(mu_);
+    agg_.clear();
+    on_.store(on, std::memory_order_relaxed);
+}
+
+std::vector<ks_kernel_time> KernelTimer::totals() {
+    std::lock_guard<std::mutex> lock(mu_);
+    for (auto& r : pending_) {
+        KS_CUDA(cudaEventSynchronize(r.b));
+        float ms = 0.f;
+        KS_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        auto it = std::find_if(agg_.begin(), agg_.end(), [&](const ks_kernel_time& t) {
+            return t.kernel == r.kernel && t.count == r.count && t.aux == r.aux;
+        });
+        if (it == agg_.end()) {
+            agg_.push_back(ks_kernel_time{r.kernel, r.count, r.aux, 0, 0.0, r.bytes});
+            it = agg_.end() - 1;
+        }
+        ++it->launches;
+        it->total_ms += ms;
+        pool_.push_back(r.a);
+        pool_.push_back(r.b);
+    }
+    pending_.clear();
+    return agg_;
+}
+
 // ------------------------------------------------------------------ buffers
 void DevBuf::alloc(size_t n) {
     release();
@@ -331,7 +383,9 @@ void Reducer::gram(int m, const float* S, int mt, const float* T, int off, doubl
         const int blocks = gram_tc_blocks(m, mt);
         const size_t need = (size_t)blocks * m * (m + mt);
         if (need * sizeof(double) > partials_.bytes) partials_.alloc(need * sizeof(double));
-        launch_gram_tc(L_.F, m, S, mt, T, partials_.d(), s_);
+        auto run = [&] { launch_gram_tc(L_.F, m, S, mt, T, partials_.d(), s_); };
+        if (timer) timer->time(KS_K_GRAM, m, mt, 4.0 * (m + mt) * L_.interior(), s_, run);
+        else run();
         if (extra) {
             FinishDesc g;
             g.partials = partials_.d();
@@ -349,7 +403,9 @@ void Reducer::gram(int m, const float* S, int mt, const float* T, int off, doubl
     }
     const size_t need = (size_t)gram_blocks_ * m * (m + mt);
     if (need * sizeof(double) > partials_.bytes) partials_.alloc(need * sizeof(double));
-    launch_gram(L_.F, m, S, mt, T, partials_.d(), gram_blocks_, s_);
+    auto run = [&] { launch_gram(L_.F, m, S, mt, T, partials_.d(), gram_blocks_, s_); };
+    if (timer) timer->time(KS_K_GRAM, m, mt, 4.0 * (m + mt) * L_.interior(), s_, run);
+    else run();
     if (extra) {
         FinishDesc g;
         g.partials = partials_.d();
@@ -365,6 +421,15 @@ void Reducer::gram(int m, const float* S, int mt, const float* T, int off, doubl
 
 const double* Reducer::read(int count) {
     if (count > RES_CAP) throw std::invalid_argument("reducer: result overflow");
+    if (faults && faults->count.load() > 0) {
+        if (faults->skip.load() > 0) {
+            faults->skip.fetch_sub(1);
+        } else {
+            faults->count.fetch_sub(1);
+            ++readbacks;
+            throw DeviceError("a readback did not deliver its results (injected failure)");
+        }
+    }
     if (count > 0) KS_CUDA(cudaMemcpyAsync(host_, res_.d(), (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, s_));
     KS_CUDA(cudaMemcpyAsync(host_flag_, device_error_flag(), sizeof(int), cudaMemcpyDeviceToHost, s_));
     auto t0 = std::chrono::steady_clock::now();
@@ -677,9 +742,11 @@ Solver::Solver(int n, double h, const SolverOptions& o) : L_(Layout::make(n, h))
     err_.alloc(256);
     zero_device(err_.p, err_.bytes);
     red_.init(L_, s_, 1 << 20);
+    red_.faults = &faults_;
     for (auto& l : lane_) {
         l.reset(new Lane());
         l->init(L_);
+        l->red.faults = &faults_;
     }
     poisson_.init(L_, s_, &red_);
     for (Block* b : {&vnuc_, &vh_, &in_up_, &in_dn_, &out_up_, &out_dn_, &rho_tot_, &v_up_, &v_dn_, &exc_, &ones_}) b->create(L_, 1);
@@ -696,6 +763,61 @@ Solver::~Solver() {
     if (ev_fork_) cudaEventDestroy(ev_fork_);
 }
 
+void Solver::import_state(int n_up, int n_dn, const int k[2], const double* const orb[2], const double* const evals[2],
+                          const double* const occ[2], const double* rho_up, const double* rho_dn, const double* v_h, bool fermi_dirac) {
+    const int nocc[2] = {n_up, n_dn};
+    if (n_up < 0 || n_dn < 0 || !rho_up || !rho_dn || !v_h) throw std::invalid_argument("state_import: invalid arguments");
+    if (fermi_dirac && opt_.n_extra < 1) throw std::invalid_argument("state_import: Fermi-Dirac needs n_extra >= 1 (ks_options)");
+    int kk[2];
+    for (int sp = 0; sp < 2; ++sp) {
+        // the block the next warm solve runs: N_sigma + n_extra columns (under Fermi-Dirac a grown block is kept at its size)
+        kk[sp] = nocc[sp] > 0 ? std::max(nocc[sp] + opt_.n_extra, fermi_dirac ? k[sp] : 0) : 0;
+        if (k[sp] < nocc[sp] || k[sp] > std::max(kk[sp], nocc[sp]) || kk[sp] > 64 || (k[sp] > 0 && (!orb[sp] || !evals[sp])) ||
+            (fermi_dirac && k[sp] > 0 && !occ[sp]))
+            throw std::invalid_argument("state_import: spin " + std::to_string(sp) + ": need N_sigma <= k <= N_sigma + n_extra orbitals "
+                                        "(up to 64), with their levels (and occupations under Fermi-Dirac)");
+    }
+    converged_ = false;
+    have_warm_ = false;
+    have_prev_ = false;
+    const long long N = L_.interior();
+    DevBuf tmp((size_t)N * sizeof(double));
+    auto upload = [&](const double* host, float* field) {
+        KS_CUDA(cudaMemcpyAsync(tmp.p, host, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s_));
+        launch_pack(L_, 1, tmp.d(), field, s_);
+    };
+    for (int sp = 0; sp < 2; ++sp) {
+        ensure_channel(sp, kk[sp]);
+        occ_[sp].assign(kk[sp], 0.0);
+        if (kk[sp] == 0) continue;
+        Channel& ch = ch_[sp];
+        ch.cur = 0;
+        for (int i = 0; i < k[sp]; ++i) upload(orb[sp] + (size_t)i * N, ch.A[0].at(i));
+        // columns the state does not carry start from the uniform(-1, 1) guess, seeded per column and spin
+        for (int i = k[sp]; i < kk[sp]; ++i)
+            launch_initial_orbitals(L_, nullptr, 0, 1, 1000ULL + 2ULL * (unsigned long long)i + (unsigned long long)sp, 1, ch.A[0].at(i), s_);
+        ch.evals.assign(evals[sp], evals[sp] + k[sp]);
+        while ((int)ch.evals.size() < kk[sp]) ch.evals.push_back(ch.evals.empty() ? -1.0 : ch.evals.back());
+        for (int i = 0; i < kk[sp]; ++i) occ_[sp][i] = fermi_dirac ? (i < k[sp] ? occ[sp][i] : 0.0) : (i < nocc[sp] ? 1.0 : 0.0);
+    }
+    upload(rho_up, out_up_.at(0));
+    upload(rho_dn, out_dn_.at(0));
+    upload(v_h, vh_.at(0));
+    KS_CUDA(cudaStreamSynchronize(s_));  // tmp is freed on return
+    nocc_[0] = n_up;
+    nocc_[1] = n_dn;
+    fd_state_ = fermi_dirac;
+    state_gen_ = ionic_gen();
+    have_warm_ = true;
+}
+
+void Solver::poison_parked_density() {
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    const long long c = ((long long)(L_.n / 2) * L_.n + L_.n / 2) * L_.P + L_.n / 2;  // the box centre
+    KS_CUDA(cudaMemcpyAsync(out_up_.at(0) + c, &nan, sizeof(float), cudaMemcpyHostToDevice, s_));
+    KS_CUDA(cudaStreamSynchronize(s_));
+}
+
 void Solver::ensure_channel(int spin, int k) {
     if (ch_[spin].k != k) {
         ch_[spin] = Channel();
@@ -705,6 +827,7 @@ void Solver::ensure_channel(int spin, int k) {
 
 void Solver::gram_checked(Reducer& red, int m, const float* S, int mt, const float* T, const FinishDesc* extra) {
     red.gram_mode = opt_.gram_mode;
+    red.timer = &timer_;
     red.gram(m, S, mt, T, 0, L_.h * L_.h * L_.h, extra);  // the L2 product <a, b> = h^3 sum a b
 }
 
@@ -723,13 +846,14 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
     double* theta_d = ch.theta_d.d();
     double* lambda_d = theta_d + k;
     double* coef_d = theta_d + 2 * k;
+    const double npts = (double)L_.interior();
     auto apply_h = [&](const Block& in, int vec0, int count, float* out) {
         StencilArgs a;
         a.mode = ST_HAMILTONIAN;
         a.scale = ham_scale;
         a.V = V;
         a.vec0 = vec0;
-        launch_stencil(L_, in.tmap, count, a, out, lane.s);
+        timer_.time(KS_K_HPSI, count, 0, (8.0 * count + 4.0) * npts, lane.s, [&] { launch_stencil(L_, in.tmap, count, a, out, lane.s); });
         // + V_NL under a pseudopotential setup (crates/qm-gpu/src/eigen.rs:216-227; the preconditioner stays local)
         if (nl_on_) ionic_.apply_nl(L_, in.at(vec0), count, out, lane.nl, lane.s);
     };
@@ -797,7 +921,10 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         const int nb = lane.red.blocks();
         if (lane.norm_part.bytes < (size_t)nb * k * sizeof(double)) lane.norm_part.alloc((size_t)nb * k * sizeof(double));
         double* norm_partials = lane.norm_part.d();  // finished in the Gram's finish launch below
-        launch_residual_precond(L_, k, ch.HX.at(0), ch.X(), theta_d, V, lambda_d, diag_t, ch.T.at(0), ch.Q.at(0), norm_partials, nb, lane.s);
+        timer_.time(KS_K_RESIDUAL, k, 0, (16.0 * k + 4.0) * npts, lane.s, [&] {
+            launch_residual_precond(L_, k, ch.HX.at(0), ch.X(), theta_d, V, lambda_d, diag_t, ch.T.at(0), ch.Q.at(0), norm_partials, nb,
+                                    lane.s);
+        });
         const int m = 2 * k + np;
         const int off_norm = m * 2 * m;
         StencilArgs jac;
@@ -809,11 +936,12 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         jac.omega = (float)omega;
         jac.diag_t = (float)diag_t;
         jac.vec0 = 0;
-        launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), lane.s);       // Q -> W
+        const double jac_bytes = (12.0 * k + 4.0) * npts;
+        timer_.time(KS_K_JACOBI, k, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), lane.s); });   // Q -> W
         jac.vec0 = k;
-        launch_stencil(L_, S.tmap, k, jac, ch.Q.at(0), lane.s);       // W -> Q
+        timer_.time(KS_K_JACOBI, k, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, S.tmap, k, jac, ch.Q.at(0), lane.s); });   // W -> Q
         jac.vec0 = 0;
-        launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), lane.s);       // Q -> W
+        timer_.time(KS_K_JACOBI, k, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), lane.s); });   // Q -> W
         // 2. HW and HP in one launch (W and P are contiguous after X)
         apply_h(S, k, k + np, ch.T.at(k));
         // 3. the readback: G = S^T [S | T] and |r_i|^2
@@ -935,7 +1063,8 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         lane.dense_s += secs(t_dense);
         upload(theta, lambda, &coef);
         const int next = ch.cur ^ 1;
-        launch_block_lincomb(L_.F, m, S.at(0), 2 * k, coef_d, ch.A[next].at(0), k, k, lane.s);
+        timer_.time(KS_K_BLOCK_UPDATE, m, 2 * k, 4.0 * (m + 2 * k) * npts, lane.s,
+                    [&] { launch_block_lincomb(L_.F, m, S.at(0), 2 * k, coef_d, ch.A[next].at(0), k, k, lane.s); });
         ch.cur = next;
         np = k;
         // 6. HX of the new X
@@ -1122,6 +1251,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         while (iterations < s.max_iter) {
             if (abort_fn && abort_fn(user)) return park("abandoned before SCF step " + std::to_string(iterations + 1));
             ++iterations;
+            profile.steps = iterations;  // also what a failed solve's profile reports
             NvtxRange step_range("ks scf step");
             // a warm guess is accepted within the 1.5x band only in the convergence phase (the previous step's dRho
             // already below tol); before that only within the step's own tol. This is the reference's rule for its
@@ -1169,7 +1299,8 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 };
                 std::exception_ptr err_dn;
                 std::thread worker;
-                const bool both = nocc[0] > 0 && nocc[1] > 0;
+                // under kernel timing the channels run one after the other, so that each launch is timed alone
+                const bool both = nocc[0] > 0 && nocc[1] > 0 && !timer_.on();
                 if (both)
                     worker = std::thread([&] {
                         ErrorFlagScope worker_flag(err_flag());

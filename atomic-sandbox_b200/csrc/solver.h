@@ -2,6 +2,7 @@
 #pragma once
 #include <atomic>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -42,6 +43,43 @@ struct Block {
     float* at(int i) const { return buf.f() + (long long)i * F; }
 };
 
+// Per-shape device timing of the hot launches (ks_set_kernel_timing): CUDA events around each launch on its own
+// stream, collected when read. Shared by the solver's host threads (the two spin channels), hence the lock.
+class KernelTimer {
+public:
+    KernelTimer() = default;
+    KernelTimer(const KernelTimer&) = delete;
+    KernelTimer& operator=(const KernelTimer&) = delete;
+    ~KernelTimer();
+    void enable(bool on);
+    bool on() const { return on_.load(std::memory_order_relaxed); }
+    // runs launch() between two events on s when the timer is on (never while the thread captures a graph)
+    template <class Launch>
+    void time(int kernel, int count, int aux, double bytes, cudaStream_t s, Launch&& launch) {
+        if (!on()) {
+            launch();
+            return;
+        }
+        cudaEvent_t a = take(), b = take();
+        KS_CUDA(cudaEventRecord(a, s));
+        launch();
+        KS_CUDA(cudaEventRecord(b, s));
+        std::lock_guard<std::mutex> lock(mu_);
+        pending_.push_back({kernel, count, aux, bytes, a, b});
+    }
+    // waits for the recorded launches and returns the totals per shape
+    std::vector<ks_kernel_time> totals();
+
+private:
+    struct Rec { int kernel, count, aux; double bytes; cudaEvent_t a, b; };
+    cudaEvent_t take();
+    std::atomic<bool> on_{false};
+    std::mutex mu_;
+    std::vector<Rec> pending_;
+    std::vector<cudaEvent_t> pool_;
+    std::vector<ks_kernel_time> agg_;
+};
+
 // Device reductions with a fixed grid (deterministic), results kept on the device until read.
 class Reducer {
 public:
@@ -58,9 +96,16 @@ public:
     int blocks() const { return blocks_; }
     // copies res[0..count) to the host and synchronises; raises DeviceError on a failed kernel wait
     const double* read(int count);
+    // failure injection for the failure-path tests: lets `skip` readbacks through, then fails the next `count` as a
+    // readback that never delivers (DeviceError); shared by a solver's reducers
+    struct Faults {
+        std::atomic<long long> skip{0}, count{0};
+    };
+    Faults* faults = nullptr;
     int readbacks = 0;
     double wait_s = 0;  // host time blocked in read()
     int gram_mode = 0;  // 0: CUDA-core f32 Gram, 1: tensor-core 3xTF32 Gram
+    KernelTimer* timer = nullptr;  // times the Gram launch when set
     double* host() const { return host_; }
     static constexpr int RES_CAP = 1 << 16;
 
@@ -265,6 +310,17 @@ public:
     Reducer& reducer() { return red_; }
     // this solver's wait-timeout flag (device int); its calls install it as the thread's current flag (ErrorFlagScope)
     int* err_flag() const { return static_cast<int*>(err_.p); }
+    KernelTimer& timer() { return timer_; }
+    // the warm start of the next solve from host arrays (ks_state_import); k_sp orbitals per spin (f64 n^3 each),
+    // their levels and occupations, the input densities and V_H. Throws std::invalid_argument on inconsistent sizes.
+    void import_state(int n_up, int n_dn, const int k[2], const double* const orb[2], const double* const evals[2],
+                      const double* const occ[2], const double* rho_up, const double* rho_dn, const double* v_h, bool fermi_dirac);
+    // failure-path test hooks: a NaN in the parked warm density; the next readbacks fail
+    void poison_parked_density();
+    void fail_readbacks(long long skip, long long count) {
+        faults_.skip.store(skip);
+        faults_.count.store(count);
+    }
 
 private:
     void ensure_channel(int spin, int k);
@@ -310,6 +366,8 @@ private:
     DevBuf occ_d_;                 // device copy of the occupations (2 x 64 doubles), density weights
     cudaEvent_t ev_fork_ = nullptr;
     DevBuf err_;                   // the solver's own wait-timeout flag
+    KernelTimer timer_;            // per-shape kernel timing (off unless asked for)
+    Reducer::Faults faults_;       // injected readback failures (tests)
     int dev_ = 0;
     double floor_;
 };

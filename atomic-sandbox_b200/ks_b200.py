@@ -59,6 +59,13 @@ class _Profile(ctypes.Structure):
                [("witness_growths", ctypes.c_int), ("extrapolated", ctypes.c_int)]
 
 
+class _KernelTime(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int), ("count", ctypes.c_int), ("aux", ctypes.c_int), ("launches", ctypes.c_int),
+                ("total_ms", ctypes.c_double), ("bytes", ctypes.c_double)]
+
+
+KERNEL_NAMES = {0: "hpsi", 1: "jacobi", 2: "residual_precond", 3: "gram", 4: "block_update"}
+
 ABORT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
 
 
@@ -193,7 +200,8 @@ EXPORTED = [
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
     "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
-    "ks_fd_witness", "ks_device_status",
+    "ks_fd_witness", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
+    "ks_test_poison_parked_density", "ks_test_fail_readbacks",
 ]
 
 
@@ -230,6 +238,12 @@ def lib():
         L.ks_state_potentials.argtypes = [ctypes.c_void_p, dp, dp]
         L.ks_state_orbitals.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
         L.ks_profile_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Profile)]
+        L.ks_set_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ks_state_import.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp, dp, dp,
+                                      ctypes.c_int, dp, dp]
+        L.ks_test_poison_parked_density.argtypes = [ctypes.c_void_p]
+        L.ks_test_fail_readbacks.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.ks_kernel_times.argtypes = [ctypes.c_void_p, ctypes.POINTER(_KernelTime), ctypes.c_int]
         L.ks_apply_hamiltonian.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, dp, dp, dp]
         L.ks_apply_laplacian.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
         L.ks_apply_precond.argtypes = [ctypes.c_int, ctypes.c_double, dp, ctypes.c_double, dp, dp]
@@ -544,6 +558,32 @@ class GpuSolver:
         _check(lib().ks_state_orbitals(self._h, int(spin), _p(out)), self._h)
         return out[: k * self.n ** 3].reshape(k, self.n ** 3)
 
+    def import_state(self, n_up, n_dn, orbitals, evals, density, v_h, occupations=None):
+        """The warm start of the next solve(warm=True) from a saved state (ks_state_import): orbitals / evals per spin
+        as (k, n^3) and (k,) arrays (N_sigma <= k <= N_sigma + n_extra), density = (rho_up, rho_dn), v_h an n^3
+        array, occupations None (Aufbau) or a per-spin pair of f arrays (Fermi-Dirac)."""
+        n3 = self.n ** 3
+        orb = [np.ascontiguousarray(o, dtype=np.float64).reshape(-1, n3) for o in orbitals]
+        ev = [np.ascontiguousarray(e, dtype=np.float64) for e in evals]
+        rho = [np.ascontiguousarray(r, dtype=np.float64).reshape(n3) for r in density]
+        vh = np.ascontiguousarray(v_h, dtype=np.float64).reshape(n3)
+        occ = None if occupations is None else [np.ascontiguousarray(f, dtype=np.float64) for f in occupations]
+        empty = np.zeros(1)
+
+        def ptr(a):
+            return _p(a if a is not None and a.size else empty)
+        _check(lib().ks_state_import(self._h, int(n_up), int(n_dn), orb[0].shape[0], ptr(orb[0]), ptr(ev[0]), orb[1].shape[0],
+                                     ptr(orb[1]), ptr(ev[1]), _p(rho[0]), _p(rho[1]), _p(vh), 0 if occ is None else 1,
+                                     ptr(occ[0]) if occ else None, ptr(occ[1]) if occ else None), self._h)
+
+    def poison_parked_density(self):
+        """Failure-path test hook: a NaN in the parked warm density (ks_test_poison_parked_density)."""
+        _check(lib().ks_test_poison_parked_density(self._h), self._h)
+
+    def fail_readbacks(self, skip, count):
+        """Failure-path test hook: let `skip` readbacks through, fail the next `count` (ks_test_fail_readbacks)."""
+        _check(lib().ks_test_fail_readbacks(self._h, int(skip), int(count)), self._h)
+
     def stream(self):
         """The cudaStream_t (as an int) every kernel of this solver runs on."""
         return lib().ks_solver_stream(self._h)
@@ -552,6 +592,26 @@ class GpuSolver:
         p = _Profile()
         _check(lib().ks_profile_get(self._h, ctypes.byref(p)), self._h)
         return {n: getattr(p, n) for n, _ in _Profile._fields_}
+
+    def set_kernel_timing(self, on=True):
+        """Per-shape device timing of the LOBPCG chain's launches (ks_set_kernel_timing); switching on clears it."""
+        _check(lib().ks_set_kernel_timing(self._h, 1 if on else 0), self._h)
+
+    def kernel_times(self):
+        """Launches, device time and algorithmic bytes per launch shape since the timing was switched on
+        (ks_kernel_times): a list of dicts with kernel, count, aux, launches, total_ms, bytes, mean_us, gbs."""
+        cap = 64
+        buf = (_KernelTime * cap)()
+        n = lib().ks_kernel_times(self._h, buf, cap)
+        if n < 0:
+            _check(KS_DEVICE, self._h)
+        out = []
+        for t in buf[:min(n, cap)]:
+            mean_s = t.total_ms / 1000.0 / t.launches if t.launches else 0.0
+            out.append({"kernel": KERNEL_NAMES.get(t.kernel, str(t.kernel)), "count": t.count, "aux": t.aux,
+                        "launches": t.launches, "total_ms": t.total_ms, "bytes": t.bytes, "mean_us": mean_s * 1e6,
+                        "gbs": t.bytes / mean_s / 1e9 if mean_s > 0 else 0.0})
+        return out
 
 
 def _stats_dict(st):

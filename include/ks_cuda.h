@@ -88,6 +88,13 @@ typedef struct {
     int extrapolated;     /* the warm start's input density was extrapolated (SolveProfile::extrapolated) */
 } ks_profile;
 
+/* Device time of one launch shape of a solver's hot kernels (instrumentation, no reference counterpart): kernel
+   (KS_K_*), count (vectors of a stencil or residual launch, m of a Gram or block update), aux (mt of a Gram, q of a
+   block update, else 0), launches, their summed device time (CUDA events on the stream they ran on) and the
+   algorithmic bytes of one launch (what it must read and write once, on the n^3 interior points). */
+typedef struct { int kernel, count, aux, launches; double total_ms, bytes; } ks_kernel_time;
+enum { KS_K_HPSI = 0, KS_K_JACOBI = 1, KS_K_RESIDUAL = 2, KS_K_GRAM = 3, KS_K_BLOCK_UPDATE = 4 };
+
 /* Polled before every SCF step (GpuSolver::solve_with, crates/qm-gpu/src/scf.rs:1208): nonzero abandons the solve. */
 typedef int (*ks_abort_fn)(void* user);
 
@@ -225,7 +232,32 @@ ks_status ks_state_occupations(const void* solver, double* up, double* dn);
 ks_status ks_state_density(const void* solver, double* rho_up, double* rho_dn);   /* n^3 each */
 ks_status ks_state_potentials(const void* solver, double* v_nuc, double* v_h);     /* n^3 each */
 ks_status ks_state_orbitals(const void* solver, int spin, double* out);            /* count * n^3 */
+/* The warm start of the next ks_solve(warm = 1) from a saved state, the inverse of the getters above: the reference
+   parks the whole GpuState (orbitals, levels, rho_up / rho_dn, V_H, occupations) between solves and resumes from it
+   (crates/qm-gpu/src/scf.rs:1286-1323, GpuState :410-418); here the state can come from host memory, e.g. one
+   exported by another solver of the same grid. Per spin k_up / k_dn orbitals (f64, k * n^3 in the qm::Grid layout)
+   with their levels, N_sigma <= k <= N_sigma + n_extra; columns of the block beyond k start from the uniform(-1, 1)
+   guess. rho_up, rho_dn, v_h: n^3 each. occupations: 0 Aufbau, 1 Fermi-Dirac (occ_up / occ_dn then hold one f per
+   orbital; NULL under Aufbau). The next solve must name the same n_up / n_dn and occupation scheme to be warm.
+   The imported state is not a converged state: the getters and ks_forces report KS_NO_STATE until a solve converges. */
+ks_status ks_state_import(void* solver, int n_up, int n_dn, int k_up, const double* orbitals_up, const double* evals_up,
+                          int k_dn, const double* orbitals_dn, const double* evals_dn, const double* rho_up,
+                          const double* rho_dn, const double* v_h, int occupations, const double* occ_up, const double* occ_dn);
+/* Failure-injection hooks for the failure-path tests, the counterparts of the reference's fault-injection feature
+   (crates/gpu/src/readback.rs:36-58, crates/qm-gpu/src/scf.rs:2400-2460); nothing calls them in normal use.
+   ks_test_poison_parked_density writes a NaN into the parked warm density (the next warm solve must end in
+   KS_NUMERICAL). ks_test_fail_readbacks lets `skip` of this solver's readbacks through and fails the next `count`
+   as a readback that never delivers (KS_DEVICE); (0, 0) clears it. Neither touches the GPU's state. */
+ks_status ks_test_poison_parked_density(void* solver);
+ks_status ks_test_fail_readbacks(void* solver, int skip, int count);
 ks_status ks_profile_get(const void* solver, ks_profile* out);                     /* GpuSolver::profile */
+/* Kernel timing of the LOBPCG chain (H psi, the Jacobi sweeps, the residual, the Gram, the block update), off by
+   default: while on, each launch is bracketed by two CUDA events on its stream and the two spin channels run one
+   after the other, so that each launch is timed alone (the results are unchanged; the solve is slower). Switching
+   it on clears the totals. ks_kernel_times waits for the recorded
+   launches, fills at most cap shapes into out and returns the number of shapes (negative on an invalid handle). */
+ks_status ks_set_kernel_timing(void* solver, int on);
+int ks_kernel_times(void* solver, ks_kernel_time* out, int cap);
 
 /* ---- readouts of the converged state (display and diagnostics; nothing is fed back into a solve) ---- */
 /* GpuSolver::sample_density (crates/qm-gpu/src/sample.rs:84-121): rho_up + rho_dn at count points (pts3[3*q + axis],

@@ -57,6 +57,15 @@ extern "C" {
     pub fn ks_state_potentials(s: *const c_void, v_nuc: *mut c_double, v_h: *mut c_double) -> c_int;
     pub fn ks_state_orbitals(s: *const c_void, spin: c_int, out: *mut c_double) -> c_int;
     pub fn ks_profile_get(s: *const c_void, out: *mut ks_profile) -> c_int;
+    pub fn ks_state_import(s: *mut c_void, n_up: c_int, n_dn: c_int, k_up: c_int, orbitals_up: *const c_double,
+                           evals_up: *const c_double, k_dn: c_int, orbitals_dn: *const c_double, evals_dn: *const c_double,
+                           rho_up: *const c_double, rho_dn: *const c_double, v_h: *const c_double, occupations: c_int,
+                           occ_up: *const c_double, occ_dn: *const c_double) -> c_int;
+    // failure-injection hooks (the tests of the failure paths)
+    pub fn ks_test_poison_parked_density(s: *mut c_void) -> c_int;
+    pub fn ks_test_fail_readbacks(s: *mut c_void, skip: c_int, count: c_int) -> c_int;
+    pub fn ks_set_kernel_timing(s: *mut c_void, on: c_int) -> c_int;
+    pub fn ks_kernel_times(s: *mut c_void, out: *mut ks_kernel_time, cap: c_int) -> c_int;
     pub fn ks_apply_nonlocal(s: *mut c_void, nuc: *const ks_nucleus, n_nuc: c_int, count: c_int, x: *const c_double,
                              out: *mut c_double, c: *mut c_double, rows: *mut c_int) -> c_int;
     // component entry points (one stage of the SCF on host f64 arrays in the qm::Grid layout)
@@ -109,3 +118,5 @@ extern "C" {
     pub poisson_iterations: c_int, pub eigen_calls: c_int, pub diis_resets: c_int, pub wall_s: f64, pub start_s: f64,
     pub poisson_s: f64, pub eigen_s: f64, pub host_dense_s: f64, pub sync_wait_s: f64, pub witness_growths: c_int,
     pub extrapolated: c_int }
+#[repr(C)] #[derive(Default, Clone, Copy)] pub struct ks_kernel_time { pub kernel: c_int, pub count: c_int, pub aux: c_int,
+    pub launches: c_int, pub total_ms: f64, pub bytes: f64 }

@@ -15,20 +15,27 @@ def _lines(out):
     return [json.loads(x) for x in out.splitlines() if x.startswith("{")]
 
 
-def _check(line, world):
+def _check(line, world, n=25):
     import bench
     assert line["impl"] == "reference"
     assert line["metric"] == bench.METRIC and line["unit"] == "s" and line["higher_is_better"] is False
-    assert line["config"] == dict(bench.CONFIG, parallelism=f"replicas x{world}")
+    config = dict(bench.CONFIG, parallelism=f"replicas x{world}", grid=n)
+    config["workload"] = bench.CONFIG["workload"].replace("95^3", f"{n}^3")
+    assert line["config"] == config
+    assert line["requested"] == {"steps": 3, "warmup": 2}
+    acc = line["accuracy"]
+    assert acc["status"] == 0 and acc["energy_ha"] < 0 and len(acc["forces"]) == 3
     assert line["value"] > 0 and line["ms_per_step"] == 1000.0 * line["value"]
     cpu = line["cpu_baseline"]
     assert cpu["kind"] == "port" and cpu["cores"] >= 1 and cpu["value"] == line["value"] and "oracle" in cpu["sample"]
+    assert "not extrapolated" in cpu["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert line["n_gpus"] == world and line["steps"] == 1 and line["warmup"] == 0
 
 
 def test_reference_arm_line():
-    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0"], cwd=ROOT,
+    """One full (small-grid) oracle solve timed as one step, whatever K and W were asked for; they are echoed."""
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "3", "--warmup", "2", "--ref-grid", "25"], cwd=ROOT,
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _lines(r.stdout)
@@ -41,7 +48,8 @@ def test_reference_arm_under_torchrun_prints_once():
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
-           "--master-port", str(port), "bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"]
+           "--master-port", str(port), "bench.py", "--impl", "reference", "--gpus", "2", "--steps", "3", "--warmup", "2",
+           "--ref-grid", "25"]
     env = dict(os.environ, OMP_NUM_THREADS="1")
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900, env=env)
     assert r.returncode == 0, r.stderr[-2000:]
@@ -56,6 +64,7 @@ def test_cpu_baseline_entry():
     import bench
     cpu = bench.cpu_baseline_entry()
     assert cpu["kind"] == "port" and cpu["unit"] == "s" and cpu["cores"] == (os.cpu_count() or 1) and cpu["value"] > 0
+    assert cpu["method"] == "extrapolated" and 0 < cpu["measured_sample_s"] < cpu["value"]
     one = cpu["single_thread"]
     assert one["cores"] == 1 and one["value"] > 0 and "oracle" in one["sample"]
     assert set(cpu["stage_s"]) == {"lobpcg_iteration_k5", "poisson_cg_iteration", "lobpcg_iteration_k5_1t",
@@ -64,12 +73,11 @@ def test_cpu_baseline_entry():
     json.dumps(cpu)
 
 
-def test_profiled_traffic_scales_the_committed_capture():
-    """The roofline's traffic: the committed ncu capture (profiles/stencil_hpsi_95.md, 48 vectors) scaled to the
-    bench's 64-vector launch, and within 5 % of the algorithmic (8k + 4) N^3 bytes (0.98: no re-reads; some of the
-    output is still in L2 at the kernel's end); None without a summary."""
+def test_roofline_traffic_constant():
+    """The roofline's traffic: the ncu-measured DRAM bytes per vector of the H psi launch scaled to the bench's
+    64-vector launch, within 5 % of the algorithmic (8k + 4) N^3 bytes (no re-reads; a little of the output is still
+    in L2 at the kernel's end)."""
     import bench
-    t = bench.profiled_traffic(64)
+    t = bench.HPSI_DRAM_BYTES_PER_VECTOR * 64
     algo = (8 * 64 + 4) * 95 ** 3
-    assert t is not None and abs(t / algo - 1.0) < 0.05, (t, algo)
-    assert bench.profiled_traffic(64, prof="/nonexistent/summary.md") is None
+    assert abs(t / algo - 1.0) < 0.05, (t, algo)

@@ -90,6 +90,23 @@ def test_nh3_96_forces_adjoint_and_md(ks, drv):
     assert moved > 1e-3  # the jittered molecule vibrates
 
 
+def test_nh3_96_matches_oracle_record(ks, drv):
+    """NH3 96^3 (h = 0.22, sigma = h, seeded 0.05 Bohr jitter) in the mixed form against a full f64 oracle SCF of the
+    same geometry (tests/golden/oracle_nh3_96.json, tests/golden/make_oracle_configs.py): |dE| < 1e-5 Ha, occupied
+    levels within 1e-5 Ha and forces within 1e-4 Ha/Bohr -- the bars of the reference's GPU-against-CPU checks
+    (crates/validate/tests/gpu_vs_cpu.rs:152-160)."""
+    rec = json.load(open(os.path.join(GOLDEN, "oracle_nh3_96.json")))
+    nuc = drv.nh3(jitter=0.05, seed=0x5EED + 3)
+    assert np.allclose(np.array(nuc), np.array(rec["nuclei"]), atol=0, rtol=0)
+    with ks.GpuSolver(96, 0.22, gram_mode=1, n_extra=3, init_mode=1) as so:
+        st = so.solve(ks.System(nuc, 5, 5), ks.ScfSettings(sigma=0.22, tol=1e-6))
+        f = so.forces(nuc, 0.22)
+        up, dn = so.evals()
+    assert abs(st["energy"]["total"] - rec["stats"]["total"]) < 1e-5, (st["energy"]["total"], rec["stats"]["total"])
+    assert np.abs(up[:5] - np.array(rec["evals_up"])).max() < 1e-5 and np.abs(dn[:5] - np.array(rec["evals_dn"])).max() < 1e-5
+    assert np.abs(f - np.array(rec["forces"])).max() < 1e-4, np.abs(f - np.array(rec["forces"])).max()
+
+
 def test_butane_128_mixed_matches_plain(ks, drv):
     """n-butane (anti, seeded 0.02 Bohr jitter) on 128^3 at h = 0.2: LOBPCG blocks of 20 bands per spin
     (17 occupied in the all-electron model + 3 extra), the tensor-core Gram (m = 60) against the
