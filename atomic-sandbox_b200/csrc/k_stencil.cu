@@ -225,12 +225,9 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
 
     float4 q[9];
     bool alive = true;
-    int waited = 0;  // planes 0..waited-1 arrived (each slot then holds at most one copy in flight)
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const bool got = mbar_wait(&bar[i], 0, p.err, alive ? WAIT_LIMIT : 1);
-        if (got && waited == i) waited = i + 1;
-        alive = alive && got;
+        alive = mbar_wait(&bar[i], 0, p.err, alive ? WAIT_LIMIT : 1) && alive;
         q[i] = lds4(ring + i * PLANE_FLOATS + ci);
     }
     __syncthreads();  // planes 0..3 are consumed: their buffers take planes 8..11
@@ -251,21 +248,21 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
     const long long plane = (long long)p.n * p.P;
     const long long row0 = ((long long)z0 * p.n + gy) * p.P + gx;
     const long long vbase = (long long)vec * p.F;
+    const float* vrow = p.V ? p.V + row0 : nullptr;
+    const float* rrow = p.R ? p.R + vbase + row0 : nullptr;
+    float* orow = out + vbase + row0;
     double dot = 0.0;
     // the compact loop body (not unrolled): unrolled bodies measured slower (the instruction cache)
 #pragma unroll 1
     for (int s = 0; s < nz; ++s) {
         const int qn = s + 8;
-        const bool got = mbar_wait(&bar[qn % NS], (unsigned)((qn / NS) & 1), p.err, alive ? WAIT_LIMIT : 1);
-        if (got && alive) waited = qn + 1;
-        alive = alive && got;
+        alive = mbar_wait(&bar[qn % NS], (unsigned)((qn / NS) & 1), p.err, alive ? WAIT_LIMIT : 1) && alive;
         q[8] = lds4(ring + (qn % NS) * PLANE_FLOATS + ci);
         const float* cpl = ring + ((s + 4) % NS) * PLANE_FLOATS + ci;
-        const long long at = row0 + s * plane;
         // the global reads are issued before the stencil arithmetic, which hides their latency
         const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 v = (MODE != ST_LAPLACIAN && ok) ? ldg4(p.V + at) : zero4;
-        const float4 r = (MODE == ST_JACOBI && ok) ? ldg4(p.R + vbase + at) : zero4;
+        const float4 v = (MODE != ST_LAPLACIAN && ok) ? ldg4(vrow + s * plane) : zero4;
+        const float4 r = (MODE == ST_JACOBI && ok) ? ldg4(rrow + s * plane) : zero4;
         u64 o0, o1;
         lap_quad(cpl, q, kc, o0, o1);
         if (!FOLD_SCALE) {
@@ -280,7 +277,9 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
                 o1 = h1;
             } else {
                 const u64 nl = pk(-lam, -lam);
-                // w + (omega / max(diag_t + V - lambda, 0.1)) (r - (H w - lambda w)), as the scalar sweep
+                // w + (omega / max(diag_t + V - lambda, 0.1)) (r - (H w - lambda w)), as the scalar sweep (an
+                // approximate division measured 2 % faster per solve but moved the NH3 96^3 finite-difference check of
+                // the adjoint past its bound: the sweep keeps the IEEE division)
                 const u64 u0 = sub2(pk(r.x, r.y), fma2(nl, pk(f.x, f.y), h0));
                 const u64 u1 = sub2(pk(r.z, r.w), fma2(nl, pk(f.z, f.w), h1));
                 const float i0 = p.omega * (1.0f / fmaxf(p.diag_t + v.x - lam, 0.1f));
@@ -292,7 +291,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
             }
         }
         if (ok) {
-            *reinterpret_cast<float4*>(out + vbase + at) =
+            *reinterpret_cast<float4*>(orow + s * plane) =
                 make_float4(lo_of(o0), e1 ? hi_of(o0) : 0.f, e2 ? lo_of(o1) : 0.f, e3 ? hi_of(o1) : 0.f);
             if (DOT) dot += quad_dot(f, o0, o1, e1, e2, e3);
         }
@@ -304,8 +303,10 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
 #pragma unroll
         for (int i = 0; i < 8; ++i) q[i] = q[i + 1];  // the z-queue moves up one plane
     }
+    // after a wait gave up: the latest copy issued into each slot may still be in flight (a parity wait on a slot's
+    // latest copy is unambiguous, and returns at once for one that arrived)
     if (threadIdx.x == 0 && !alive)
-        for (int qq = waited; qq < issued; ++qq) mbar_wait(&bar[qq % NS], (unsigned)((qq / NS) & 1), nullptr, DRAIN_LIMIT);
+        for (int qq = max(0, issued - NS); qq < issued; ++qq) mbar_wait(&bar[qq % NS], (unsigned)((qq / NS) & 1), nullptr, DRAIN_LIMIT);
     if (DOT) {
         const double sum = block_sum(dot);
         if (threadIdx.x == 0) p.dot_partials[blockIdx.x + (size_t)gridDim.x * blockIdx.y] = sum;

@@ -222,7 +222,7 @@ def bench_reference(args):
 # DRAM bytes (read + write) per vector of one H psi launch on 95^3 fields, from one ncu capture of this kernel
 # (dram__bytes_read.sum + dram__bytes_write.sum of a 48-vector launch, over 48): the traffic grows with the vectors,
 # every vector being streamed once. Re-measured whenever the stencil changes.
-HPSI_DRAM_BYTES_PER_VECTOR = 325067520 / 48
+HPSI_DRAM_BYTES_PER_VECTOR = (183170560 + 129918976) / 48
 
 
 def hpsi_roofline(torch, ks, peak, source, count=64):
@@ -444,6 +444,18 @@ def bench_batch(args):
     if args.serial:
         _, serial = drv.solve_batch(jobs, workers=1, native=args.native)
     wall, steps = max_over_ranks([wall, 0.0], dev)[0], sum(r["iterations"] for r in results)
+    # outside the timed region: the seeded 8-molecule subset (48^3..64^3) against full f64 oracle SCFs of each
+    accuracy = None
+    rec_path = os.path.join(ROOT, "tests", "golden", "oracle_batch8.json")
+    if rank == 0 and os.path.exists(rec_path):
+        import numpy as np
+        with open(rec_path) as f:
+            recs = json.load(f)["molecules"]
+        sub = drv.batch_workload(count=8, n_min=48, n_max=64)
+        got, _ = drv.solve_batch(sub, workers=args.workers, native=args.native)
+        accuracy = [{"molecule": j["name"], "grid": j["n"], "abs_dE_vs_fp64": abs(g["energy"] - r["stats"]["total"]),
+                     "max_dF_vs_fp64": float(np.abs(np.asarray(g["forces"]) - np.array(r["forces"])).max())}
+                    for j, g, r in zip(sub, got, recs)]
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -454,7 +466,8 @@ def bench_batch(args):
             "scf_steps_rank0": int(steps), "dtype": "f32", "data": "synthetic (seeded templates)", "scaling": "strong",
             "config": {"workload": "batch of seeded molecules, per-molecule cubic grids U{48..96}, h=0.25, sigma=0.5, mixed form",
                        "runtime": "library thread pool (ks_solve_batch)" if args.native else "Python threads over GpuSolver"},
-            "serial_wall_s": serial, "timing": "wall clock around the batch (many solvers and streams)"}
+            "serial_wall_s": serial, "timing": "wall clock around the batch (many solvers and streams)",
+            "accuracy_vs_fp64": accuracy}
     print(json.dumps(line), flush=True)
 
 

@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures of this directory from the reference's own sources (read as
-text; nothing of the reference is executed). Run from the repository root:
+text; nothing of the reference is executed). Run from the repository root, naming the checkout of the
+reference (ItsKodas/atomic-sandbox) to read:
 
-    python tests/golden/make_pins.py /root/reference
+    python tests/golden/make_pins.py PATH_TO_REFERENCE_CHECKOUT
 
 - reference_pins.json: the reference's known answers for the Kohn-Sham path -- the bitwise-pinned
   33^3 Aufbau energies and forces of H2 and LiH (crates/qm/src/scf.rs:1276-1279, geometry :1304-1305),
@@ -87,4 +88,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_pins.py PATH_TO_REFERENCE_CHECKOUT")
+    main(sys.argv[1])

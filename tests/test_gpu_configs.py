@@ -150,3 +150,17 @@ def test_batch_concurrent_equals_one_by_one(ks, drv):
         assert a["energy"] == b["energy"], (j["name"], a["energy"], b["energy"])
         assert np.array_equal(a["forces"], b["forces"])
     assert wall > 0
+
+
+def test_batch_subset_matches_oracle_records(ks, drv):
+    """The same eight seeded batch molecules (H2, NH3, H2O, CH4 on 49^3..59^3 grids) solved concurrently in the mixed
+    form against full f64 oracle SCFs of each (tests/golden/oracle_batch8.json, tests/golden/make_oracle_configs.py):
+    |dE| < 1e-5 Ha and forces within 1e-4 Ha/Bohr per molecule (crates/validate/tests/gpu_vs_cpu.rs:152-160)."""
+    rec = json.load(open(os.path.join(GOLDEN, "oracle_batch8.json")))["molecules"]
+    jobs = drv.batch_workload(count=8, n_min=48, n_max=64)
+    assert [j["n"] for j in jobs] == [r["n"] for r in rec]
+    out, _ = drv.solve_batch(jobs, workers=3)
+    for j, o, r in zip(jobs, out, rec):
+        assert np.array_equal(np.array(j["nuclei"]), np.array(r["nuclei"]))
+        assert abs(o["energy"] - r["stats"]["total"]) < 1e-5, (j["name"], j["n"], o["energy"], r["stats"]["total"])
+        assert np.abs(o["forces"] - np.array(r["forces"])).max() < 1e-4, (j["name"], j["n"])
