@@ -71,6 +71,8 @@ struct Params {
     double* dot_partials;
     int* err;
     int vec0;
+    const double* theta;
+    float* out2;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -244,13 +246,17 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
     kc[3] = pk(C3 * ks, C3 * ks);
     kc[4] = pk(C4 * ks, C4 * ks);
     const u64 scale2 = pk(p.scale, p.scale);
-    const float lam = (MODE == ST_JACOBI) ? (float)p.lambda[vec] : 0.0f;
+    const float lam = (MODE == ST_JACOBI || MODE == ST_HAM_RESIDUAL) ? (float)p.lambda[vec] : 0.0f;
+    // theta split into f32 hi + lo, as the residual kernel does: r = fma(-lo, x, fma(-hi, x, Hx))
+    const double th = (MODE == ST_HAM_RESIDUAL) ? p.theta[vec] : 0.0;
+    const float th_hi = (float)th, th_lo = (float)(th - (double)th_hi);
     const long long plane = (long long)p.n * p.P;
     const long long row0 = ((long long)z0 * p.n + gy) * p.P + gx;
     const long long vbase = (long long)vec * p.F;
     const float* vrow = p.V ? p.V + row0 : nullptr;
     const float* rrow = p.R ? p.R + vbase + row0 : nullptr;
     float* orow = out + vbase + row0;
+    float* orow2 = (MODE == ST_HAM_RESIDUAL) ? p.out2 + vbase + row0 : nullptr;
     double dot = 0.0;
     // the compact loop body (not unrolled): unrolled bodies measured slower (the instruction cache)
 #pragma unroll 1
@@ -275,6 +281,17 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
             if (MODE == ST_HAMILTONIAN) {
                 o0 = h0;
                 o1 = h1;
+            } else if (MODE == ST_HAM_RESIDUAL) {
+                // r = Hx - theta x (hi and lo parts of theta), w0 = r / max(diag_t + V - lambda, 0.1)
+                o0 = fma2(pk(-th_lo, -th_lo), pk(f.x, f.y), fma2(pk(-th_hi, -th_hi), pk(f.x, f.y), h0));
+                o1 = fma2(pk(-th_lo, -th_lo), pk(f.z, f.w), fma2(pk(-th_hi, -th_hi), pk(f.z, f.w), h1));
+                if (ok) {
+                    const float w0 = lo_of(o0) / fmaxf(p.diag_t + v.x - lam, 0.1f);
+                    const float w1 = hi_of(o0) / fmaxf(p.diag_t + v.y - lam, 0.1f);
+                    const float w2 = lo_of(o1) / fmaxf(p.diag_t + v.z - lam, 0.1f);
+                    const float w3 = hi_of(o1) / fmaxf(p.diag_t + v.w - lam, 0.1f);
+                    *reinterpret_cast<float4*>(orow2 + s * plane) = make_float4(w0, e1 ? w1 : 0.f, e2 ? w2 : 0.f, e3 ? w3 : 0.f);
+                }
             } else {
                 const u64 nl = pk(-lam, -lam);
                 // w + (omega / max(diag_t + V - lambda, 0.1)) (r - (H w - lambda w)), as the scalar sweep (an
@@ -293,7 +310,17 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
         if (ok) {
             *reinterpret_cast<float4*>(orow + s * plane) =
                 make_float4(lo_of(o0), e1 ? hi_of(o0) : 0.f, e2 ? lo_of(o1) : 0.f, e3 ? hi_of(o1) : 0.f);
-            if (DOT) dot += quad_dot(f, o0, o1, e1, e2, e3);
+            if (DOT) {
+                if (MODE == ST_HAM_RESIDUAL) {
+                    const double r0 = lo_of(o0), r1 = hi_of(o0), r2 = lo_of(o1), r3 = hi_of(o1);
+                    dot += r0 * r0;
+                    if (e1) dot += r1 * r1;
+                    if (e2) dot += r2 * r2;
+                    if (e3) dot += r3 * r3;
+                } else {
+                    dot += quad_dot(f, o0, o1, e1, e2, e3);
+                }
+            }
         }
         __syncthreads();  // the centre plane's buffer is free
         if (alive && threadIdx.x == 0 && s + 12 < nplanes) {
@@ -309,7 +336,11 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
         for (int qq = max(0, issued - NS); qq < issued; ++qq) mbar_wait(&bar[qq % NS], (unsigned)((qq / NS) & 1), nullptr, DRAIN_LIMIT);
     if (DOT) {
         const double sum = block_sum(dot);
-        if (threadIdx.x == 0) p.dot_partials[blockIdx.x + (size_t)gridDim.x * blockIdx.y] = sum;
+        // [vector][CTA] for the Laplacian / H dots; [CTA][vector] for the residual norms (the residual kernel's layout)
+        if (threadIdx.x == 0) {
+            if (MODE == ST_HAM_RESIDUAL) p.dot_partials[(size_t)blockIdx.x * gridDim.y + blockIdx.y] = sum;
+            else p.dot_partials[blockIdx.x + (size_t)gridDim.x * blockIdx.y] = sum;
+        }
     }
 }
 
@@ -386,11 +417,16 @@ int stencil_ctas(const Layout& L, int count) {
     return sh.tiles_x * sh.tiles_y * sh.chunks * count;
 }
 
+int stencil_ctas_per_vector(const Layout& L, int count) {
+    Shape sh = shape_for(L, count);
+    return sh.tiles_x * sh.tiles_y * sh.chunks;
+}
+
 int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const StencilArgs& a, float* out, cudaStream_t s) {
     if (count <= 0) return 0;
     // the quads' 16-byte loads and stores need 16-byte aligned fields (P is a multiple of 4 floats)
     if ((reinterpret_cast<uintptr_t>(out) & 15) || (a.V && (reinterpret_cast<uintptr_t>(a.V) & 15)) ||
-        (a.R && (reinterpret_cast<uintptr_t>(a.R) & 15)))
+        (a.R && (reinterpret_cast<uintptr_t>(a.R) & 15)) || (a.out2 && (reinterpret_cast<uintptr_t>(a.out2) & 15)))
         throw std::invalid_argument("stencil: fields must be 16-byte aligned");
     Shape sh = shape_for(L, count);
     Params p;
@@ -409,6 +445,8 @@ int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const St
     p.dot_partials = a.dot_partials;
     p.err = device_error_flag();
     p.vec0 = a.vec0;
+    p.theta = a.theta;
+    p.out2 = a.out2;
     const bool dot = a.dot_partials != nullptr;
     switch (a.mode) {
         case ST_LAPLACIAN:
@@ -419,8 +457,12 @@ int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const St
             if (dot) launch_mode<ST_HAMILTONIAN, true>(sh, count, tmap, p, out, s);
             else launch_mode<ST_HAMILTONIAN, false>(sh, count, tmap, p, out, s);
             break;
+        case ST_HAM_RESIDUAL:
+            if (!dot || !a.theta || !a.lambda || !a.out2 || !a.V) throw std::invalid_argument("stencil: the residual form needs theta, lambda, V, W0 and partials");
+            launch_mode<ST_HAM_RESIDUAL, true>(sh, count, tmap, p, out, s);
+            break;
         default:
-            if (dot) throw std::invalid_argument("stencil: dot partials are for the Laplacian and H only");
+            if (dot) throw std::invalid_argument("stencil: dot partials are for the Laplacian, H and the residual form only");
             launch_mode<ST_JACOBI, false>(sh, count, tmap, p, out, s);
             break;
     }

@@ -61,7 +61,10 @@ void launch_extrapolate(long long F, const float* cur, const float* prev, float*
 void launch_scale_ratio(long long F, float* x, const double* sum_dev, double target, cudaStream_t s);
 
 // ---------------------------------------------------------------- stencil (k_stencil.cu)
-enum StencilMode { ST_LAPLACIAN = 0, ST_HAMILTONIAN = 1, ST_JACOBI = 2 };
+// ST_HAM_RESIDUAL: H x followed, in the same pass, by the LOBPCG residual r = Hx - theta x, the first Jacobi sweep
+// w0 = r / max(diag_t + V - lambda, 0.1) and the |r|^2 partials -- what launch_residual_precond computes from a stored
+// Hx, bit for bit (out = R, out2 = W0; dot_partials = [CTAs per vector][count] f64 sums of r^2, dv not applied).
+enum StencilMode { ST_LAPLACIAN = 0, ST_HAMILTONIAN = 1, ST_JACOBI = 2, ST_HAM_RESIDUAL = 3 };
 struct StencilArgs {
     int mode = ST_LAPLACIAN;
     float scale = 0;        // multiplies sum_m c_m (second differences): 1/h^2 or -1/(2 h^2)
@@ -71,7 +74,11 @@ struct StencilArgs {
     float omega = 0, diag_t = 0;
     double* dot_partials = nullptr; // optional: sum_points x*out per CTA (Poisson's p.Ap), [CTAs] f64
     int vec0 = 0;               // first vector of the tensor map's block to read (outputs, R, lambda are indexed from 0)
+    const double* theta = nullptr;  // HAM_RESIDUAL: Ritz value per vector (device f64)
+    float* out2 = nullptr;          // HAM_RESIDUAL: the first sweep W0 (block, stride F)
 };
+// CTAs per vector of a stencil launch of `count` vectors (the leading dimension of ST_HAM_RESIDUAL's partials)
+int stencil_ctas_per_vector(const Layout& L, int count);
 // out_v = op(x_v) for the `count` vectors of the block x (stride F). `tmap` must describe x
 // (make_field_tmap). Returns the number of CTAs launched (for dot partials).
 int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const StencilArgs& a, float* out, cudaStream_t s);

@@ -912,19 +912,30 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
     bool have_prev = false;
     std::vector<double> prev_theta;
     std::vector<double> res(k);
+    // the H X launch that ends an iteration also forms the next residual, its first Jacobi sweep and the |r|^2
+    // partials (ST_HAM_RESIDUAL, bit for bit the residual kernel's R and W0); a pseudopotential's V_NL is added after
+    // the stencil, so under one the residual kernel runs on the stored H X instead
+    const int nb = lane.red.blocks();
+    const int cpv = stencil_ctas_per_vector(L_, k);
+    const size_t norm_cap = (size_t)std::max(nb, cpv) * k;
+    if (lane.norm_part.bytes < norm_cap * sizeof(double)) lane.norm_part.alloc(norm_cap * sizeof(double));
+    double* norm_partials = lane.norm_part.d();  // finished in the Gram's finish launch
+    bool fused_r = false;
+    int norm_blocks = nb;
     for (;;) {
         // the inner cancellation point (crates/qm-gpu/src/scf.rs:1224-1235): the calling thread polls, every channel obeys
         if (inner_fn_ && std::this_thread::get_id() == poll_thread_ && inner_fn_(inner_user_)) inner_flag_.store(1);
         if (inner_flag_.load()) throw AbortInside();
         Block& S = ch.A[ch.cur];
         // 1. R = HX - theta X with the first Jacobi sweep fused (into Q), then 3 damped sweeps Q -> W -> Q -> W
-        const int nb = lane.red.blocks();
-        if (lane.norm_part.bytes < (size_t)nb * k * sizeof(double)) lane.norm_part.alloc((size_t)nb * k * sizeof(double));
-        double* norm_partials = lane.norm_part.d();  // finished in the Gram's finish launch below
-        timer_.time(KS_K_RESIDUAL, k, 0, (16.0 * k + 4.0) * npts, lane.s, [&] {
-            launch_residual_precond(L_, k, ch.HX.at(0), ch.X(), theta_d, V, lambda_d, diag_t, ch.T.at(0), ch.Q.at(0), norm_partials, nb,
-                                    lane.s);
-        });
+        if (!fused_r) {
+            timer_.time(KS_K_RESIDUAL, k, 0, (16.0 * k + 4.0) * npts, lane.s, [&] {
+                launch_residual_precond(L_, k, ch.HX.at(0), ch.X(), theta_d, V, lambda_d, diag_t, ch.T.at(0), ch.Q.at(0), norm_partials,
+                                        nb, lane.s);
+            });
+            norm_blocks = nb;
+        }
+        fused_r = false;
         const int m = 2 * k + np;
         const int off_norm = m * 2 * m;
         StencilArgs jac;
@@ -947,7 +958,7 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         // 3. the readback: G = S^T [S | T] and |r_i|^2
         FinishDesc norms;
         norms.partials = norm_partials;
-        norms.blocks = nb;
+        norms.blocks = norm_blocks;
         norms.nvals = k;
         norms.scale = L_.h * L_.h * L_.h;
         norms.out = lane.red.res() + off_norm;
@@ -1067,8 +1078,24 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
                     [&] { launch_block_lincomb(L_.F, m, S.at(0), 2 * k, coef_d, ch.A[next].at(0), k, k, lane.s); });
         ch.cur = next;
         np = k;
-        // 6. HX of the new X
-        apply_h(ch.A[ch.cur], 0, k, ch.HX.at(0));
+        // 6. HX of the new X -- with the next iteration's residual, first sweep and |r|^2 partials formed in the same pass
+        if (!nl_on_) {
+            StencilArgs a;
+            a.mode = ST_HAM_RESIDUAL;
+            a.scale = ham_scale;
+            a.V = V;
+            a.theta = theta_d;
+            a.lambda = lambda_d;
+            a.diag_t = (float)diag_t;
+            a.out2 = ch.Q.at(0);
+            a.dot_partials = norm_partials;
+            timer_.time(KS_K_HPSI_RESIDUAL, k, 0, (12.0 * k + 4.0) * npts, lane.s,
+                        [&] { launch_stencil(L_, ch.A[ch.cur].tmap, k, a, ch.T.at(0), lane.s); });
+            fused_r = true;
+            norm_blocks = cpv;
+        } else {
+            apply_h(ch.A[ch.cur], 0, k, ch.HX.at(0));
+        }
     }
     es.readbacks = lane.red.readbacks - rb0;
     return es;

@@ -64,7 +64,7 @@ class _KernelTime(ctypes.Structure):
                 ("total_ms", ctypes.c_double), ("bytes", ctypes.c_double)]
 
 
-KERNEL_NAMES = {0: "hpsi", 1: "jacobi", 2: "residual_precond", 3: "gram", 4: "block_update"}
+KERNEL_NAMES = {0: "hpsi", 1: "jacobi", 2: "residual_precond", 3: "gram", 4: "block_update", 5: "hpsi_residual"}
 
 ABORT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
 

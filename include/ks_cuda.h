@@ -93,7 +93,7 @@ typedef struct {
    block update, else 0), launches, their summed device time (CUDA events on the stream they ran on) and the
    algorithmic bytes of one launch (what it must read and write once, on the n^3 interior points). */
 typedef struct { int kernel, count, aux, launches; double total_ms, bytes; } ks_kernel_time;
-enum { KS_K_HPSI = 0, KS_K_JACOBI = 1, KS_K_RESIDUAL = 2, KS_K_GRAM = 3, KS_K_BLOCK_UPDATE = 4 };
+enum { KS_K_HPSI = 0, KS_K_JACOBI = 1, KS_K_RESIDUAL = 2, KS_K_GRAM = 3, KS_K_BLOCK_UPDATE = 4, KS_K_HPSI_RESIDUAL = 5 };
 
 /* Polled before every SCF step (GpuSolver::solve_with, crates/qm-gpu/src/scf.rs:1208): nonzero abandons the solve. */
 typedef int (*ks_abort_fn)(void* user);
