@@ -198,18 +198,23 @@ __global__ void __launch_bounds__(LCB) block_lincomb_kernel(long long F4, int m,
         cs[jj * 64 + i] = ((unsigned long long)__float_as_uint(c) << 32) | __float_as_uint(c);
     }
     __syncthreads();
-    // bounded wait on the copies: on timeout the error flag is raised (the host's next readback reports it)
-    for (long long n = 0;; ++n) {
-        unsigned ok;
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-                     : "=r"(ok)
-                     : "r"(lc_su32(&bar))
-                     : "memory");
-        if (ok) break;
-        if (n > LC_WAIT_LIMIT) {
-            if (err) atomicExch(err, 1);
-            break;
+    // bounded wait on the copies: on timeout the error flag is raised (the host's next readback reports it) and the
+    // outputs are undefined; a second bounded wait then gives the copies in flight time to land before the CTA exits
+    // and its shared memory is reused
+    auto wait_copies = [&](long long limit) {
+        for (long long n = 0;; ++n) {
+            unsigned ok;
+            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                         : "=r"(ok)
+                         : "r"(lc_su32(&bar))
+                         : "memory");
+            if (ok) return true;
+            if (n > limit) return false;
         }
+    };
+    if (!wait_copies(LC_WAIT_LIMIT)) {
+        if (err) atomicExch(err, 1);
+        wait_copies(1LL << 16);
     }
     const int tid = threadIdx.x;
     if (tid >= cnt) return;
@@ -237,118 +242,10 @@ __global__ void __launch_bounds__(LCB) block_lincomb_kernel(long long F4, int m,
         }
 }
 
-// The persistent form for m <= LC2_MAX_M inputs: each CTA walks chunks gridDim.x apart with two shared-memory slices,
-// the bulk copies of the next chunk in flight while the current one is combined (the one-shot form above loads, then
-// computes, then stores, and only the other resident CTAs overlap its phases). Same per-element arithmetic and order:
-// bitwise the same outputs.
-constexpr int LC2_MAX_M = 48;  // two m x 2 KB slices per CTA: 192 KB at m = 48
-__device__ __forceinline__ bool lc_wait(uint64_t* bar, unsigned parity, long long limit) {
-    for (long long n = 0;; ++n) {
-        unsigned ok;
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-                     : "=r"(ok)
-                     : "r"(lc_su32(bar)), "r"(parity)
-                     : "memory");
-        if (ok) return true;
-        if (n > limit) return false;
-    }
-}
-
-__global__ void __launch_bounds__(LCB) block_lincomb2_kernel(long long F4, int m, const ulonglong2* __restrict__ S, int q,
-                                                             const double* __restrict__ C, ulonglong2* __restrict__ out, int split,
-                                                             int gap, long long nchunks, int* err) {
-    extern __shared__ __align__(128) ulonglong2 sv2[];  // 2 slices of m x LCB
-    __shared__ unsigned long long cs[64 * QG];          // (c, c) pairs
-    __shared__ __align__(8) uint64_t bar[2];
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(lc_su32(&bar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(lc_su32(&bar[1])) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    // one bulk copy per field of chunk c into slice b (lanes of warp 0)
-    auto issue = [&](long long c, int b) {
-        const long long e0 = c * LCB;
-        const unsigned bytes = (unsigned)min((long long)LCB, F4 - e0) * 16u;
-        if (threadIdx.x == 0)
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(lc_su32(&bar[b])), "r"(bytes * (unsigned)m)
-                         : "memory");
-        __syncwarp();
-        for (int i = threadIdx.x; i < m; i += 32)
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                             lc_su32(sv2 + ((size_t)b * m + i) * LCB)),
-                         "l"(S + (long long)i * F4 + e0), "r"(bytes), "r"(lc_su32(&bar[b]))
-                         : "memory");
-    };
-    long long c = blockIdx.x;
-    // thread 0's record of the copies in flight per slice (for the drain after a wait gave up)
-    unsigned pending = 0u, pend_par = 0u;  // bit b: slice b has a copy in flight / the parity it completes
-    if (threadIdx.x < 32 && c < nchunks) issue(c, 0);
-    if (c < nchunks) pending = 1u;
-    const int j0 = blockIdx.y * QG;
-    const int qn = min(QG, q - j0);
-    for (int t = threadIdx.x; t < m * qn; t += blockDim.x) {
-        int i = t % m, jj = t / m;
-        const float cf = (float)C[i + (size_t)m * (j0 + jj)];
-        cs[jj * 64 + i] = ((unsigned long long)__float_as_uint(cf) << 32) | __float_as_uint(cf);
-    }
-    __syncthreads();
-    bool alive = true;
-    int it = 0;
-    for (; c < nchunks; c += gridDim.x, ++it) {
-        const int b = it & 1;
-        // the other slice was released by the barrier that ended the previous chunk: prefetch the next chunk into it
-        if (alive && c + gridDim.x < nchunks) {
-            if (threadIdx.x < 32) issue(c + gridDim.x, b ^ 1);
-            pending |= 1u << (b ^ 1);
-            pend_par = (pend_par & ~(1u << (b ^ 1))) | ((unsigned)(((it + 1) >> 1) & 1) << (b ^ 1));
-        }
-        if (lc_wait(&bar[b], (unsigned)((it >> 1) & 1), alive ? LC_WAIT_LIMIT : 1)) {
-            pending &= ~(1u << b);
-        } else {
-            if (alive && err) atomicExch(err, 1);
-            alive = false;  // outputs undefined; the host's next readback reports the error
-        }
-        const long long e0 = c * LCB;
-        const int cnt = (int)min((long long)LCB, F4 - e0);
-        const int tid = threadIdx.x;
-        if (tid < cnt) {
-            const ulonglong2* slice = sv2 + (size_t)b * m * LCB;
-            unsigned long long acc[QG][2];
-#pragma unroll
-            for (int jj = 0; jj < QG; ++jj) acc[jj][0] = acc[jj][1] = 0ull;
-#pragma unroll 4
-            for (int i = 0; i < m; ++i) {
-                const ulonglong2 v = slice[(size_t)i * LCB + tid];
-#pragma unroll
-                for (int jj = 0; jj < QG; ++jj) {
-                    if (jj < qn) {
-                        const unsigned long long c2 = cs[jj * 64 + i];
-                        acc[jj][0] = lc_fma2(c2, v.x, acc[jj][0]);
-                        acc[jj][1] = lc_fma2(c2, v.y, acc[jj][1]);
-                    }
-                }
-            }
-            const long long e = e0 + tid;
-#pragma unroll
-            for (int jj = 0; jj < QG; ++jj)
-                if (jj < qn) {
-                    const int j = j0 + jj;
-                    out[(long long)(j < split ? j : j + gap) * F4 + e] = make_ulonglong2(acc[jj][0], acc[jj][1]);
-                }
-        }
-        __syncthreads();  // slice b is free for the copy issued at the next chunk but one
-    }
-    // after a wait gave up: the copies still in flight land before the CTA's shared memory is released
-    if (!alive && threadIdx.x == 0)
-        for (int b = 0; b < 2; ++b)
-            if (pending & (1u << b)) lc_wait(&bar[b], (pend_par >> b) & 1u, 1LL << 16);
-}
-
-__global__ void residual_precond_kernel(long long F4, const float4* __restrict__ HX, const float4* __restrict__ X,
+__global__ void residual_precond_kernel(long long F4, const float4* HX, const float4* __restrict__ X,
                                         const double* __restrict__ theta, const float4* __restrict__ V,
                                         const double* __restrict__ lambda, float diag_t, float4* __restrict__ R,
-                                        float4* __restrict__ W0, double* __restrict__ partials) {
+                                        float4* __restrict__ W0, double* __restrict__ partials, float omega, float4* Dinv) {
     const int v = blockIdx.y;
     const double th = theta[v];
     const float hi = (float)th;
@@ -370,6 +267,14 @@ __global__ void residual_precond_kernel(long long F4, const float4* __restrict__
         w.z = r.z / fmaxf(diag_t + vv.z - lam, 0.1f);
         w.w = r.w / fmaxf(diag_t + vv.w - lam, 0.1f);
         W0[off + e] = w;
+        if (Dinv) {  // the later sweeps' factor, as they compute it (HX[off + e] was read above: Dinv may be HX)
+            float4 d;
+            d.x = omega * (1.0f / fmaxf(diag_t + vv.x - lam, 0.1f));
+            d.y = omega * (1.0f / fmaxf(diag_t + vv.y - lam, 0.1f));
+            d.z = omega * (1.0f / fmaxf(diag_t + vv.z - lam, 0.1f));
+            d.w = omega * (1.0f / fmaxf(diag_t + vv.w - lam, 0.1f));
+            Dinv[off + e] = d;
+        }
         acc += (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z + (double)r.w * r.w;
     }
     double s = block_sum(acc);
@@ -573,20 +478,7 @@ void launch_block_lincomb(long long F, int m, const float* S, int q, const doubl
     static std::atomic<unsigned long long> attr_set{0};
     once_per_device(attr_set, [] {  // 64 fields x LCB float4 of dynamic shared memory at most
         KS_CUDA(cudaFuncSetAttribute(block_lincomb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * LCB * 16));
-        KS_CUDA(cudaFuncSetAttribute(block_lincomb2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * LC2_MAX_M * LCB * 16));
     });
-    const long long nchunks = (F4 + LCB - 1) / LCB;
-    if (m <= LC2_MAX_M) {
-        // persistent CTAs: as many as the slices let reside per SM (2 x m x 2 KB each), never more than the chunks
-        const int per_sm = std::max(1, std::min(8, (int)((200LL * 1024) / (2LL * m * LCB * 16))));
-        const long long ctas = std::min(nchunks, (long long)per_sm * sm_count());
-        dim3 grid2((unsigned)ctas, ceil_div(q, QG));
-        block_lincomb2_kernel<<<grid2, LCB, (size_t)2 * m * LCB * 16, s>>>(F4, m, reinterpret_cast<const ulonglong2*>(S), q, C,
-                                                                          reinterpret_cast<ulonglong2*>(out), split, gap, nchunks,
-                                                                          device_error_flag());
-        KS_LAUNCH_CHECK();
-        return;
-    }
     dim3 grid((unsigned)((F4 + LCB - 1) / LCB), ceil_div(q, QG));
     block_lincomb_kernel<<<grid, LCB, (size_t)m * LCB * 16, s>>>(F4, m, reinterpret_cast<const ulonglong2*>(S), q, C,
                                                                  reinterpret_cast<ulonglong2*>(out), split, gap, device_error_flag());
@@ -594,11 +486,13 @@ void launch_block_lincomb(long long F, int m, const float* S, int q, const doubl
 }
 
 void launch_residual_precond(const Layout& L, int k, const float* HX, const float* X, const double* theta, const float* V,
-                             const double* lambda, double diag_t, float* R, float* W0, double* partials, int blocks, cudaStream_t s) {
+                             const double* lambda, double diag_t, float* R, float* W0, double* partials, int blocks, cudaStream_t s,
+                             float omega, float* dinv) {
     dim3 grid(blocks, k);
     residual_precond_kernel<<<grid, TPB, 0, s>>>(L.F / 4, reinterpret_cast<const float4*>(HX), reinterpret_cast<const float4*>(X),
                                                  theta, reinterpret_cast<const float4*>(V), lambda, (float)diag_t,
-                                                 reinterpret_cast<float4*>(R), reinterpret_cast<float4*>(W0), partials);
+                                                 reinterpret_cast<float4*>(R), reinterpret_cast<float4*>(W0), partials, omega,
+                                                 reinterpret_cast<float4*>(dinv));
     KS_LAUNCH_CHECK();
 }
 

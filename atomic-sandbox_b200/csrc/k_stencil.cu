@@ -73,6 +73,7 @@ struct Params {
     int vec0;
     const double* theta;
     float* out2;
+    float* dinv;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -257,6 +258,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
     const float* rrow = p.R ? p.R + vbase + row0 : nullptr;
     float* orow = out + vbase + row0;
     float* orow2 = (MODE == ST_HAM_RESIDUAL) ? p.out2 + vbase + row0 : nullptr;
+    float* drow = p.dinv ? p.dinv + vbase + row0 : nullptr;
     double dot = 0.0;
     // the compact loop body (not unrolled): unrolled bodies measured slower (the instruction cache)
 #pragma unroll 1
@@ -269,6 +271,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
         const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 v = (MODE != ST_LAPLACIAN && ok) ? ldg4(vrow + s * plane) : zero4;
         const float4 r = (MODE == ST_JACOBI && ok) ? ldg4(rrow + s * plane) : zero4;
+        const float4 dq = (MODE == ST_JACOBI && ok && drow) ? ldg4(drow + s * plane) : zero4;
         u64 o0, o1;
         lap_quad(cpl, q, kc, o0, o1);
         if (!FOLD_SCALE) {
@@ -291,6 +294,13 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
                     const float w2 = lo_of(o1) / fmaxf(p.diag_t + v.z - lam, 0.1f);
                     const float w3 = hi_of(o1) / fmaxf(p.diag_t + v.w - lam, 0.1f);
                     *reinterpret_cast<float4*>(orow2 + s * plane) = make_float4(w0, e1 ? w1 : 0.f, e2 ? w2 : 0.f, e3 ? w3 : 0.f);
+                    if (drow) {  // the sweeps' factor, as the JACOBI mode computes it
+                        const float d0 = p.omega * (1.0f / fmaxf(p.diag_t + v.x - lam, 0.1f));
+                        const float d1 = p.omega * (1.0f / fmaxf(p.diag_t + v.y - lam, 0.1f));
+                        const float d2 = p.omega * (1.0f / fmaxf(p.diag_t + v.z - lam, 0.1f));
+                        const float d3 = p.omega * (1.0f / fmaxf(p.diag_t + v.w - lam, 0.1f));
+                        *reinterpret_cast<float4*>(drow + s * plane) = make_float4(d0, e1 ? d1 : 0.f, e2 ? d2 : 0.f, e3 ? d3 : 0.f);
+                    }
                 }
             } else {
                 const u64 nl = pk(-lam, -lam);
@@ -299,10 +309,18 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
                 // the adjoint past its bound: the sweep keeps the IEEE division)
                 const u64 u0 = sub2(pk(r.x, r.y), fma2(nl, pk(f.x, f.y), h0));
                 const u64 u1 = sub2(pk(r.z, r.w), fma2(nl, pk(f.z, f.w), h1));
-                const float i0 = p.omega * (1.0f / fmaxf(p.diag_t + v.x - lam, 0.1f));
-                const float i1 = p.omega * (1.0f / fmaxf(p.diag_t + v.y - lam, 0.1f));
-                const float i2 = p.omega * (1.0f / fmaxf(p.diag_t + v.z - lam, 0.1f));
-                const float i3 = p.omega * (1.0f / fmaxf(p.diag_t + v.w - lam, 0.1f));
+                float i0, i1, i2, i3;
+                if (drow) {  // the factor stored by the residual pass of this iteration
+                    i0 = dq.x;
+                    i1 = dq.y;
+                    i2 = dq.z;
+                    i3 = dq.w;
+                } else {
+                    i0 = p.omega * (1.0f / fmaxf(p.diag_t + v.x - lam, 0.1f));
+                    i1 = p.omega * (1.0f / fmaxf(p.diag_t + v.y - lam, 0.1f));
+                    i2 = p.omega * (1.0f / fmaxf(p.diag_t + v.z - lam, 0.1f));
+                    i3 = p.omega * (1.0f / fmaxf(p.diag_t + v.w - lam, 0.1f));
+                }
                 o0 = fma2(pk(i0, i1), u0, pk(f.x, f.y));
                 o1 = fma2(pk(i2, i3), u1, pk(f.z, f.w));
             }
@@ -426,7 +444,8 @@ int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const St
     if (count <= 0) return 0;
     // the quads' 16-byte loads and stores need 16-byte aligned fields (P is a multiple of 4 floats)
     if ((reinterpret_cast<uintptr_t>(out) & 15) || (a.V && (reinterpret_cast<uintptr_t>(a.V) & 15)) ||
-        (a.R && (reinterpret_cast<uintptr_t>(a.R) & 15)) || (a.out2 && (reinterpret_cast<uintptr_t>(a.out2) & 15)))
+        (a.R && (reinterpret_cast<uintptr_t>(a.R) & 15)) || (a.out2 && (reinterpret_cast<uintptr_t>(a.out2) & 15)) ||
+        (a.dinv && (reinterpret_cast<uintptr_t>(a.dinv) & 15)))
         throw std::invalid_argument("stencil: fields must be 16-byte aligned");
     Shape sh = shape_for(L, count);
     Params p;
@@ -447,6 +466,7 @@ int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const St
     p.vec0 = a.vec0;
     p.theta = a.theta;
     p.out2 = a.out2;
+    p.dinv = a.dinv;
     const bool dot = a.dot_partials != nullptr;
     switch (a.mode) {
         case ST_LAPLACIAN:

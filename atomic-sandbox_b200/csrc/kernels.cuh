@@ -39,8 +39,11 @@ void launch_block_lincomb(long long F, int m, const float* S, int q, const doubl
 // LOBPCG residual, first Jacobi sweep and |r|^2 partials in one pass (crates/qm-gpu/src/eigen.rs:743-759):
 //   R_i = HX_i - th_hi_i X_i - th_lo_i X_i,  W0_i = R_i / max(diag_t + V - lambda_i, 0.1)
 // theta/lambda device f64 [k]; partials: [blocks][k] f64 of sum R_i^2 (dv not applied).
+// With dinv set, each vector's sweep factor omega / max(diag_t + V - lambda, 0.1) is written there too (dinv may be HX
+// itself: each element is read before it is overwritten).
 void launch_residual_precond(const Layout& L, int k, const float* HX, const float* X, const double* theta, const float* V,
-                             const double* lambda, double diag_t, float* R, float* W0, double* partials, int blocks, cudaStream_t s);
+                             const double* lambda, double diag_t, float* R, float* W0, double* partials, int blocks, cudaStream_t s,
+                             float omega = 0.f, float* dinv = nullptr);
 // XC (LSDA: Slater exchange + PW92, crates/qm/src/xc.rs:88-207) on (up, dn), f64 arithmetic, and the
 // effective potentials v_sigma = vnuc + vh + vxc_sigma. exc gets n*eps_xc. With a partial core pc, XC runs on
 // (up + pc/2, dn + pc/2).
@@ -76,6 +79,9 @@ struct StencilArgs {
     int vec0 = 0;               // first vector of the tensor map's block to read (outputs, R, lambda are indexed from 0)
     const double* theta = nullptr;  // HAM_RESIDUAL: Ritz value per vector (device f64)
     float* out2 = nullptr;          // HAM_RESIDUAL: the first sweep W0 (block, stride F)
+    // the sweep's per-point factor omega / max(diag_t + V - lambda, 0.1) of each vector (block, stride F): written by
+    // HAM_RESIDUAL when set, read by JACOBI when set (else JACOBI computes it, to the same bits)
+    float* dinv = nullptr;
 };
 // CTAs per vector of a stencil launch of `count` vectors (the leading dimension of ST_HAM_RESIDUAL's partials)
 int stencil_ctas_per_vector(const Layout& L, int count);

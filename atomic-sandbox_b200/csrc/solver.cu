@@ -931,7 +931,7 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         if (!fused_r) {
             timer_.time(KS_K_RESIDUAL, k, 0, (16.0 * k + 4.0) * npts, lane.s, [&] {
                 launch_residual_precond(L_, k, ch.HX.at(0), ch.X(), theta_d, V, lambda_d, diag_t, ch.T.at(0), ch.Q.at(0), norm_partials,
-                                        nb, lane.s);
+                                        nb, lane.s, (float)omega, ch.HX.at(0));
             });
             norm_blocks = nb;
         }
@@ -946,8 +946,9 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         jac.lambda = lambda_d;
         jac.omega = (float)omega;
         jac.diag_t = (float)diag_t;
+        jac.dinv = ch.HX.at(0);  // the sweep factors of this iteration (H X itself is not needed past the residual)
         jac.vec0 = 0;
-        const double jac_bytes = (12.0 * k + 4.0) * npts;
+        const double jac_bytes = (16.0 * k + 4.0) * npts;  // w, r and the stored factor in, w' out, V once
         timer_.time(KS_K_JACOBI, k, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), lane.s); });   // Q -> W
         jac.vec0 = k;
         timer_.time(KS_K_JACOBI, k, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, S.tmap, k, jac, ch.Q.at(0), lane.s); });   // W -> Q
@@ -1088,8 +1089,10 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
             a.lambda = lambda_d;
             a.diag_t = (float)diag_t;
             a.out2 = ch.Q.at(0);
+            a.omega = (float)omega;
+            a.dinv = ch.HX.at(0);
             a.dot_partials = norm_partials;
-            timer_.time(KS_K_HPSI_RESIDUAL, k, 0, (12.0 * k + 4.0) * npts, lane.s,
+            timer_.time(KS_K_HPSI_RESIDUAL, k, 0, (16.0 * k + 4.0) * npts, lane.s,  // x in; r, w0, factors out; V once
                         [&] { launch_stencil(L_, ch.A[ch.cur].tmap, k, a, ch.T.at(0), lane.s); });
             fused_r = true;
             norm_blocks = cpv;

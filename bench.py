@@ -263,7 +263,8 @@ def hpsi_roofline(torch, ks, peak, source, count=64):
 def in_scf_rooflines(kernels, peak, source):
     """The LOBPCG chain's kernels as one solve launches them (the library's per-shape CUDA-event timing): per shape the
     launches, mean device time, algorithmic bytes per launch (n^3 interior points: H psi (8k + 4), Jacobi sweep
-    (12k + 4), residual + first sweep (16k + 4), Gram 4 (m + mt), block update 4 (m + q) bytes per point) and the
+    (16k + 4: w, r and the stored sweep factor in, w' out, V once), H x with the residual, first sweep and sweep factors
+    (16k + 4), residual + first sweep (16k + 4), Gram 4 (m + mt), block update 4 (m + q) bytes per point) and the
     fraction of the HBM peak; `dominant` is the shape with the largest total device time. The SCF's 95^3 blocks of
     8 and 16 vectors partly fit the 126 MB L2, so these fractions are of achieved algorithmic bandwidth, not DRAM."""
     rows = []

@@ -58,6 +58,11 @@ def test_null_handles_and_bad_sizes_return_invalid(ks):
     assert lib.ks_rayleigh_ritz(4, p, p, 5, p, p, p) == ks.KS_INVALID  # nk > m
     assert lib.ks_footprint_bytes(4, 1, 1, None, 6, 0) == -1
     assert lib.ks_footprint_bytes(33, -1, 1, None, 6, 0) == -1
+    assert lib.ks_set_kernel_timing(None, 1) == ks.KS_INVALID
+    assert lib.ks_kernel_times(None, None, 0) < 0
+    assert lib.ks_state_import(None, 1, 0, 1, p, p, 0, p, p, p, p, p, 0, None, None) == ks.KS_INVALID
+    assert lib.ks_test_poison_parked_density(None) == ks.KS_INVALID
+    assert lib.ks_test_fail_readbacks(None, 0, 1) == ks.KS_INVALID
     assert lib.ks_last_error(None)  # a message for the last refusal
 
 
@@ -73,3 +78,5 @@ def test_no_device_fails_loudly(ks):
         ks.GpuSolver(33, 0.25, gram_mode=1, n_extra=3, init_mode=1)
     with pytest.raises(ks.Device):
         ks.apply_laplacian(33, 0.25, np.zeros(33 ** 3))
+    # the wait-timeout status of the device-pointer calls needs a device too: a status, not a trap
+    assert lib.ks_device_status(None) == ks.KS_DEVICE
