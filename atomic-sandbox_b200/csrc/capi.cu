@@ -758,7 +758,8 @@ ks_status ks_device_status(void* stream) {
 ks_status ks_gram_device_noalloc(void* stream, int n, int m, const float* s, int mt, const float* t, double* out) {
     if (n < 5 || n > 1024 || m < 1 || mt < 0 || !s || (mt > 0 && !t) || !out) return fail(nullptr, KS_INVALID, "invalid arguments");
     return guarded(nullptr, [&] {
-        // the same grid as the solver's CUDA-core Gram (Reducer::init), hence the same partials and result
+        // the solver's CUDA-core Gram kernel and grid, hence the same partials and result; it writes at most 2 * SMs
+        // partial blocks, the bound the scratch is sized against
         const int blocks = 2 * sm_count();
         const size_t need = (size_t)blocks * m * (m + mt);
         if (need > NOALLOC_PARTIALS)
@@ -767,8 +768,8 @@ ks_status ks_gram_device_noalloc(void* stream, int n, int m, const float* s, int
         double* partials = noalloc_partials();
         const Layout L = Layout::make(n, 1.0);
         cudaStream_t st = static_cast<cudaStream_t>(stream);
-        launch_gram(L.F, m, s, mt, mt > 0 ? t : s, partials, blocks, st);
-        launch_finish(partials, blocks, m * (m + mt), 1.0, out, st);
+        const int written = launch_gram(L.F, m, s, mt, mt > 0 ? t : s, partials, st);
+        launch_finish(partials, written, m * (m + mt), 1.0, out, st);
         return KS_OK;
     });
 }

@@ -7,6 +7,7 @@
 // compensation. The same inputs therefore give the same bits on every run, and no host round
 // trip is needed until a scalar is actually wanted on the host.
 #include <cmath>
+#include <cudaTypedefs.h>
 #include "kernels.cuh"
 #include "reduce_util.cuh"
 #include "harmonics.cuh"
@@ -147,6 +148,161 @@ __global__ void __launch_bounds__(GW * 32) gram_kernel(long long F, int m, const
             double v = warp_sum((double)acc[a][b]);
             if (lane == 0 && r0 + a < m && c0 + b < mc) partials[base + (size_t)(r0 + a) * mc + (c0 + b)] = v;
         }
+}
+
+// ---- the Gram block on CUDA cores with the chunk staged in shared memory (blocks whose tiles fit one CTA).
+// The CTA's warps cover every 8 x 8 tile of G, so each field value is read from HBM once for all of them: per chunk of
+// 32 points, two TMA boxes (the 32-point slab of the m rows of S, and of the mt rows of T) land in a shared-memory
+// slice, with the next G2_RING - 1 chunks in flight. Lane l owns point l of each chunk; the arithmetic is the form
+// above (f32 per lane over its points, f64 across the lanes). S^T S is symmetric bit for bit (the same products in the
+// same order), so only its upper tiles are computed and each off-diagonal one is also written transposed: at
+// m = mt = 24 that is 6 + 9 = 15 tiles, one warp each.
+constexpr int G2_MAX_TILES = 16;  // warps per CTA (512 threads: up to 128 registers each)
+constexpr int G2_RING = 8;        // shared-memory slices: the next G2_RING - 1 chunks in flight
+constexpr long long G2_WAIT_LIMIT = 1LL << 22;
+// a 32-point box's inner extent is 128 bytes and its x coordinate a multiple of 32 floats: both multiples of 16 bytes,
+// as TMA requires (a violation faults the GPU instead of returning an error)
+static_assert((32 * 4) % 16 == 0, "TMA box inner extent and x coordinates must be multiples of 16 bytes");
+__device__ __forceinline__ unsigned g2_su32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool g2_wait(uint64_t* bar, unsigned parity, long long limit) {
+    for (long long n = 0;; ++n) {
+        unsigned ok;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(ok)
+                     : "r"(g2_su32(bar)), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+        if (n > limit) return false;
+    }
+}
+__device__ __forceinline__ void g2_tma(void* dst, const CUtensorMap* map, int x, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(g2_su32(dst)),
+        "l"((unsigned long long)map), "r"(x), "r"(0), "r"(g2_su32(bar))
+        : "memory");
+}
+
+__global__ void __launch_bounds__(G2_MAX_TILES * 32, 1) gram2_kernel(const __grid_constant__ CUtensorMap tm_s,
+                                                                     const __grid_constant__ CUtensorMap tm_t, long long F, int m,
+                                                                     int mt, int ntiles, double* __restrict__ partials, int* err) {
+    // G2_RING slices of rows x 32 points: S at rows [0, m), T at rows [r8m, r8m + mt), r8m = round8(m); rows that no box
+    // writes only feed tile entries that are discarded, so every tile reads 8 whole rows without clamping
+    extern __shared__ __align__(128) float g2buf[];
+    __shared__ __align__(8) uint64_t bar[G2_RING];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mc = m + mt;
+    const int r8m = (m + 7) & ~7;
+    const int rows = r8m + ((mt + 7) & ~7);
+    const long long chunks = (F + 31) / 32;
+    const int nmine = (int)((chunks - blockIdx.x + gridDim.x - 1) / gridDim.x);  // chunks blockIdx.x + j * gridDim.x
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < G2_RING; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(g2_su32(&bar[i])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const unsigned box_bytes = (unsigned)(mc * 32 * 4);  // whole boxes land, the zero fill past F included
+    auto issue = [&](int j) {  // thread 0: this CTA's j-th chunk into slice j % G2_RING
+        const int sl = j % G2_RING;
+        const int x = (int)(((long long)blockIdx.x + (long long)j * gridDim.x) * 32);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(g2_su32(&bar[sl])), "r"(box_bytes) : "memory");
+        float* dst = g2buf + (size_t)sl * rows * 32;
+        g2_tma(dst, &tm_s, x, &bar[sl]);
+        if (mt > 0) g2_tma(dst + (size_t)r8m * 32, &tm_t, x, &bar[sl]);
+    };
+    // tiles: the upper triangle of S^T S (tile rows ti <= tj), then S^T T (tiles_r x tiles_t); c0 is the shared-memory
+    // row of the tile's first column, col0 its column in G
+    const int tiles_r = (m + GT - 1) / GT, tiles_t = (mt + GT - 1) / GT;
+    const int nsym = tiles_r * (tiles_r + 1) / 2;
+    const bool active = warp < ntiles;
+    int r0 = 0, c0 = 0, col0 = 0;
+    bool mirror = false;
+    if (active) {
+        if (warp < nsym) {
+            int ti = 0, rem = warp;
+            while (rem >= tiles_r - ti) { rem -= tiles_r - ti; ++ti; }
+            const int tj = ti + rem;
+            r0 = ti * GT;
+            c0 = col0 = tj * GT;
+            mirror = tj != ti;
+        } else {
+            const int t = warp - nsym;
+            r0 = (t / tiles_t) * GT;
+            c0 = r8m + (t % tiles_t) * GT;
+            col0 = m + (t % tiles_t) * GT;
+        }
+    }
+    float acc[GT][GT];
+#pragma unroll
+    for (int a = 0; a < GT; ++a)
+#pragma unroll
+        for (int c = 0; c < GT; ++c) acc[a][c] = 0.f;
+    int issued = min(G2_RING - 1, nmine);
+    if (threadIdx.x == 0)
+        for (int j = 0; j < issued; ++j) issue(j);
+    bool alive = true;
+    for (int j = 0; j < nmine; ++j) {
+        const int sl = j % G2_RING;
+        // the slice of chunk j - 1 was released by the barrier that ended it: keep G2_RING - 1 chunks in flight
+        if (alive && issued < nmine) {
+            if (threadIdx.x == 0) issue(issued);
+            ++issued;
+        }
+        if (!g2_wait(&bar[sl], (unsigned)((j / G2_RING) & 1), alive ? G2_WAIT_LIMIT : 1)) {
+            if (alive && err) atomicExch(err, 1);
+            alive = false;  // the partials are undefined; the host's next readback reports the error
+        }
+        if (active) {  // points past F are the boxes' zero fill: they add nothing
+            const float* slp = g2buf + (size_t)sl * rows * 32 + lane;
+            float cv[GT];
+#pragma unroll
+            for (int c = 0; c < GT; ++c) cv[c] = slp[(c0 + c) * 32];
+#pragma unroll
+            for (int a = 0; a < GT; ++a) {
+                const float r = slp[(r0 + a) * 32];
+#pragma unroll
+                for (int c = 0; c < GT; ++c) acc[a][c] = fmaf(r, cv[c], acc[a][c]);
+            }
+        }
+        __syncthreads();  // slice sl is free for chunk j + G2_RING
+    }
+    if (!alive && threadIdx.x == 0)  // copies still in flight land before the CTA's shared memory is released
+        for (int j = max(0, issued - G2_RING); j < issued; ++j) g2_wait(&bar[j % G2_RING], (unsigned)((j / G2_RING) & 1), 1LL << 16);
+    if (!active) return;
+    const size_t base = (size_t)blockIdx.x * ((size_t)m * mc);
+    const int cend = col0 < m ? m : mc;  // a tile's columns stay inside its block (S or T)
+#pragma unroll
+    for (int a = 0; a < GT; ++a)
+#pragma unroll
+        for (int c = 0; c < GT; ++c) {
+            const double v = warp_sum((double)acc[a][c]);
+            if (lane == 0 && r0 + a < m && col0 + c < cend) {
+                partials[base + (size_t)(r0 + a) * mc + (col0 + c)] = v;
+                if (mirror) partials[base + (size_t)(col0 + c) * mc + (r0 + a)] = v;
+            }
+        }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g2_encode() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        cudaDriverEntryPointQueryResult q;
+        void* ptr = nullptr;
+        KS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !ptr) throw DeviceError("cuTensorMapEncodeTiled is not available");
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    }();
+    return fn;
+}
+
+// rows fields of F floats (stride F) as a 2-D tensor map with 32-point x rows boxes, no swizzle
+void g2_rows_map(CUtensorMap* map, const float* base, long long F, int rows) {
+    cuuint64_t dims[2] = {(cuuint64_t)F, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)F * 4};
+    cuuint32_t box[2] = {32, (cuuint32_t)rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g2_encode()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw DeviceError("cuTensorMapEncodeTiled (CUDA-core Gram) failed, code " + std::to_string((int)r));
 }
 
 // ---- multipole moments with on-the-fly real solid harmonics (harmonics.cuh)
@@ -315,13 +471,39 @@ void launch_dots(long long F, const Pairs& p, double* partials, int blocks, cuda
     KS_LAUNCH_CHECK();
 }
 
-void launch_gram(long long F, int m, const float* S, int mt, const float* T, double* partials, int blocks, cudaStream_t s) {
+// warps of the staged form: the upper tiles of S^T S and the tiles of S^T T
+static int gram2_tiles(int m, int mt) {
+    const int tr = ceil_div(m, GT), tt = ceil_div(mt, GT);
+    return tr * (tr + 1) / 2 + tr * tt;
+}
+
+int gram_blocks(int m, int mt) { return gram2_tiles(m, mt) <= G2_MAX_TILES ? sm_count() : 2 * sm_count(); }
+
+int launch_gram(long long F, int m, const float* S, int mt, const float* T, double* partials, cudaStream_t s) {
     const int tiles_r = ceil_div(m, GT), tiles_c = ceil_div(m + mt, GT);
     const int ntiles = tiles_r * tiles_c;
+    const int blocks = gram_blocks(m, mt);
+    const int tiles2 = gram2_tiles(m, mt);
+    if (tiles2 <= G2_MAX_TILES) {
+        if (F % 4 != 0 || reinterpret_cast<uintptr_t>(S) % 16 != 0 || (mt > 0 && reinterpret_cast<uintptr_t>(T) % 16 != 0))
+            throw std::invalid_argument("gram: fields must be 16-byte aligned with F a multiple of 4 floats");
+        const size_t smem = (size_t)G2_RING * (((m + 7) & ~7) + ((mt + 7) & ~7)) * 32 * sizeof(float);
+        static std::atomic<unsigned long long> attr_set{0};
+        once_per_device(attr_set, [] {
+            KS_CUDA(cudaFuncSetAttribute(gram2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, G2_RING * 136 * 32 * (int)sizeof(float)));
+        });
+        CUtensorMap ms, mtm;
+        g2_rows_map(&ms, S, F, m);
+        g2_rows_map(&mtm, mt > 0 ? T : S, F, mt > 0 ? mt : 1);
+        gram2_kernel<<<blocks, tiles2 * 32, smem, s>>>(ms, mtm, F, m, mt, tiles2, partials, device_error_flag());
+        KS_LAUNCH_CHECK();
+        return blocks;
+    }
     dim3 grid(blocks, ceil_div(ntiles, GW));
     // partials are indexed by blockIdx.x only: every tile of a CTA column writes its own entries
     gram_kernel<<<grid, GW * 32, 0, s>>>(F, m, S, mt, T, tiles_c, ntiles, partials);
     KS_LAUNCH_CHECK();
+    return blocks;
 }
 
 void launch_moments(const Layout& L, const float* rho, double* partials, int blocks, cudaStream_t s) {

@@ -121,9 +121,10 @@ struct Pairs {
     const float* b[MAX];
 };
 void launch_dots(long long F, const Pairs& p, double* partials, int blocks, cudaStream_t s);
-// G = S^T [S | T]: S m fields, T mt fields (both blocks stride F); partials [blocks][m*(m+mt)] row-major
-// (row i = S_i, column j < m = S_j, j >= m = T_{j-m}).
-void launch_gram(long long F, int m, const float* S, int mt, const float* T, double* partials, int blocks, cudaStream_t s);
+// G = S^T [S | T] on CUDA cores: S m fields, T mt fields (both blocks stride F); partials [gram_blocks(m, mt)][m*(m+mt)]
+// row-major (row i = S_i, column j < m = S_j, j >= m = T_{j-m}). Returns the number of partial blocks written.
+int gram_blocks(int m, int mt);
+int launch_gram(long long F, int m, const float* S, int mt, const float* T, double* partials, cudaStream_t s);
 // multipole moments Q_lm = sum rho R_lm(r) (l <= 6, Racah real solid harmonics, crates/qm/src/poisson.rs:89-120)
 void launch_moments(const Layout& L, const float* rho, double* partials, int blocks, cudaStream_t s);
 // max |f| over the six outer planes of the box -> partials [blocks] (max, finished by launch_finish_max)

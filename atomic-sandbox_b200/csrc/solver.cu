@@ -401,21 +401,22 @@ void Reducer::gram(int m, const float* S, int mt, const float* T, int off, doubl
         }
         return;
     }
-    const size_t need = (size_t)gram_blocks_ * m * (m + mt);
+    const int gblocks = gram_blocks(m, mt);
+    const size_t need = (size_t)gblocks * m * (m + mt);
     if (need * sizeof(double) > partials_.bytes) partials_.alloc(need * sizeof(double));
-    auto run = [&] { launch_gram(L_.F, m, S, mt, T, partials_.d(), gram_blocks_, s_); };
+    auto run = [&] { launch_gram(L_.F, m, S, mt, T, partials_.d(), s_); };
     if (timer) timer->time(KS_K_GRAM, m, mt, 4.0 * (m + mt) * L_.interior(), s_, run);
     else run();
     if (extra) {
         FinishDesc g;
         g.partials = partials_.d();
-        g.blocks = gram_blocks_;
+        g.blocks = gblocks;
         g.nvals = m * (m + mt);
         g.scale = scale;
         g.out = res_.d() + off;
         launch_finish_pair(g, *extra, s_);
     } else {
-        launch_finish(partials_.d(), gram_blocks_, m * (m + mt), scale, res_.d() + off, s_);
+        launch_finish(partials_.d(), gblocks, m * (m + mt), scale, res_.d() + off, s_);
     }
 }
 

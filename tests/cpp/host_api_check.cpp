@@ -127,7 +127,10 @@ void check_scf() {
     const std::vector<Vec3> f = so.forces(h2.nuclei, st.sigma);
     expect(f.size() == 2 && std::fabs(f[0][0] - 0.12875596866453332) < 1e-4, "forces: the H2 33^3 force pin", std::to_string(f[0][0]));
     const auto ev = so.evals();
-    expect(ev.first.size() == 1 && ev.second.size() == 1 && ev.first[0] == ev.second[0], "evals: one level per spin, equal");
+    // the two spin channels of H2 converge from different seeded guesses: the same level to the eigen tolerance
+    expect(ev.first.size() == 1 && ev.second.size() == 1 && std::fabs(ev.first[0] - ev.second[0]) < 1e-5,
+           "evals: one level per spin, equal to the eigen tolerance",
+           std::to_string(ev.first.empty() ? 0.0 : ev.first[0]) + " " + std::to_string(ev.second.empty() ? 0.0 : ev.second[0]));
     const ScfStats warm = so.solve(h2, st, true);
     expect(warm.iterations < cold.iterations, "solve: a warm start takes fewer steps");
     expect(throws<Aborted>([&] { so.solve_with(h2, st, false, [] { return true; }); }), "solve_with: should_abort abandons the solve");
