@@ -34,10 +34,12 @@ def test_laplacian_matches_oracle_33(ks, oracle):
     assert err_kernel < 1e-6, err_kernel
 
 
-@pytest.mark.parametrize("n", [9, 17, 32, 33, 48, 50])
+@pytest.mark.parametrize("n", [5, 6, 9, 17, 32, 33, 48, 50])
 def test_hamiltonian_block_matches_oracle(ks, oracle, n):
     """H psi = -1/2 lap psi + V psi for a block of 3 vectors, every tile / chunk edge case of the
-    TMA tiling (n below, at and above multiples of the 32 x 16 tile and of the pitch)."""
+    TMA tiling (n below, at and above multiples of the 32 x 16 tile and of the pitch), down to the
+    reference's smallest grid, n = 5 (crates/qm-gpu/src/grid.rs:200-211: the whole box inside one
+    tile's halo, the pitch 8 > n)."""
     h = 0.3
     nuc = [(0.4, 0.0, -0.3, 3), (-1.1, 0.5, 0.2, 1)]
     v = f32(oracle.nuclear_potential(n, h, nuc, 0.5))
@@ -62,9 +64,11 @@ def test_dirichlet_boundary_is_exact_zero_outside(ks, oracle):
     assert np.abs(gpu - want).max() < 1e-6 * np.abs(want).max()
 
 
-def test_precond_matches_oracle(ks, oracle):
-    """precond_init + 3 jacobi_step sweeps (shaders/eigen.wgsl:25-34, stencil.wgsl:94-106)."""
-    n, h, lam = 25, 0.25, -0.6
+@pytest.mark.parametrize("n", [5, 25])
+def test_precond_matches_oracle(ks, oracle, n):
+    """precond_init + 3 jacobi_step sweeps (shaders/eigen.wgsl:25-34, stencil.wgsl:94-106), at the reference's
+    smallest grid too."""
+    h, lam = 0.25, -0.6
     v = f32(oracle.nuclear_potential(n, h, [(0.0, 0.0, 0.0, 2)], 0.5))
     r = f32(smooth_field(oracle, n, h, 4))
     gpu = ks.apply_precond(n, h, v, lam, r)
