@@ -1,8 +1,9 @@
 """ks_gram_device_noalloc, the Gram entry point that allocates no device memory, against the allocating
 ks_gram (gram_mode 0): bit-for-bit the same matrix on two calls in a row (the static scratch is reused
-without clearing), with and without a T block, and a clear KS_INVALID (ValueError) without any launch
-for a block beyond the 4 MiB scratch. This file is collected last so that it also runs after every
-other GPU test in the same process."""
+without clearing), with and without a T block, and against the f64 products of the same f32 inputs to
+the Gram tests' 2e-6 relative bound (an independent answer, not only the solver's own Gram); and a clear
+KS_INVALID (ValueError) without any launch for a block beyond the 4 MiB scratch. This file is collected
+last so that it also runs after every other GPU test in the same process."""
 import numpy as np
 import pytest
 
@@ -39,6 +40,12 @@ def test_noalloc_gram_matches_ks_gram_on_two_calls(ks, m, mt):
     for out in outs:
         got = out.cpu().numpy()
         assert np.array_equal(got, ref), np.abs(got - ref).max()
+    s32 = s.astype(np.float32).astype(np.float64)
+    t32 = t.astype(np.float32).astype(np.float64)
+    cols = np.concatenate([s32, t32]) if mt > 0 else s32
+    want = s32 @ cols.T
+    scale = np.sqrt(np.outer((s32 * s32).sum(1), (cols * cols).sum(1)))
+    assert np.abs(outs[-1].cpu().numpy() - want).max() / scale.max() < 2e-6
 
 
 def test_noalloc_gram_rejects_a_block_beyond_its_scratch(ks):
