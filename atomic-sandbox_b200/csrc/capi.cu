@@ -685,9 +685,13 @@ ks_status ks_fermi_dirac(const double* evals, int k, int n, double kt, double* f
 }
 
 ks_status ks_fd_witness(const double* evals, int k, int n, double mu, double kt, int* reached, int* keep) {
+    return ks_fd_witness_bound(evals, nullptr, k, n, mu, kt, reached, keep);
+}
+
+ks_status ks_fd_witness_bound(const double* evals, const double* residuals, int k, int n, double mu, double kt, int* reached, int* keep) {
     if (k < 0 || n < 0 || (k > 0 && !evals) || !reached || !keep) return fail(nullptr, KS_INVALID, "invalid arguments");
-    *reached = dense::fd_witness(evals, k, n, mu, kt) ? 1 : 0;
-    *keep = dense::fd_witness_keep(evals, k, n, mu, kt);
+    *reached = dense::fd_witness(evals, residuals, k, n, mu, kt) ? 1 : 0;
+    *keep = dense::fd_witness_keep(evals, residuals, k, n, mu, kt);
     return KS_OK;
 }
 

@@ -365,20 +365,31 @@ bool fermi_dirac(const double* ev, int k, int n, double kt, double* f, double& m
     return true;
 }
 
-bool fd_witness(const double* ev, int k, int n, double mu, double kt) {
-    if (n == 0) return true;
-    if (k <= n) return false;
-    std::vector<double> s(ev, ev + k);
-    std::sort(s.begin(), s.end());
-    return s.back() >= s[n - 1] + 0.1 && s.back() - mu >= 36.0 * kt;
+// ranks of the levels, ascending (ties by index)
+static std::vector<int> ascending(const double* ev, int k) {
+    std::vector<int> o(k);
+    for (int i = 0; i < k; ++i) o[i] = i;
+    std::stable_sort(o.begin(), o.end(), [&](int a, int b) { return ev[a] < ev[b]; });
+    return o;
 }
 
-int fd_witness_keep(const double* ev, int k, int n, double mu, double kt) {
+bool fd_witness(const double* ev, const double* res, int k, int n, double mu, double kt) {
+    if (n == 0) return true;
+    if (k <= n) return false;
+    const std::vector<int> o = ascending(ev, k);
+    const int top = o[k - 1];
+    const double lower = ev[top] - (res ? res[top] : 0.0);
+    return lower >= ev[o[n - 1]] + 0.1 && lower - mu >= 36.0 * kt;
+}
+
+int fd_witness_keep(const double* ev, const double* res, int k, int n, double mu, double kt) {
     if (n == 0 || k <= n) return k;
-    std::vector<double> s(ev, ev + k);
-    std::sort(s.begin(), s.end());
-    const double eps_n = s[n - 1];
-    auto passes = [&](int r) { return s[r] >= eps_n + 0.1 && s[r] - mu >= 36.0 * kt; };
+    const std::vector<int> o = ascending(ev, k);
+    const double eps_n = ev[o[n - 1]];
+    auto passes = [&](int r) {
+        const double lower = ev[o[r]] - (res ? res[o[r]] : 0.0);
+        return lower >= eps_n + 0.1 && lower - mu >= 36.0 * kt;
+    };
     for (int t = n; t < k; ++t)
         if (passes(t)) return (t + 1 < k && passes(t + 1)) ? t + 2 : t + 1;
     return k;

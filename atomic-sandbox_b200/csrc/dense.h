@@ -37,11 +37,14 @@ bool diis_coefficients(int m, const Mat& gram, std::vector<double>& c);
 // n = 0 gives every f = 0 and mu = NaN. Returns false on refused inputs (k < n + 1, a non-finite
 // level or kT).
 bool fermi_dirac(const double* evals, int k, int n, double kt, double* f, double& mu, double& entropy);
-// The highest level at least 0.1 Ha above the n-th lowest and 36 kT above mu (occupations.rs witness_reached).
-bool fd_witness(const double* evals, int k, int n, double mu, double kt);
-// After a passed witness, how many of the lowest levels to keep (occupations.rs:367-394 witness_keep, read on the levels
-// themselves): t + 1 for the lowest rank t >= n that is a witness, t + 2 when the level above it is one too; k when none.
-int fd_witness_keep(const double* evals, int k, int n, double mu, double kt);
+// The gap witness on the lower bounds theta_j - r_j of k levels (any order) with residual norms r (NULL: all zero):
+// the highest level's bound at least 0.1 Ha above the n-th lowest level and 36 kT above mu (occupations.rs:299-317
+// witness_bound_reached; with r = 0 it is witness_reached, :283-292). A NaN residual never passes.
+bool fd_witness(const double* evals, const double* res, int k, int n, double mu, double kt);
+// After a passed witness, how many of the lowest levels to keep (occupations.rs:372-394 witness_keep, on the same lower
+// bounds): t + 1 for the lowest rank t >= n whose bound passes both arms, t + 2 when the rank above passes too; k when
+// none does or n = 0.
+int fd_witness_keep(const double* evals, const double* res, int k, int n, double mu, double kt);
 
 }  // namespace dense
 }  // namespace ks

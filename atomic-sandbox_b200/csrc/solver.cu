@@ -116,8 +116,11 @@ constexpr double EIG_TOL_FLOOR_FACTOR = 3.0;
 constexpr double EIG_GUESS_FACTOR = 1.5;
 // Fermi-Dirac (crates/qm/src/occupations.rs): a level with min(f, 1 - f) at or above PARTIAL_OCCUPATION_MIN is partly
 // occupied, and a step with one is tested against max(tol, GPU_PARTIAL_TOL); the columns of the block whose occupation
-// tail stays below LOOSE_F_FACTOR * tol are left out of the eigensolver's stop test (the guard tier).
+// tail stays below LOOSE_F_FACTOR * tol are held to the guard tolerance WITNESS_GUARD_TOL = WITNESS_GAP / 100 (or the
+// step's eigen tolerance when that is looser; occupations.rs:91-92, :184-186), so that their lower bounds theta - r,
+// on which the gap witness is read, are within 1e-3 Ha of their levels.
 constexpr double PARTIAL_OCCUPATION_MIN = 1e-6;
+constexpr double WITNESS_GUARD_TOL = 1e-3;
 constexpr double GPU_PARTIAL_TOL = 1e-5;
 constexpr double LOOSE_F_FACTOR = 1e-2;
 constexpr double EIG_TOL_FRACTION = 0.0015;
@@ -690,6 +693,7 @@ void Channel::create(const Layout& L, int kk) {
     Q.create(L, k);
     theta_d.alloc((size_t)(2 * k + 6 * k * k) * sizeof(double));  // [theta | lambda | coef 3k x 2k]
     evals.assign(k, -1.0);
+    res.assign(k, std::nan(""));
 }
 
 // ------------------------------------------------------------------ solver
@@ -705,6 +709,7 @@ void Solver::resize_channel(int sp, int newk, const Nuc* dnuc, int nn) {
         launch_initial_orbitals(L_, dnuc, nn, 1, 1000ULL + 2ULL * (unsigned long long)i + (unsigned long long)sp, 0, nc.A[0].at(i), s_);
     nc.evals.assign(old.evals.begin(), old.evals.begin() + std::min<size_t>(keep, old.evals.size()));
     while ((int)nc.evals.size() < newk) nc.evals.push_back(nc.evals.empty() ? -1.0 : nc.evals.back());
+    for (int i = 0; i < keep && i < (int)old.res.size(); ++i) nc.res[i] = old.res[i];
     nc.cur = 0;
     KS_CUDA(cudaStreamSynchronize(s_));  // the old block is freed below
     ch_[sp] = std::move(nc);
@@ -799,6 +804,7 @@ void Solver::import_state(int n_up, int n_dn, const int k[2], const double* cons
             launch_initial_orbitals(L_, nullptr, 0, 1, 1000ULL + 2ULL * (unsigned long long)i + (unsigned long long)sp, 1, ch.A[0].at(i), s_);
         ch.evals.assign(evals[sp], evals[sp] + k[sp]);
         while ((int)ch.evals.size() < kk[sp]) ch.evals.push_back(ch.evals.empty() ? -1.0 : ch.evals.back());
+        ch.res.assign(kk[sp], std::nan(""));
         for (int i = 0; i < kk[sp]; ++i) occ_[sp][i] = fermi_dirac ? (i < k[sp] ? occ[sp][i] : 0.0) : (i < nocc[sp] ? 1.0 : 0.0);
     }
     upload(rho_up, out_up_.at(0));
@@ -832,7 +838,7 @@ void Solver::gram_checked(Reducer& red, int m, const float* S, int mt, const flo
     red.gram(m, S, mt, T, 0, L_.h * L_.h * L_.h, extra);  // the L2 product <a, b> = h^3 sum a b
 }
 
-EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked) {
+EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked, double tail_tol) {
     NvtxRange range("ks lobpcg");
     EigenStats es;
     const int k = ch.k;
@@ -988,8 +994,10 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
             if (!std::isfinite(res[i]) || !std::isfinite(lambda[i])) throw NumericalError("lobpcg: non-finite residual");
             max_res = std::max(max_res, res[i]);
             if (i < checked) stop_res = std::max(stop_res, res[i]);
+            else if (std::isfinite(tail_tol)) stop_res = std::max(stop_res, res[i] * (tol / tail_tol));
         }
         ch.evals = lambda;
+        ch.res = res;
         // formation check (crates/qm-gpu/src/eigen.rs:800-825): undo a step whose moved columns' stored
         // Rayleigh quotients rose above their Ritz values
         if (have_prev) {
@@ -1187,6 +1195,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                     ch_[sp].cur = 0;
                     launch_initial_orbitals(L_, dnuc, nn, kk[sp], (unsigned long long)(sp + 1), opt_.init_mode, ch_[sp].X(), s_);
                     ch_[sp].evals.assign(kk[sp], -1.0);
+                    ch_[sp].res.assign(kk[sp], std::nan(""));
                 }
             }
             const double total = (double)(n_up + n_dn);
@@ -1326,7 +1335,8 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 for (auto& l : lane_) KS_CUDA(cudaStreamWaitEvent(l->s, ev_fork_, 0));
                 auto run = [&](int sp) {
                     est[sp] = lobpcg(ch_[sp], *lane_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, guess_factor * step_tol,
-                                     EIGEN_MAX_ITER, fd ? tight[sp] : nocc[sp]);
+                                     EIGEN_MAX_ITER, fd ? tight[sp] : nocc[sp],
+                                     fd ? std::max(WITNESS_GUARD_TOL, step_tol) : std::numeric_limits<double>::infinity());
                 };
                 std::exception_ptr err_dn;
                 std::thread worker;
@@ -1378,9 +1388,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 profile.eigen_iterations += es.iterations;
                 eig_its += es.iterations;
                 if (es.restores_exhausted) throw NumericalError("LOBPCG: a Ritz-vector formation failed again after its restores");
-                double tight = 0.0;
-                for (int i = 0; i < nocc[sp]; ++i) tight = std::max(tight, 0.0);
-                tight = es.max_residual;
+                const double tight = es.max_residual;
                 if (step_tol <= eig_lo) max_eig_res = std::max(max_eig_res, tight);
                 last_step_res = std::max(last_step_res, tight);
                 if (es.stop == 2) last_step_maxiter = true;
@@ -1389,7 +1397,8 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             // no witness, its extra levels double (at most the witness cap, 32 by default, and 64 levels in all; a new vector is the
             // reference's initial orbital with seed 1000 + 2 * index + spin) and the channel is solved again with every
             // level held to the step's tolerance; once witnessed, the overshoot above the lowest witness is trimmed, never
-            // below the configured N_sigma + n_extra. The witness is read on the Ritz values.
+            // below the configured N_sigma + n_extra. The witness is read on the lower bounds theta - r (occupations.rs:93-99,
+            // witness_bound_reached): every column is held to the step's tolerance, so r is that small.
             for (int sp = 0; sp < 2 && fd; ++sp) {
                 if (nocc[sp] == 0) continue;
                 const int base = nocc[sp] + opt_.n_extra;
@@ -1400,8 +1409,8 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                     if (!dense::fermi_dirac(ch_[sp].evals.data(), kk[sp], nocc[sp], s.kt, f.data(), m_sp, s_sp))
                         throw NumericalError("Fermi-Dirac occupations refused (a non-finite level)");
                     const int extras = kk[sp] - nocc[sp];
-                    if (dense::fd_witness(ch_[sp].evals.data(), kk[sp], nocc[sp], m_sp, s.kt)) {
-                        const int keep = std::max(base, dense::fd_witness_keep(ch_[sp].evals.data(), kk[sp], nocc[sp], m_sp, s.kt));
+                    if (dense::fd_witness(ch_[sp].evals.data(), ch_[sp].res.data(), kk[sp], nocc[sp], m_sp, s.kt)) {
+                        const int keep = std::max(base, dense::fd_witness_keep(ch_[sp].evals.data(), ch_[sp].res.data(), kk[sp], nocc[sp], m_sp, s.kt));
                         if (keep < kk[sp]) {
                             resize_channel(sp, keep, dnuc, nn);
                             kk[sp] = keep;
@@ -1603,7 +1612,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         }
         if (fd)
             for (int sp = 0; sp < 2; ++sp)
-                if (nocc[sp] > 0 && !dense::fd_witness(ch_[sp].evals.data(), kk[sp], nocc[sp], mu[sp], s.kt)) {
+                if (nocc[sp] > 0 && !dense::fd_witness(ch_[sp].evals.data(), ch_[sp].res.data(), kk[sp], nocc[sp], mu[sp], s.kt)) {
                     error = "no Fermi-Dirac gap witness in the block of " + std::to_string(kk[sp]) + " levels of spin " + std::to_string(sp) +
                             " (its top level must lie 0.1 Ha above level N and 36 kT above mu) within the witness cap of " +
                             std::to_string(witness_cap_) + " extra levels";

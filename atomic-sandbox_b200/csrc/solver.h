@@ -1,6 +1,7 @@
 // solver.h -- the B200 Kohn-Sham solver behind the C ABI (include/ks_cuda.h).
 #pragma once
 #include <atomic>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -229,7 +230,8 @@ struct Channel {
     int cur = 0;
     Block T, HX, Q;
     DevBuf theta_d, lambda_d, coef_d;
-    std::vector<double> evals;
+    std::vector<double> evals;  // Ritz values of the columns (ascending after a solve)
+    std::vector<double> res;    // their residual norms |H x - theta x| at the last LOBPCG exit (NaN: not measured)
     void create(const Layout& L, int k);
     float* X() const { return A[cur].at(0); }
 };
@@ -282,7 +284,10 @@ public:
     double effective_eig_tol(double eig_tol) const;
     // the ionic setup of the next solves (n = 0: all-electron); throws std::invalid_argument on bad tables
     void set_ionic(const ks_species* sp, int n) { ionic_.set(sp, n); }
-    EigenStats lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked);
+    // columns [0, checked) are held to tol, the others to tail_tol (infinite: untested; the split stop test of
+    // crates/qm-gpu/src/eigen.rs:781-787, a column's residual scaled by tol / its own tolerance)
+    EigenStats lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked,
+                      double tail_tol = std::numeric_limits<double>::infinity());
     Lane& lane(int i) { return *lane_[i]; }
     std::string error;
     const Layout& layout() const { return L_; }

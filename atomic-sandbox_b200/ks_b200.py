@@ -200,7 +200,7 @@ EXPORTED = [
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
     "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
-    "ks_fd_witness", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
+    "ks_fd_witness", "ks_fd_witness_bound", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
     "ks_test_poison_parked_density", "ks_test_fail_readbacks",
 ]
 
@@ -257,6 +257,7 @@ def lib():
         L.ks_rayleigh_ritz.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp]
         L.ks_fermi_dirac.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
         L.ks_fd_witness.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
+        L.ks_fd_witness_bound.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
         L.ks_field_pitch.argtypes = [ctypes.c_int]
         L.ks_launch_count.restype = ctypes.c_longlong
         L.ks_launch_count.argtypes = []
@@ -733,12 +734,20 @@ def fermi_dirac(evals, n, kt):
     return f[:ev.size], mu.value, s.value
 
 
-def fd_witness(evals, n, mu, kt):
-    """The solver's gap witness of a Fermi-Dirac block read on its levels (crates/qm/src/occupations.rs
-    witness_reached, witness_keep): (reached, keep)."""
+def fd_witness(evals, n, mu, kt, residuals=None):
+    """The solver's gap witness of a Fermi-Dirac block: (reached, keep). Without residuals it is read on the levels
+    themselves (crates/qm/src/occupations.rs witness_reached, witness_keep); with them on the lower bounds
+    theta - r, as the solver reads it (witness_bound_reached, witness_keep)."""
     ev = _f64(evals)
     reached, keep = ctypes.c_int(), ctypes.c_int()
-    _check(lib().ks_fd_witness(_p(ev), ev.size, int(n), float(mu), float(kt), ctypes.byref(reached), ctypes.byref(keep)))
+    if residuals is None:
+        _check(lib().ks_fd_witness(_p(ev), ev.size, int(n), float(mu), float(kt), ctypes.byref(reached), ctypes.byref(keep)))
+    else:
+        r = _f64(residuals)
+        if r.size != ev.size:
+            raise ValueError("fd_witness: one residual per level")
+        _check(lib().ks_fd_witness_bound(_p(ev), _p(r), ev.size, int(n), float(mu), float(kt), ctypes.byref(reached),
+                                         ctypes.byref(keep)))
     return bool(reached.value), keep.value
 
 

@@ -327,6 +327,11 @@ ks_status ks_fermi_dirac(const double* evals, int k, int n, double kt, double* f
    36 kT above mu; always for n = 0), keep = witness_keep on the levels themselves (occupations.rs:372-394: t + 1 for
    the lowest rank t >= n that passes both arms, t + 2 when rank t + 1 passes too, k when none does or n = 0). */
 ks_status ks_fd_witness(const double* evals, int k, int n, double mu, double kt, int* reached, int* keep);
+/* The same witness read on the lower bounds theta_j - r_j, r the levels' residual norms |H x - theta x| (the
+   Krylov-Weinstein bound, as the solver reads it): reached = witness_bound_reached (crates/qm/src/occupations.rs:299-317),
+   keep = witness_keep (:372-394). residuals may be NULL (all zero: ks_fd_witness); a NaN residual never passes. */
+ks_status ks_fd_witness_bound(const double* evals, const double* residuals, int k, int n, double mu, double kt, int* reached,
+                              int* keep);
 
 /* ---- device-pointer entry points for callers that keep fields on the GPU (bench, integrations) ----
    Fields are in the pitched layout: element (i, j, k) at (k*n + j)*P + i, P = ks_field_pitch(n),

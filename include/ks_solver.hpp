@@ -369,5 +369,13 @@ inline std::pair<bool, int> fd_witness(const std::vector<double>& evals, int n, 
     detail::check(ks_fd_witness(evals.data(), (int)evals.size(), n, mu, kt, &reached, &keep), nullptr);
     return {reached != 0, keep};
 }
+// witness_bound_reached and witness_keep (occupations.rs:299-317, :372-394) on the lower bounds theta - r.
+inline std::pair<bool, int> fd_witness_bound(const std::vector<double>& evals, const std::vector<double>& residuals, int n, double mu,
+                                             double kt) {
+    if (residuals.size() != evals.size()) throw InvalidArgument("fd_witness_bound: one residual per level");
+    int reached = 0, keep = 0;
+    detail::check(ks_fd_witness_bound(evals.data(), residuals.data(), (int)evals.size(), n, mu, kt, &reached, &keep), nullptr);
+    return {reached != 0, keep};
+}
 
 }  // namespace qm_gpu

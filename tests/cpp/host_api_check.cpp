@@ -102,6 +102,10 @@ void check_occupations() {
     const auto w = qm_gpu::fd_witness(evals, 1, -0.4, 5e-3);
     expect(w.first && w.second == 5, "fd_witness: the witness and its passing spare are kept");
     expect(!qm_gpu::fd_witness({-0.3, -0.3 + 0.099, -0.5}, 2, -0.4, 5e-3).first, "fd_witness: the gap arm");
+    const auto wb = qm_gpu::fd_witness_bound(evals, {0.0, 0.0, 0.0, 0.15, 0.0, 0.0, 0.0}, 1, -0.4, 5e-3);
+    expect(wb.first && wb.second == 6, "fd_witness_bound: the witness's own residual pushes it up a rank");
+    expect(throws<qm_gpu::InvalidArgument>([&] { qm_gpu::fd_witness_bound(evals, {0.0}, 1, -0.4, 5e-3); }),
+           "fd_witness_bound: one residual per level");
 }
 
 void check_arguments() {

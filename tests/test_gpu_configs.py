@@ -53,6 +53,23 @@ def test_vjp_matches_central_differences_of_the_energy(ks):
     assert abs(gs - (4 * fs[0.005] - fs[0.01]) / 3) < 2e-5, (gs, fs)
 
 
+def test_vjp_error_from_a_loose_solve(ks):
+    """The adjoint is the explicit derivative, exact at self-consistency; its error away from it grows with the
+    solve's own residual. H2 49^3 (sigma = h): the dE/dx0 after solves at tol 1e-3, 1e-4 and 1e-5 (density
+    residual 3.5e-5 .. 1.3e-6) against the one after a tight solve (tol 1e-7, eig_tol 1e-8). Measured on the B200:
+    2e-7 Ha/Bohr at tol 1e-3, below the reference's 2e-4 force bound (crates/qm-gpu/src/forces.rs:667) by three
+    orders; the bound here is 2e-6."""
+    sig = 0.25
+    with ks.GpuSolver(49, 0.25) as so:
+        so.solve(ks.System(_h2(0.7), 1, 1), ks.ScfSettings(sigma=sig, tol=1e-7, eig_tol=1e-8))
+        g_tight, _ = so.vjp(_h2(0.7), sig)
+        for tol in (1e-3, 1e-4, 1e-5):
+            st = so.solve(ks.System(_h2(0.7), 1, 1), ks.ScfSettings(sigma=sig, tol=tol, eig_tol=min(1e-6, tol)))
+            g, _ = so.vjp(_h2(0.7), sig)
+            assert st["delta_rho"] < tol
+            assert np.abs(g - g_tight).max() < 2e-6, (tol, st["delta_rho"], g[0, 0], g_tight[0, 0])
+
+
 def test_nh3_96_forces_adjoint_and_md(ks, drv):
     """NH3 on 96^3 at h = 0.22 (N at the origin, H at 1.91 Bohr, 106.7 deg, seeded 0.05 Bohr jitter,
     the reference's default smearing sigma = h), mixed form: the adjoint equals -forces and matches

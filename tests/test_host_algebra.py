@@ -86,3 +86,33 @@ def test_witness_known_answers(ks):
     assert ks.fd_witness(evals[:keep], 1, mu, kt)[0]  # what is kept passes on its own
     assert ks.fd_witness(evals, 0, mu, kt)[1] == 7    # an empty channel keeps its block
     assert ks.fd_witness([0.3, -0.5, -0.05, -0.1, 0.0, -0.25, -0.3], 1, mu, kt)[1] == 5  # order does not matter
+
+
+def test_witness_reads_the_lower_bound(ks):
+    """The reference's tests of the witness on theta - r (crates/qm/src/occupations.rs:666-683
+    witness_reads_the_lower_bound; :686-704 witness_keep_trims_the_overshoot, its residual cases), on the rule the
+    solver reads after each eigensolve."""
+    kt, mu = 5e-3, -0.4
+    top = mu + 36.0 * kt + 0.001  # the Ritz value clears the tail arm by 1 mHa (the gap arm by far)
+    evals = [-0.5, top, -0.3]
+    assert ks.fd_witness(evals, 1, mu, kt)[0]
+    assert ks.fd_witness(evals, 1, mu, kt, residuals=[0.0, 0.0009, 0.0])[0]      # theta - r still clears it
+    assert not ks.fd_witness(evals, 1, mu, kt, residuals=[0.0, 0.002, 0.0])[0]  # theta - r = top - 2 mHa does not
+    near = [-0.5, -0.399]  # the gap arm on the lower bound: top - r must be >= -0.4
+    assert ks.fd_witness(near, 1, -0.9, kt)[0]
+    assert not ks.fd_witness(near, 1, -0.9, kt, residuals=[0.0, 0.002])[0]
+    assert not ks.fd_witness(evals, 1, mu, kt, residuals=[0.0, float("nan"), 0.0])[0]  # a NaN residual never passes
+    assert ks.fd_witness([], 0, 0.0, kt, residuals=[])[0]
+    assert not ks.fd_witness([-0.5], 1, -0.9, kt, residuals=[0.0])[0]
+    block = [-0.5, -0.3, -0.25, -0.1, -0.05, 0.0, 0.3]
+    zero = [0.0] * 7
+    assert ks.fd_witness(block, 1, mu, kt, residuals=zero)[1] == 5
+    spare_fails = [0.0, 0.0, 0.0, 0.0, 0.2, 0.0, 0.0]
+    assert ks.fd_witness(block, 1, mu, kt, residuals=spare_fails)[1] == 4                      # the witness alone on top
+    assert ks.fd_witness(block, 1, mu, kt, residuals=[0.0, 0.0, 0.0, 0.15, 0.0, 0.0, 0.0])[1] == 6  # pushed up a rank
+    for res in (zero, spare_fails):  # whatever is kept passes the witness on its own
+        k = ks.fd_witness(block, 1, mu, kt, residuals=res)[1]
+        assert ks.fd_witness(block[:k], 1, mu, kt, residuals=res[:k])[0]
+    assert ks.fd_witness(block, 0, mu, kt, residuals=zero)[1] == 7  # an empty channel keeps its block
+    with pytest.raises(ValueError):
+        ks.fd_witness(block, 1, mu, kt, residuals=zero[:3])
