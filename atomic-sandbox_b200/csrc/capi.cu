@@ -642,6 +642,65 @@ ks_status ks_multipole_moments(int n, double h, const double* rho, double* q49) 
     });
 }
 
+ks_status ks_density_residual(int n, double h, int k, const double* psi, const double* f, const double* rho_in, double* rho_out,
+                              double* r, double* sums) {
+    if (!valid_grid(n, h) || k < 0 || k > 64 || (k > 0 && !psi) || !rho_in || !rho_out || !r || !sums)
+        return fail(nullptr, KS_INVALID, "invalid arguments");
+    if (f)
+        for (int i = 0; i < k; ++i)
+            if (!std::isfinite(f[i])) return fail(nullptr, KS_INVALID, "density_residual: a non-finite occupation");
+    return guarded(nullptr, [&] {
+        Solver so(n, h, SolverOptions());
+        Scratch sc(n, h);
+        const Layout& L = so.layout();
+        Block P, in, out, rr;
+        P.create(L, std::max(k, 1));
+        in.create(L, 1);
+        out.create(L, 1);
+        rr.create(L, 1);
+        if (k > 0) sc.upload_fields(psi, k, P);
+        sc.upload_fields(rho_in, 1, in);
+        DevBuf df(64 * sizeof(double));
+        if (f && k > 0) KS_CUDA(cudaMemcpyAsync(df.p, f, (size_t)k * sizeof(double), cudaMemcpyHostToDevice, sc.s));
+        Reducer& red = so.reducer();
+        // the solver's launch: the density kernel and the fixed-order finish of its (|r|, rho) partials
+        launch_density_residual(L.F, k, k > 0 ? P.at(0) : in.at(0), f ? df.d() : nullptr, in.at(0), out.at(0), rr.at(0), red.partials(),
+                                red.blocks(), sc.s);
+        launch_finish(red.partials(), red.blocks(), 2, L.h * L.h * L.h, red.res(), sc.s);
+        KS_CUDA(cudaStreamSynchronize(sc.s));
+        const double* q = red.read(2);
+        sums[0] = q[0];
+        sums[1] = q[1];
+        sc.download_fields(out.at(0), 1, rho_out);
+        sc.download_fields(rr.at(0), 1, r);
+        return KS_OK;
+    });
+}
+
+ks_status ks_diis_mix(int n, int m, const double* rho, const double* r, const double* c, const double* a, double* out) {
+    if (!valid_grid(n, 1.0) || m < 1 || m > 16 || !rho || !r || (m > 1 && !c) || !a || !out) return fail(nullptr, KS_INVALID, "invalid arguments");
+    return guarded(nullptr, [&] {
+        Scratch sc(n, 1.0);
+        Block R, Rr, O;
+        R.create(sc.L, m);
+        Rr.create(sc.L, m);
+        O.create(sc.L, 1);
+        sc.upload_fields(rho, m, R);
+        sc.upload_fields(r, m, Rr);
+        std::vector<const float*> rp(m), rq(m);
+        std::vector<float> cf(m, 0.f), af(m);
+        for (int i = 0; i < m; ++i) {
+            rp[i] = R.at(i);
+            rq[i] = Rr.at(i);
+            af[i] = (float)a[i];
+            if (i < m - 1) cf[i] = (float)c[i];
+        }
+        launch_diis_mix(sc.L.F, m, rp.data(), rq.data(), cf.data(), af.data(), O.at(0), sc.s);
+        sc.download_fields(O.at(0), 1, out);
+        return KS_OK;
+    });
+}
+
 ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gram_mode, double* out) {
     if (n < 1 || m < 1 || mt < 0 || !s || (mt > 0 && !t) || !out || gram_mode < 0 || gram_mode > 1 || (gram_mode == 1 && mt < 1))
         return fail(nullptr, KS_INVALID, "invalid arguments");

@@ -200,7 +200,7 @@ EXPORTED = [
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
     "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
-    "ks_fd_witness", "ks_fd_witness_bound", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
+    "ks_fd_witness", "ks_fd_witness_bound", "ks_density_residual", "ks_diis_mix", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
     "ks_test_poison_parked_density", "ks_test_fail_readbacks",
 ]
 
@@ -251,6 +251,8 @@ def lib():
         L.ks_nuclear_potential.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(Nucleus), ctypes.c_int, ctypes.c_double, dp]
         L.ks_poisson_solve.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp, ctypes.c_double, ctypes.c_int, dp, ip]
         L.ks_gram.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int, dp]
+        L.ks_density_residual.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp, dp]
+        L.ks_diis_mix.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp]
         L.ks_lobpcg.argtypes = [ctypes.c_int, ctypes.c_double, dp, ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                 dp, ip]
         L.ks_multipole_moments.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
@@ -749,6 +751,34 @@ def fd_witness(evals, n, mu, kt, residuals=None):
         _check(lib().ks_fd_witness_bound(_p(ev), _p(r), ev.size, int(n), float(mu), float(kt), ctypes.byref(reached),
                                          ctypes.byref(keep)))
     return bool(reached.value), keep.value
+
+
+def density_residual(n, h, psi, rho_in, f=None):
+    """The SCF's density step (the solver's kernel and finish): (rho_out = sum_i f_i psi_i^2, r = rho_out - rho_in,
+    (h^3 sum |r|, h^3 sum rho_out)) for psi of shape (k, n^3); f None means every f_i = 1."""
+    n3 = n ** 3
+    psi = np.ascontiguousarray(np.asarray(psi, dtype=np.float64).reshape(-1, n3))
+    k = psi.shape[0]
+    rin = _f64(rho_in, n3)
+    fa = None if f is None else _f64(f, k)
+    out, r, sums = np.empty(n3), np.empty(n3), np.empty(2)
+    _check(lib().ks_density_residual(n, float(h), k, _p(psi), None if fa is None else _p(fa), _p(rin), _p(out), _p(r), _p(sums)))
+    return out, r, sums
+
+
+def diis_mix(n, rho, r, c, a):
+    """The SCF's Pulay mix: max(base + sum_{i<m-1} c_i (rho_i - base) + sum_i a_i r_i, 0), base = rho_{m-1}, for rho
+    and r of shape (m, n^3)."""
+    n3 = n ** 3
+    rho = np.ascontiguousarray(np.asarray(rho, dtype=np.float64).reshape(-1, n3))
+    r = np.ascontiguousarray(np.asarray(r, dtype=np.float64).reshape(-1, n3))
+    m = rho.shape[0]
+    if r.shape[0] != m:
+        raise ValueError("diis_mix: one residual per density")
+    ca, aa = _f64([] if c is None else c, m - 1), _f64(a, m)
+    out = np.empty(n3)
+    _check(lib().ks_diis_mix(n, m, _p(rho), _p(r), _p(ca) if m > 1 else None, _p(aa), _p(out)))
+    return out
 
 
 def gram(n, s, t, gram_mode=0):

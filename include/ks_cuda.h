@@ -302,6 +302,17 @@ ks_status ks_nuclear_potential(int n, double h, const ks_nucleus* nuclei, int n_
    v is the initial guess and the output; returns the true relative residual and the iteration count. */
 ks_status ks_poisson_solve(int n, double h, const double* rho, double* v, double tol, int max_iter, double* residual,
                            int* iterations);
+/* The SCF's density step on host arrays, the kernel and finish the solve runs (crates/qm-gpu/src/scf.rs: the output
+   density as pointwise mul_add_sq over the orbitals, its residual against the input and the step's |r| and charge
+   reductions): rho_out = sum_i f_i psi_i^2 over k orbitals of n^3 points (f NULL: every f_i = 1; f is applied in f32),
+   r = rho_out - rho_in, sums = (h^3 sum |r|, h^3 sum rho_out) summed in f64. 0 <= k <= 64. */
+ks_status ks_density_residual(int n, double h, int k, const double* psi, const double* f, const double* rho_in, double* rho_out,
+                              double* r, double* sums);
+/* The SCF's Pulay mix on host arrays (crates/qm-gpu/src/scf.rs:628-645, pointwise diis_mix re-centred on the latest
+   input): out = max(base + sum_{i<m-1} c_i (rho_i - base) + sum_{i<m} a_i r_i, 0) with base = rho_{m-1}; rho and r
+   hold m fields of n^3 points each, c m - 1 and a m coefficients (applied in f32), 1 <= m <= 16; c may be NULL for
+   m = 1. */
+ks_status ks_diis_mix(int n, int m, const double* rho, const double* r, const double* c, const double* a, double* out);
 /* Reducer::gram / block_dots (crates/qm-gpu/src/reduce.rs:340-420): G = S^T [S | T], m and mt fields, gram_mode as
    in ks_options; out row-major m x (m + mt). */
 ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gram_mode, double* out);

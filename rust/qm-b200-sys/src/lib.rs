@@ -101,6 +101,10 @@ extern "C" {
     pub fn ks_density_to_volume(s: *mut c_void, dense_dev: *mut f32, stream: *mut c_void) -> c_int;
     pub fn ks_density_with_core_to_volume(s: *mut c_void, dense_dev: *mut f32, stream: *mut c_void,
                                           max_out: *mut c_double) -> c_int;
+    pub fn ks_density_residual(n: c_int, h: c_double, k: c_int, psi: *const c_double, f: *const c_double, rho_in: *const c_double,
+                               rho_out: *mut c_double, r: *mut c_double, sums: *mut c_double) -> c_int;
+    pub fn ks_diis_mix(n: c_int, m: c_int, rho: *const c_double, r: *const c_double, c: *const c_double, a: *const c_double,
+                       out: *mut c_double) -> c_int;
     pub fn ks_gram(n: c_int, m: c_int, s: *const c_double, mt: c_int, t: *const c_double, gram_mode: c_int,
                    out: *mut c_double) -> c_int;
     // device-pointer entry points (pitched f32 fields on the caller's stream; section 4)

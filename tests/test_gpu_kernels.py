@@ -191,3 +191,60 @@ def test_lobpcg_tensor_core_gram_matches_oracle(ks, oracle):
     ev, xs, it, mr = ks.lobpcg(n, h, v, guess, tol=2e-5, max_iter=400, gram_mode=1)
     evo, _, _, _ = oracle.lobpcg(n, h, v, guess, tol=1e-8, max_iter=500, precond_lambda=1.5)
     assert np.abs(np.sort(ev) - np.sort(evo)).max() < 1e-5, (ev, evo)
+
+
+def _check_rel(name, got, want, mag, rel=1e-6):
+    """The reference's pointwise bound (crates/qm-gpu/src/pointwise.rs check: |gpu - cpu| <= 1e-6 * max(mag, 1e-6))."""
+    bad = np.abs(got - want) > rel * np.maximum(mag, 1e-6)
+    assert not bad.any(), (name, np.abs(got - want)[bad].max(), int(bad.sum()))
+
+
+@pytest.mark.parametrize("n", [5, 17, 33])
+def test_density_residual_matches_f64(ks, oracle, n):
+    """The SCF's density step: rho_out = sum_i f_i psi_i^2 over three orbitals, r = rho_out - rho_in, and the step's
+    reductions (h^3 sum |r|, h^3 sum rho_out), against the f64 formula on the f32-rounded inputs the kernel sees, to
+    the reference's pointwise bound (axpy_scale_lincomb_mul_density_match_cpu, crates/qm-gpu/src/pointwise.rs:329-438,
+    its mul_add_sq case): once with Fermi-Dirac weights (f32 on the device) and once with f = 1."""
+    h = 0.3
+    psi = np.stack([smooth_field(oracle, n, h, 40 + i, centre=(0.1 * i, -0.2, 0.3)) for i in range(3)])
+    x, y, z = oracle.grid_points(n, h)
+    rho_in = 0.2 * np.exp(-(x * x + y * y + z * z) / 3)
+    p32, rin32 = f32(psi), f32(rho_in)
+    for f in ([1.0, 0.6, 0.05], None):
+        w = np.ones(3) if f is None else f32(f)
+        out, r, sums = ks.density_residual(n, h, psi, rho_in, f=f)
+        want = (w[:, None] * p32 * p32).sum(0)
+        mag = (np.abs(w)[:, None] * p32 * p32).sum(0)
+        _check_rel("rho_out", out, want, mag)
+        _check_rel("r", r, want - rin32, mag + np.abs(rin32))
+        # the reductions read the device's own rho_out and r (f32), summed in f64
+        assert abs(sums[0] - h ** 3 * np.abs(f32(r)).sum()) <= 1e-12 * max(1.0, sums[0]), (sums[0], h ** 3 * np.abs(r).sum())
+        assert abs(sums[1] - h ** 3 * f32(out).sum()) <= 1e-12 * max(1.0, sums[1]), (sums[1], h ** 3 * out.sum())
+    out, r, sums = ks.density_residual(n, h, np.zeros((0, n ** 3)), rho_in)  # an empty channel: rho_out = 0
+    assert np.all(out == 0.0) and np.allclose(r, -rin32, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("m", [1, 3, 6])
+def test_diis_mix_matches_oracle_step(ks, oracle, m):
+    """The SCF's Pulay mix with the oracle's coefficients (oracle.diis_coefficients on the residuals' Gram) against the
+    oracle's own mix step, max(sum_e c_e (rho_e + alpha r_e), 0) (oracle/ks_oracle.cpp diis_mix, crates/qm/src/scf.rs),
+    to the reference's pointwise bound (crates/qm-gpu/src/pointwise.rs diis_mix case: 1e-6 of the terms' magnitude);
+    with one and three entries the mixed density goes negative somewhere, so the clamp at 0 is exercised (six entries
+    cancel the residuals too well for that)."""
+    n, h, alpha = 17, 0.3, 0.3
+    x, y, z = oracle.grid_points(n, h)
+    rng = np.random.default_rng(0xD115 + m)
+    base = np.exp(-(x * x + y * y + z * z) / 2)
+    rho = np.stack([base * (1.0 + 0.05 * rng.standard_normal()) + 0.01 * smooth_field(oracle, n, h, 60 + e) for e in range(m)])
+    r = np.stack([0.5 * smooth_field(oracle, n, h, 80 + e) for e in range(m)])
+    c = oracle.diis_coefficients(np.array([[h ** 3 * (r[i] * r[j]).sum() for j in range(m)] for i in range(m)]))
+    assert c is not None and abs(c.sum() - 1.0) < 1e-12
+    out = ks.diis_mix(n, rho, r, c[:-1], alpha * c)
+    rho32, r32 = f32(rho), f32(r)
+    want = np.maximum((c[:, None] * (rho32 + alpha * r32)).sum(0), 0.0)
+    b = rho32[-1]
+    mag = np.abs(b) + (np.abs(c[:-1, None]) * np.abs(rho32[:-1] - b)).sum(0) + (alpha * np.abs(c[:, None] * r32)).sum(0)
+    _check_rel("diis_mix", out, want, mag)
+    if m < 6:
+        assert (want == 0.0).any() and (out == 0.0).any(), "the clamp must be exercised"
+    assert np.all(out >= 0.0)
