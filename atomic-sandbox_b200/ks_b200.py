@@ -332,6 +332,12 @@ class ScfSettings:
     occupations: str = "aufbau"  # or "fermi_dirac" (qm::Occupations, crates/qm/src/scf.rs:278)
     kt: float = 5e-3             # Fermi-Dirac temperature (Ha), ELECTRON_KT (crates/qm/src/occupations.rs)
 
+    @classmethod
+    def for_grid(cls, h):
+        """The reference's defaults (ScfSettings::for_grid, crates/qm/src/scf.rs:381-395): sigma = h and Fermi-Dirac
+        occupations at ELECTRON_KT; the solver then needs n_extra >= 1 (room for the gap witness)."""
+        return cls(sigma=float(h), occupations="fermi_dirac", kt=5e-3)
+
 
 @dataclasses.dataclass
 class System:

@@ -46,7 +46,10 @@ struct System {
 // qm::Occupations (crates/qm/src/scf.rs:278).
 enum class Occupations { Aufbau, FermiDirac };
 
-// qm::ScfSettings (crates/qm/src/scf.rs:375) with the reference's defaults; sigma has none here (the reference's is h).
+// qm::ScfSettings (crates/qm/src/scf.rs:375). A default-constructed one has the reference's tolerances, mixing and
+// history but Aufbau occupations and no sigma (which the solve refuses): the reference's defaults come from for_grid,
+// which needs a grid spacing. ScfSettings::for_grid(h) is that constructor (scf.rs:381-395: sigma = h, Fermi-Dirac at
+// ELECTRON_KT); under Fermi-Dirac the solver needs options with n_extra >= 1, a block with room for the gap witness.
 struct ScfSettings {
     double sigma = 0.0;
     double tol = 1e-6;
@@ -57,6 +60,14 @@ struct ScfSettings {
     int stall_window = 50;
     Occupations occupations = Occupations::Aufbau;
     double kt = 5e-3;  // ELECTRON_KT (crates/qm/src/occupations.rs:166), used under FermiDirac only
+
+    static ScfSettings for_grid(double h) {
+        ScfSettings s;
+        s.sigma = h;
+        s.occupations = Occupations::FermiDirac;
+        s.kt = 5e-3;
+        return s;
+    }
 };
 
 using Energy = ks_energy;        // qm::Energy (crates/qm/src/scf.rs:533)

@@ -102,6 +102,10 @@ void check_occupations() {
     const auto w = qm_gpu::fd_witness(evals, 1, -0.4, 5e-3);
     expect(w.first && w.second == 5, "fd_witness: the witness and its passing spare are kept");
     expect(!qm_gpu::fd_witness({-0.3, -0.3 + 0.099, -0.5}, 2, -0.4, 5e-3).first, "fd_witness: the gap arm");
+    const qm_gpu::ScfSettings fg = qm_gpu::ScfSettings::for_grid(0.25);
+    expect(fg.sigma == 0.25 && fg.occupations == qm_gpu::Occupations::FermiDirac && fg.kt == 5e-3 && fg.tol == 1e-6 &&
+               fg.eig_tol == 1e-6 && fg.mixing == 0.3 && fg.max_iter == 200 && fg.diis_history == 6 && fg.stall_window == 50,
+           "ScfSettings::for_grid: the reference's defaults");
     const auto wb = qm_gpu::fd_witness_bound(evals, {0.0, 0.0, 0.0, 0.15, 0.0, 0.0, 0.0}, 1, -0.4, 5e-3);
     expect(wb.first && wb.second == 6, "fd_witness_bound: the witness's own residual pushes it up a rank");
     expect(throws<qm_gpu::InvalidArgument>([&] { qm_gpu::fd_witness_bound(evals, {0.0}, 1, -0.4, 5e-3); }),

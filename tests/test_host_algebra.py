@@ -116,3 +116,12 @@ def test_witness_reads_the_lower_bound(ks):
     assert ks.fd_witness(block, 0, mu, kt, residuals=zero)[1] == 7  # an empty channel keeps its block
     with pytest.raises(ValueError):
         ks.fd_witness(block, 1, mu, kt, residuals=zero[:3])
+
+
+def test_scf_settings_for_grid_has_the_reference_defaults(ks):
+    """ScfSettings::for_grid (crates/qm/src/scf.rs:381-395): sigma = h, tol 1e-6, 200 iterations, mixing 0.3, eig_tol
+    1e-6, DIIS history 6, Fermi-Dirac at ELECTRON_KT = 5e-3, the stall window 50; the plain constructor keeps Aufbau."""
+    s = ks.ScfSettings.for_grid(0.25)
+    assert (s.sigma, s.tol, s.max_iter, s.mixing, s.eig_tol, s.diis_history, s.stall_window) == (0.25, 1e-6, 200, 0.3, 1e-6, 6, 50)
+    assert s.occupations == "fermi_dirac" and s.kt == 5e-3
+    assert ks.ScfSettings().occupations == "aufbau"
