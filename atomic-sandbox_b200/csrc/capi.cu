@@ -701,6 +701,107 @@ ks_status ks_diis_mix(int n, int m, const double* rho, const double* r, const do
     });
 }
 
+ks_status ks_autotune_stencil(int n, const int* counts, int ncount, int* chunks_out) {
+    if (n < 5 || n > 1024 || !counts || ncount < 1 || ncount > 64) return fail(nullptr, KS_INVALID, "invalid arguments");
+    int kmax = 0;
+    for (int i = 0; i < ncount; ++i) {
+        if (counts[i] < 1 || counts[i] > 64) return fail(nullptr, KS_INVALID, "autotune_stencil: vector counts are 1..64");
+        kmax = std::max(kmax, counts[i]);
+    }
+    return guarded(nullptr, [&] {
+        const double h = 0.25;
+        Scratch sc(n, h);
+        const Layout& L = sc.L;
+        // scratch fields (zero): x and its tensor map, the output, r and the stored factors, V, lambda
+        Block x, y, r, d, v;
+        x.create(L, kmax);
+        y.create(L, kmax);
+        r.create(L, kmax);
+        d.create(L, kmax);
+        v.create(L, 1);
+        DevBuf lam((size_t)kmax * sizeof(double));
+        for (Block* b : {&x, &y, &r, &d, &v}) KS_CUDA(cudaMemsetAsync(b->buf.p, 0, b->buf.bytes, sc.s));
+        KS_CUDA(cudaMemsetAsync(lam.p, 0, lam.bytes, sc.s));
+        cudaEvent_t e0, e1;
+        KS_CUDA(cudaEventCreate(&e0));
+        KS_CUDA(cudaEventCreate(&e1));
+        for (int i = 0; i < ncount; ++i) {
+            const int k = counts[i];
+            for (int mi = 0; mi < 2; ++mi) {
+                StencilArgs a;
+                a.mode = mi == 0 ? ST_HAMILTONIAN : ST_JACOBI;
+                a.scale = (float)(-0.5 / (h * h));
+                a.V = v.at(0);
+                if (a.mode == ST_JACOBI) {
+                    a.R = r.at(0);
+                    a.lambda = lam.d();
+                    a.omega = 0.5f;
+                    a.diag_t = (float)(1.5 * 205.0 / 72.0 / (h * h));
+                    a.dinv = d.at(0);
+                }
+                // every distinct chunking of the candidates 1 .. max: the best of three timings of four launches each
+                int best_c = 0, last_zc = -1;
+                float best_ms = 0.f;
+                for (int c = 1; c <= stencil_max_chunks(L); ++c) {
+                    const int zc = (n + c - 1) / c;
+                    if (zc == last_zc) continue;
+                    last_zc = zc;
+                    a.chunks = c;
+                    for (int w = 0; w < 2; ++w) launch_stencil(L, x.tmap, k, a, y.at(0), sc.s);
+                    float t_min = 0.f;
+                    for (int rep = 0; rep < 3; ++rep) {
+                        KS_CUDA(cudaEventRecord(e0, sc.s));
+                        for (int j = 0; j < 4; ++j) launch_stencil(L, x.tmap, k, a, y.at(0), sc.s);
+                        KS_CUDA(cudaEventRecord(e1, sc.s));
+                        KS_CUDA(cudaEventSynchronize(e1));
+                        float ms = 0.f;
+                        KS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                        if (rep == 0 || ms < t_min) t_min = ms;
+                    }
+                    if (best_c == 0 || t_min < best_ms) { best_c = c; best_ms = t_min; }
+                }
+                stencil_set_tuned_chunks(n, k, a.mode, best_c);
+                if (chunks_out) chunks_out[2 * i + mi] = best_c;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        check_device_flag(sc.s);
+        return KS_OK;
+    });
+}
+
+int ks_stencil_tuning_get(int* entries4, int cap) {
+    try {
+        const auto e = stencil_tuning_entries();
+        for (int i = 0; i < (int)e.size() && i < cap && entries4; ++i)
+            for (int j = 0; j < 4; ++j) entries4[4 * i + j] = e[i][j];
+        return (int)e.size();
+    } catch (...) {
+        return -1;
+    }
+}
+
+ks_status ks_stencil_tuning_set(const int* entries4, int count) {
+    if (count < 0 || (count > 0 && !entries4)) return fail(nullptr, KS_INVALID, "invalid arguments");
+    for (int i = 0; i < count; ++i) {
+        const int* e = entries4 + 4 * i;
+        if (e[0] < 5 || e[0] > 1024 || e[1] < 1 || e[1] > 64 || (e[2] != ST_HAMILTONIAN && e[2] != ST_JACOBI) || e[3] < 1 || e[3] > e[0])
+            return fail(nullptr, KS_INVALID, "stencil_tuning_set: entries are (n in 5..1024, count in 1..64, mode 1 or 2, 1 <= chunks <= n)");
+    }
+    return guarded(nullptr, [&] {
+        for (int i = 0; i < count; ++i) stencil_set_tuned_chunks(entries4[4 * i], entries4[4 * i + 1], entries4[4 * i + 2], entries4[4 * i + 3]);
+        return KS_OK;
+    });
+}
+
+ks_status ks_stencil_tuning_clear(void) {
+    return guarded(nullptr, [&] {
+        stencil_tuning_clear();
+        return KS_OK;
+    });
+}
+
 ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gram_mode, double* out) {
     if (n < 1 || m < 1 || mt < 0 || !s || (mt > 0 && !t) || !out || gram_mode < 0 || gram_mode > 1 || (gram_mode == 1 && mt < 1))
         return fail(nullptr, KS_INVALID, "invalid arguments");

@@ -21,6 +21,9 @@
 // the quad's pad columns are stored as 0. Measured against the 2 x 2-outputs-per-thread form it replaces: the same
 // outputs bit for bit at h = 0.25, and H psi on 95^3 at 8 / 16 / 64 vectors 13 / 13 / 21 % faster.
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cudaTypedefs.h>
 #include "kernels.cuh"
 #include "reduce_util.cuh"
@@ -403,6 +406,28 @@ Shape shape_for(const Layout& L, int count) {
     return sh;
 }
 
+// the shape of a launch with c z-chunks per tile column
+Shape shape_with_chunks(const Layout& L, int c) {
+    Shape sh;
+    sh.tiles_x = ceil_div(L.n, BX);
+    sh.tiles_y = ceil_div(L.n, BY);
+    sh.zc = ceil_div(L.n, std::max(1, std::min(c, L.n)));
+    sh.chunks = ceil_div(L.n, sh.zc);
+    return sh;
+}
+
+// the autotuner's table: (device, n, count, mode) -> z-chunks
+std::mutex tune_mu;
+std::map<std::tuple<int, int, int, int>, int>& tune_table() {
+    static std::map<std::tuple<int, int, int, int>, int> t;
+    return t;
+}
+int current_device() {
+    int d = 0;
+    KS_CUDA(cudaGetDevice(&d));
+    return d;
+}
+
 template <int MODE, bool DOT>
 void launch_mode(const Shape& sh, int count, const CUtensorMap& tmap, const Params& p, float* out, cudaStream_t s) {
     const int smem = NS * PLANE_BYTES;
@@ -430,6 +455,40 @@ void make_field_tmap(CUtensorMap* map, const Layout& L, const float* base, int c
     if (r != CUDA_SUCCESS) throw DeviceError("cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");
 }
 
+void stencil_set_tuned_chunks(int n, int count, int mode, int chunks) {
+    if (mode != ST_HAMILTONIAN && mode != ST_JACOBI) throw std::invalid_argument("stencil tuning: only H psi and the Jacobi sweep are tuned");
+    if (n < 1 || count < 1 || chunks < 1 || chunks > n) throw std::invalid_argument("stencil tuning: need n, count >= 1 and 1 <= chunks <= n");
+    std::lock_guard<std::mutex> g(tune_mu);
+    tune_table()[std::make_tuple(current_device(), n, count, mode)] = chunks;
+}
+
+int stencil_tuned_chunks(int n, int count, int mode) {
+    const int dev = current_device();
+    std::lock_guard<std::mutex> g(tune_mu);
+    auto it = tune_table().find(std::make_tuple(dev, n, count, mode));
+    return it == tune_table().end() ? 0 : it->second;
+}
+
+int stencil_max_chunks(const Layout& L) { return std::max(1, L.n / 8); }
+
+int stencil_model_chunks(const Layout& L, int count) { return shape_for(L, count).chunks; }
+
+std::vector<std::array<int, 4>> stencil_tuning_entries() {
+    const int dev = current_device();
+    std::lock_guard<std::mutex> g(tune_mu);
+    std::vector<std::array<int, 4>> out;
+    for (const auto& e : tune_table())
+        if (std::get<0>(e.first) == dev) out.push_back({std::get<1>(e.first), std::get<2>(e.first), std::get<3>(e.first), e.second});
+    return out;
+}
+
+void stencil_tuning_clear() {
+    const int dev = current_device();
+    std::lock_guard<std::mutex> g(tune_mu);
+    for (auto it = tune_table().begin(); it != tune_table().end();)
+        it = std::get<0>(it->first) == dev ? tune_table().erase(it) : std::next(it);
+}
+
 int stencil_ctas(const Layout& L, int count) {
     Shape sh = shape_for(L, count);
     return sh.tiles_x * sh.tiles_y * sh.chunks * count;
@@ -447,7 +506,12 @@ int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const St
         (a.R && (reinterpret_cast<uintptr_t>(a.R) & 15)) || (a.out2 && (reinterpret_cast<uintptr_t>(a.out2) & 15)) ||
         (a.dinv && (reinterpret_cast<uintptr_t>(a.dinv) & 15)))
         throw std::invalid_argument("stencil: fields must be 16-byte aligned");
-    Shape sh = shape_for(L, count);
+    const bool dot = a.dot_partials != nullptr;
+    // the chunking: the caller's, else the autotuner's for the modes whose outputs do not depend on it, else the model's
+    int chunks = a.chunks;
+    if (chunks <= 0 && !dot && (a.mode == ST_HAMILTONIAN || a.mode == ST_JACOBI)) chunks = stencil_tuned_chunks(L.n, count, a.mode);
+    if (chunks > 0 && dot) throw std::invalid_argument("stencil: a forced chunking is for the launches without dot partials");
+    Shape sh = chunks > 0 ? shape_with_chunks(L, chunks) : shape_for(L, count);
     Params p;
     p.n = L.n;
     p.P = L.P;
@@ -467,7 +531,6 @@ int launch_stencil(const Layout& L, const CUtensorMap& tmap, int count, const St
     p.theta = a.theta;
     p.out2 = a.out2;
     p.dinv = a.dinv;
-    const bool dot = a.dot_partials != nullptr;
     switch (a.mode) {
         case ST_LAPLACIAN:
             if (dot) launch_mode<ST_LAPLACIAN, true>(sh, count, tmap, p, out, s);

@@ -1,6 +1,8 @@
 // kernels.cuh -- host-side launchers of the B200 kernels (sm_100a). Every launcher takes the
 // stream it enqueues on and returns immediately; none synchronises.
 #pragma once
+#include <array>
+#include <vector>
 #include <cuda.h>
 #include "common.cuh"
 
@@ -82,7 +84,20 @@ struct StencilArgs {
     // the sweep's per-point factor omega / max(diag_t + V - lambda, 0.1) of each vector (block, stride F): written by
     // HAM_RESIDUAL when set, read by JACOBI when set (else JACOBI computes it, to the same bits)
     float* dinv = nullptr;
+    // z-chunks per tile column; 0: the tuned choice for this shape (ST_HAMILTONIAN without dots, ST_JACOBI) when the
+    // autotuner recorded one on this device, else the cost model's
+    int chunks = 0;
 };
+// The launch-shape autotuner's table (per device, process-wide): the z-chunk count for H psi (ST_HAMILTONIAN without
+// dots) and the Jacobi sweep (ST_JACOBI) of `count` vectors on an n^3 grid. Those two modes are the ones whose outputs
+// do not depend on the chunking (no per-CTA partial sums), so a tuned launch gives the same bits.
+void stencil_set_tuned_chunks(int n, int count, int mode, int chunks);
+int stencil_tuned_chunks(int n, int count, int mode);  // 0: none
+int stencil_max_chunks(const Layout& L);                // the candidates are 1 .. this
+int stencil_model_chunks(const Layout& L, int count);   // the cost model's choice
+// the current device's entries as (n, count, mode, chunks) quadruples
+std::vector<std::array<int, 4>> stencil_tuning_entries();
+void stencil_tuning_clear();
 // CTAs per vector of a stencil launch of `count` vectors (the leading dimension of ST_HAM_RESIDUAL's partials)
 int stencil_ctas_per_vector(const Layout& L, int count);
 // out_v = op(x_v) for the `count` vectors of the block x (stride F). `tmap` must describe x

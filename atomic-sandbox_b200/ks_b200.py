@@ -14,6 +14,7 @@ missing or cannot be loaded raises at load time -- there is no CPU fallback.
 """
 import ctypes
 import dataclasses
+import json
 import math
 import os
 import subprocess
@@ -200,7 +201,8 @@ EXPORTED = [
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
     "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
-    "ks_fd_witness", "ks_fd_witness_bound", "ks_density_residual", "ks_diis_mix", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
+    "ks_fd_witness", "ks_fd_witness_bound", "ks_density_residual", "ks_diis_mix", "ks_autotune_stencil",
+    "ks_stencil_tuning_get", "ks_stencil_tuning_set", "ks_stencil_tuning_clear", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
     "ks_test_poison_parked_density", "ks_test_fail_readbacks",
 ]
 
@@ -261,6 +263,11 @@ def lib():
         L.ks_fd_witness.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
         L.ks_fd_witness_bound.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
         L.ks_field_pitch.argtypes = [ctypes.c_int]
+        L.ks_autotune_stencil.argtypes = [ctypes.c_int, ip, ctypes.c_int, ip]
+        L.ks_stencil_tuning_get.restype = ctypes.c_int
+        L.ks_stencil_tuning_get.argtypes = [ip, ctypes.c_int]
+        L.ks_stencil_tuning_set.argtypes = [ip, ctypes.c_int]
+        L.ks_stencil_tuning_clear.argtypes = []
         L.ks_launch_count.restype = ctypes.c_longlong
         L.ks_launch_count.argtypes = []
         L.ks_solver_stream.restype = ctypes.c_void_p
@@ -757,6 +764,60 @@ def fd_witness(evals, n, mu, kt, residuals=None):
         _check(lib().ks_fd_witness_bound(_p(ev), _p(r), ev.size, int(n), float(mu), float(kt), ctypes.byref(reached),
                                          ctypes.byref(keep)))
     return bool(reached.value), keep.value
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+STENCIL_MODES = {1: "hpsi", 2: "jacobi"}
+
+
+def autotune_stencil(n, counts):
+    """Times every z-chunking of H psi and of the Jacobi sweep for each vector count on an n^3 grid and keeps the
+    fastest for this process's later launches on this device (the outputs do not depend on the chunking).
+    Returns {count: {"hpsi": chunks, "jacobi": chunks}}."""
+    c = np.ascontiguousarray(counts, dtype=np.int32)
+    out = np.zeros(2 * c.size, dtype=np.int32)
+    _check(lib().ks_autotune_stencil(int(n), _ip(c), c.size, _ip(out)))
+    return {int(k): {"hpsi": int(out[2 * i]), "jacobi": int(out[2 * i + 1])} for i, k in enumerate(c)}
+
+
+def stencil_tuning():
+    """The current device's tuning table: [(n, count, mode, chunks)], mode 1 = H psi, 2 = the Jacobi sweep."""
+    total = lib().ks_stencil_tuning_get(None, 0)
+    if total < 0:
+        raise Device("stencil_tuning: no CUDA device")
+    buf = np.zeros(4 * max(total, 1), dtype=np.int32)
+    total = lib().ks_stencil_tuning_get(_ip(buf), total)
+    return [tuple(int(v) for v in buf[4 * i:4 * i + 4]) for i in range(total)]
+
+
+def set_stencil_tuning(entries):
+    """Installs (n, count, mode, chunks) entries on the current device (e.g. loaded from a file)."""
+    e = np.ascontiguousarray(np.asarray(list(entries), dtype=np.int32).reshape(-1, 4))
+    _check(lib().ks_stencil_tuning_set(_ip(e), e.shape[0]))
+
+
+def clear_stencil_tuning():
+    _check(lib().ks_stencil_tuning_clear())
+
+
+def save_stencil_tuning(path):
+    """Writes the current device's tuning table as JSON (with the device's name, which a load checks)."""
+    import torch
+    with open(path, "w") as f:
+        json.dump({"device": torch.cuda.get_device_name(), "entries": [list(e) for e in stencil_tuning()]}, f)
+
+
+def load_stencil_tuning(path):
+    """Installs a table written by save_stencil_tuning; a table from another device model is refused (ValueError)."""
+    import torch
+    with open(path) as f:
+        d = json.load(f)
+    if d.get("device") != torch.cuda.get_device_name():
+        raise ValueError(f"stencil tuning for {d.get('device')!r}, not {torch.cuda.get_device_name()!r}")
+    set_stencil_tuning(d["entries"])
 
 
 def density_residual(n, h, psi, rho_in, f=None):

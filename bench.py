@@ -297,6 +297,9 @@ def bench_ours(args):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
     system = ks.System(NUCLEI, N_UP, N_DN)
     settings = ks.ScfSettings(sigma=SIGMA, tol=1e-6)
+    # the stencil's launch-shape autotuner, before any timing: it picks the z-chunking of the H psi and sweep shapes of
+    # this workload (the outputs do not depend on it)
+    tuned = ks.autotune_stencil(N, [N_UP + N_EXTRA, 2 * (N_UP + N_EXTRA), 64]) if args.autotune else None
 
     def barrier():
         torch.cuda.synchronize()
@@ -380,7 +383,8 @@ def bench_ours(args):
     line = {
         "metric": METRIC, "value": t_max, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * t_max, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (fixed geometry)", "config": dict(CONFIG, parallelism=f"replicas x{world}"),
+        "data": "synthetic (fixed geometry)",
+        "config": dict(CONFIG, parallelism=f"replicas x{world}", stencil_chunks=("autotuned " + json.dumps(tuned)) if tuned else "cost model"),
         "forms": {"plain_fp32_s": statistics.mean(plain["times"]) if plain else None,
                   "mixed_s": statistics.mean(mixed["times"]) if mixed else None,
                   "mixed_speedup": (statistics.mean(plain["times"]) / statistics.mean(mixed["times"])) if (plain and mixed) else None,
@@ -490,6 +494,7 @@ def main():
     ap.add_argument("--workers", type=int, default=4, help="concurrent solves for --workload batch")
     ap.add_argument("--serial", action="store_true", help="also time the batch one molecule at a time")
     ap.add_argument("--native", action="store_true", help="--workload batch through the library's thread pool (ks_solve_batch)")
+    ap.add_argument("--autotune", action="store_true", help="run the stencil's launch-shape autotuner before timing")
     ap.add_argument("--ref-grid", type=int, default=0, help="--impl reference: solve this grid instead of 95^3 (a quick check of the line)")
     args = ap.parse_args()
     if args.workload == "batch":

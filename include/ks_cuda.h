@@ -313,6 +313,19 @@ ks_status ks_density_residual(int n, double h, int k, const double* psi, const d
    hold m fields of n^3 points each, c m - 1 and a m coefficients (applied in f32), 1 <= m <= 16; c may be NULL for
    m = 1. */
 ks_status ks_diis_mix(int n, int m, const double* rho, const double* r, const double* c, const double* a, double* out);
+/* The stencil's launch-shape autotuner. For an n^3 grid and each of the ncount vector counts (1..64), times every
+   distinct z-chunking of H psi and of the Jacobi sweep on zeroed scratch fields of the current device (CUDA events, the
+   best of three timings of four launches) and records the fastest in a process-wide table that later launches of that
+   shape on this device use. Only these two modes are tuned: their outputs do not depend on the chunking, so a tuned
+   solve gives the same bits as an untuned one. chunks_out (2 * ncount ints, may be NULL) receives the choices, H psi
+   then the sweep for each count. Synchronises the device's work on its own stream; takes well under a second at 95^3. */
+ks_status ks_autotune_stencil(int n, const int* counts, int ncount, int* chunks_out);
+/* The tuning table of the current device as (n, count, mode, chunks) quadruples (mode 1 H psi, 2 the sweep): copies up
+   to cap entries and returns their total number (-1 without a device). _set installs entries (e.g. saved by an earlier
+   process), _clear drops this device's. */
+int ks_stencil_tuning_get(int* entries4, int cap);
+ks_status ks_stencil_tuning_set(const int* entries4, int count);
+ks_status ks_stencil_tuning_clear(void);
 /* Reducer::gram / block_dots (crates/qm-gpu/src/reduce.rs:340-420): G = S^T [S | T], m and mt fields, gram_mode as
    in ks_options; out row-major m x (m + mt). */
 ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gram_mode, double* out);

@@ -101,6 +101,10 @@ extern "C" {
     pub fn ks_density_to_volume(s: *mut c_void, dense_dev: *mut f32, stream: *mut c_void) -> c_int;
     pub fn ks_density_with_core_to_volume(s: *mut c_void, dense_dev: *mut f32, stream: *mut c_void,
                                           max_out: *mut c_double) -> c_int;
+    pub fn ks_autotune_stencil(n: c_int, counts: *const c_int, ncount: c_int, chunks_out: *mut c_int) -> c_int;
+    pub fn ks_stencil_tuning_get(entries4: *mut c_int, cap: c_int) -> c_int;
+    pub fn ks_stencil_tuning_set(entries4: *const c_int, count: c_int) -> c_int;
+    pub fn ks_stencil_tuning_clear() -> c_int;
     pub fn ks_density_residual(n: c_int, h: c_double, k: c_int, psi: *const c_double, f: *const c_double, rho_in: *const c_double,
                                rho_out: *mut c_double, r: *mut c_double, sums: *mut c_double) -> c_int;
     pub fn ks_diis_mix(n: c_int, m: c_int, rho: *const c_double, r: *const c_double, c: *const c_double, a: *const c_double,

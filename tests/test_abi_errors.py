@@ -80,3 +80,19 @@ def test_no_device_fails_loudly(ks):
         ks.apply_laplacian(33, 0.25, np.zeros(33 ** 3))
     # the wait-timeout status of the device-pointer calls needs a device too: a status, not a trap
     assert lib.ks_device_status(None) == ks.KS_DEVICE
+
+
+def test_autotuner_arguments_are_refused_before_any_device_work(ks):
+    """The stencil autotuner and its table refuse bad grids, vector counts and entries with KS_INVALID (ValueError)."""
+    with pytest.raises(ValueError):
+        ks.autotune_stencil(4, [8])        # grid below 5
+    with pytest.raises(ValueError):
+        ks.autotune_stencil(95, [0])       # vector counts are 1..64
+    with pytest.raises(ValueError):
+        ks.autotune_stencil(95, [65])
+    with pytest.raises(ValueError):
+        ks.set_stencil_tuning([(95, 8, 3, 5)])   # only H psi (1) and the sweep (2) are tuned
+    with pytest.raises(ValueError):
+        ks.set_stencil_tuning([(95, 8, 1, 96)])  # more chunks than planes
+    with pytest.raises(ValueError):
+        ks.set_stencil_tuning([(95, 0, 1, 5)])
