@@ -848,6 +848,14 @@ ks_status ks_fd_witness(const double* evals, int k, int n, double mu, double kt,
     return ks_fd_witness_bound(evals, nullptr, k, n, mu, kt, reached, keep);
 }
 
+ks_status ks_fd_witness_keep_within(const double* evals, const double* residuals, int k, int n, double mu, double kt, double tail_kt,
+                                    double r_max, int* keep) {
+    if (k < 0 || n < 0 || (k > 0 && (!evals || !residuals)) || !keep || !std::isfinite(tail_kt))
+        return fail(nullptr, KS_INVALID, "invalid arguments");
+    *keep = dense::fd_witness_keep_within(evals, residuals, k, n, mu, kt, tail_kt, r_max);
+    return KS_OK;
+}
+
 ks_status ks_fd_witness_bound(const double* evals, const double* residuals, int k, int n, double mu, double kt, int* reached, int* keep) {
     if (k < 0 || n < 0 || (k > 0 && !evals) || !reached || !keep) return fail(nullptr, KS_INVALID, "invalid arguments");
     *reached = dense::fd_witness(evals, residuals, k, n, mu, kt) ? 1 : 0;

@@ -382,6 +382,20 @@ bool fd_witness(const double* ev, const double* res, int k, int n, double mu, do
     return lower >= ev[o[n - 1]] + 0.1 && lower - mu >= 36.0 * kt;
 }
 
+int fd_witness_keep_within(const double* ev, const double* res, int k, int n, double mu, double kt, double tail_kt, double r_max) {
+    if (n == 0) return k;
+    if (k <= n) return -1;
+    const std::vector<int> o = ascending(ev, k);
+    const double eps_n = ev[o[n - 1]];
+    auto passes = [&](int r) {
+        const double lower = ev[o[r]] - (res ? res[o[r]] : 0.0);
+        return lower >= eps_n + 0.1 && lower - mu >= tail_kt * kt;
+    };
+    for (int t = n; t < k; ++t)
+        if (passes(t) && (res ? res[o[t]] : 0.0) <= r_max) return (t + 1 < k && passes(t + 1)) ? t + 2 : t + 1;
+    return -1;
+}
+
 int fd_witness_keep(const double* ev, const double* res, int k, int n, double mu, double kt) {
     if (n == 0 || k <= n) return k;
     const std::vector<int> o = ascending(ev, k);

@@ -45,6 +45,11 @@ bool fd_witness(const double* evals, const double* res, int k, int n, double mu,
 // bounds): t + 1 for the lowest rank t >= n whose bound passes both arms, t + 2 when the rank above passes too; k when
 // none does or n = 0.
 int fd_witness_keep(const double* evals, const double* res, int k, int n, double mu, double kt);
+// The lowest converged witness (occupations.rs:396-419 witness_keep_within, the tail arm at tail_kt kT): the lowest rank
+// t >= n whose lower bound passes both arms with its residual at most r_max decides, keeping t + 1 levels (t + 2 when
+// rank t + 1 passes on its lower bound too); -1 when no such level exists (the block must grow); k for n = 0. A NaN
+// residual never qualifies.
+int fd_witness_keep_within(const double* evals, const double* res, int k, int n, double mu, double kt, double tail_kt, double r_max);
 
 }  // namespace dense
 }  // namespace ks

@@ -1398,7 +1398,9 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             // reference's initial orbital with seed 1000 + 2 * index + spin) and the channel is solved again with every
             // level held to the step's tolerance; once witnessed, the overshoot above the lowest witness is trimmed, never
             // below the configured N_sigma + n_extra. The witness is read on the lower bounds theta - r (occupations.rs:93-99,
-            // witness_bound_reached): every column is held to the step's tolerance, so r is that small.
+            // witness_bound_reached). On a tight step a witness whose top level exits above EIG_GUESS_FACTOR * the guard
+            // tolerance decides only through the lowest level that passes at or below that residual (witness_keep_within,
+            // occupations.rs:396-419; crates/qm-gpu/src/scf.rs:940-965); without one the block grows by one vector.
             for (int sp = 0; sp < 2 && fd; ++sp) {
                 if (nocc[sp] == 0) continue;
                 const int base = nocc[sp] + opt_.n_extra;
@@ -1409,17 +1411,33 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                     if (!dense::fermi_dirac(ch_[sp].evals.data(), kk[sp], nocc[sp], s.kt, f.data(), m_sp, s_sp))
                         throw NumericalError("Fermi-Dirac occupations refused (a non-finite level)");
                     const int extras = kk[sp] - nocc[sp];
-                    if (dense::fd_witness(ch_[sp].evals.data(), ch_[sp].res.data(), kk[sp], nocc[sp], m_sp, s.kt)) {
-                        const int keep = std::max(base, dense::fd_witness_keep(ch_[sp].evals.data(), ch_[sp].res.data(), kk[sp], nocc[sp], m_sp, s.kt));
-                        if (keep < kk[sp]) {
-                            resize_channel(sp, keep, dnuc, nn);
-                            kk[sp] = keep;
-                            tight[sp] = std::min(tight[sp], keep);
+                    const double* ev = ch_[sp].evals.data();
+                    const double* rv = ch_[sp].res.data();
+                    int grown;
+                    if (dense::fd_witness(ev, rv, kk[sp], nocc[sp], m_sp, s.kt)) {
+                        int top = 0;
+                        for (int i = 1; i < kk[sp]; ++i)
+                            if (ev[i] > ev[top]) top = i;
+                        const double r_witness = EIG_GUESS_FACTOR * WITNESS_GUARD_TOL;
+                        int keep;
+                        if (step_tol <= eig_lo && !(rv[top] <= r_witness) && extras < cap)
+                            keep = dense::fd_witness_keep_within(ev, rv, kk[sp], nocc[sp], m_sp, s.kt, 36.0, r_witness);
+                        else
+                            keep = dense::fd_witness_keep(ev, rv, kk[sp], nocc[sp], m_sp, s.kt);
+                        if (keep >= 0) {
+                            keep = std::max(base, keep);
+                            if (keep < kk[sp]) {
+                                resize_channel(sp, keep, dnuc, nn);
+                                kk[sp] = keep;
+                                tight[sp] = std::min(tight[sp], keep);
+                            }
+                            break;
                         }
-                        break;
+                        grown = extras + 1;  // no converged witness below the loose top: one vector more
+                    } else {
+                        if (extras >= cap) break;  // the witness check at convergence reports the cap
+                        grown = std::min(std::max(2 * extras, extras + 1), cap);
                     }
-                    if (extras >= cap) break;  // the witness check at convergence reports the cap
-                    const int grown = std::min(std::max(2 * extras, extras + 1), cap);
                     resize_channel(sp, nocc[sp] + grown, dnuc, nn);
                     kk[sp] = nocc[sp] + grown;
                     ++profile.witness_growths;

@@ -201,7 +201,7 @@ EXPORTED = [
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
     "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
-    "ks_fd_witness", "ks_fd_witness_bound", "ks_density_residual", "ks_diis_mix", "ks_autotune_stencil",
+    "ks_fd_witness", "ks_fd_witness_bound", "ks_fd_witness_keep_within", "ks_density_residual", "ks_diis_mix", "ks_autotune_stencil",
     "ks_stencil_tuning_get", "ks_stencil_tuning_set", "ks_stencil_tuning_clear", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
     "ks_test_poison_parked_density", "ks_test_fail_readbacks",
 ]
@@ -262,6 +262,8 @@ def lib():
         L.ks_fermi_dirac.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
         L.ks_fd_witness.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
         L.ks_fd_witness_bound.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
+        L.ks_fd_witness_keep_within.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_double, ip]
         L.ks_field_pitch.argtypes = [ctypes.c_int]
         L.ks_autotune_stencil.argtypes = [ctypes.c_int, ip, ctypes.c_int, ip]
         L.ks_stencil_tuning_get.restype = ctypes.c_int
@@ -846,6 +848,18 @@ def diis_mix(n, rho, r, c, a):
     out = np.empty(n3)
     _check(lib().ks_diis_mix(n, m, _p(rho), _p(r), _p(ca) if m > 1 else None, _p(aa), _p(out)))
     return out
+
+
+def fd_witness_keep_within(evals, residuals, n, mu, kt, r_max, tail_kt=36.0):
+    """The lowest converged witness (crates/qm/src/occupations.rs witness_keep_within): the count of levels to keep, or
+    None when no level above the n-th passes both arms on its lower bound at a residual within r_max."""
+    ev, r = _f64(evals), _f64(residuals)
+    if r.size != ev.size:
+        raise ValueError("fd_witness_keep_within: one residual per level")
+    keep = ctypes.c_int()
+    _check(lib().ks_fd_witness_keep_within(_p(ev), _p(r), ev.size, int(n), float(mu), float(kt), float(tail_kt), float(r_max),
+                                           ctypes.byref(keep)))
+    return None if keep.value < 0 else keep.value
 
 
 def gram(n, s, t, gram_mode=0):

@@ -356,6 +356,12 @@ ks_status ks_fd_witness(const double* evals, int k, int n, double mu, double kt,
    keep = witness_keep (:372-394). residuals may be NULL (all zero: ks_fd_witness); a NaN residual never passes. */
 ks_status ks_fd_witness_bound(const double* evals, const double* residuals, int k, int n, double mu, double kt, int* reached,
                               int* keep);
+/* The lowest converged witness (crates/qm/src/occupations.rs:396-419 witness_keep_within): the lowest level above the
+   n-th whose lower bound theta - r passes both arms (the tail arm at tail_kt kT) with r <= r_max decides, and keep gets
+   the levels to keep (its rank + 1, + 2 with a passing spare above it); keep = -1 when no level qualifies (the block must
+   grow), k for n = 0. The solver applies it on a tight step whose top level passes only at r > 1.5e-3 Ha. */
+ks_status ks_fd_witness_keep_within(const double* evals, const double* residuals, int k, int n, double mu, double kt, double tail_kt,
+                                    double r_max, int* keep);
 
 /* ---- device-pointer entry points for callers that keep fields on the GPU (bench, integrations) ----
    Fields are in the pitched layout: element (i, j, k) at (k*n + j)*P + i, P = ks_field_pitch(n),

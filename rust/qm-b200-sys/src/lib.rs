@@ -92,6 +92,8 @@ extern "C" {
                           entropy: *mut c_double) -> c_int;
     pub fn ks_fd_witness(evals: *const c_double, k: c_int, n: c_int, mu: c_double, kt: c_double, reached: *mut c_int,
                          keep: *mut c_int) -> c_int;
+    pub fn ks_fd_witness_keep_within(evals: *const c_double, residuals: *const c_double, k: c_int, n: c_int, mu: c_double,
+                                     kt: c_double, tail_kt: c_double, r_max: c_double, keep: *mut c_int) -> c_int;
     pub fn ks_fd_witness_bound(evals: *const c_double, residuals: *const c_double, k: c_int, n: c_int, mu: c_double,
                                kt: c_double, reached: *mut c_int, keep: *mut c_int) -> c_int;
     pub fn ks_solve_batch(jobs: *mut ks_batch_job, n_jobs: c_int, opts: *const ks_options, workers: c_int) -> c_int;

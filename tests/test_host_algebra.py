@@ -125,3 +125,32 @@ def test_scf_settings_for_grid_has_the_reference_defaults(ks):
     assert (s.sigma, s.tol, s.max_iter, s.mixing, s.eig_tol, s.diis_history, s.stall_window) == (0.25, 1e-6, 200, 0.3, 1e-6, 6, 50)
     assert s.occupations == "fermi_dirac" and s.kt == 5e-3
     assert ks.ScfSettings().occupations == "aufbau"
+
+
+def test_witness_keep_within_reads_the_lowest_converged_witness(ks):
+    """The reference's test of the lowest converged witness (crates/qm/src/occupations.rs:706-745
+    witness_keep_within_reads_the_lowest_converged_witness), on the rule the solver applies on a tight step whose top
+    level passes only above 1.5e-3 Ha."""
+    kt, mu, r_max = 5e-3, -0.4, 1.5e-3  # the arms: lower bound >= mu + 0.18 = -0.22 and >= eps_(1) + 0.1 = -0.4
+    evals = [-0.5, -0.3, -0.25, -0.1, -0.05, 0.0, 0.3]
+    zero = [0.0] * 7
+    kw = ks.fd_witness_keep_within
+    assert kw(evals, zero, 1, mu, kt, r_max) == ks.fd_witness(evals, 1, mu, kt, residuals=zero)[1] == 5
+    top_loose = [0.0, 0.0, 0.0, 1e-4, 0.0, 0.0, 3e-3]
+    assert kw(evals, top_loose, 1, mu, kt, r_max) == 5
+    first_loose = [0.0, 0.0, 0.0, 2e-3, 1e-3, 3e-3, 3e-3]
+    assert kw(evals, first_loose, 1, mu, kt, r_max) == 6
+    only_top = [0.0, 0.0, 0.0, 2e-3, 2e-3, 2e-3, 1e-3]
+    assert kw(evals, only_top, 1, mu, kt, r_max) == 7
+    assert kw(evals, [0.0, 0.0, 0.0, 2e-3, 2e-3, 2e-3, 2e-3], 1, mu, kt, r_max) is None
+    assert kw(evals[:3], zero[:3], 1, mu, kt, r_max) is None               # rank 2, -0.25 < -0.22: no witness
+    assert kw(evals[:3], zero[:3], 1, mu, kt, r_max, tail_kt=6.0) == 3     # a 6 kT tail lets rank 1 decide
+    for res in (zero, top_loose, first_loose, only_top):
+        k = kw(evals, res, 1, mu, kt, r_max)
+        assert ks.fd_witness(evals[:k], 1, mu, kt, residuals=res[:k])[0]
+        assert res[k - 1] <= r_max or res[k - 2] <= r_max
+    assert kw(evals, zero, 0, mu, kt, r_max) == 7
+    assert kw(evals[:1], zero[:1], 1, mu, kt, r_max) is None
+    e2, r2 = [0.0, -0.5, 0.3, -0.1, -0.3, -0.05, -0.25], [0.0, 0.0, 3e-3, 2e-3, 0.0, 1e-3, 0.0]
+    assert kw(e2, r2, 1, mu, kt, r_max) == 6                                # order-independent
+    assert kw(evals, [0.0, 0.0, 0.0, float("nan"), 0.0, 0.0, 0.0], 1, mu, kt, r_max) == 6  # a NaN residual never qualifies
