@@ -418,6 +418,7 @@ Shape shape_with_chunks(const Layout& L, int c) {
 
 // the autotuner's table: (device, n, count, mode) -> z-chunks
 std::mutex tune_mu;
+std::atomic<int> tune_entries{0};  // table size, read without the lock by every tunable launch
 std::map<std::tuple<int, int, int, int>, int>& tune_table() {
     static std::map<std::tuple<int, int, int, int>, int> t;
     return t;
@@ -460,9 +461,11 @@ void stencil_set_tuned_chunks(int n, int count, int mode, int chunks) {
     if (n < 1 || count < 1 || chunks < 1 || chunks > n) throw std::invalid_argument("stencil tuning: need n, count >= 1 and 1 <= chunks <= n");
     std::lock_guard<std::mutex> g(tune_mu);
     tune_table()[std::make_tuple(current_device(), n, count, mode)] = chunks;
+    tune_entries.store((int)tune_table().size());
 }
 
 int stencil_tuned_chunks(int n, int count, int mode) {
+    if (tune_entries.load() == 0) return 0;
     const int dev = current_device();
     std::lock_guard<std::mutex> g(tune_mu);
     auto it = tune_table().find(std::make_tuple(dev, n, count, mode));
@@ -487,6 +490,7 @@ void stencil_tuning_clear() {
     std::lock_guard<std::mutex> g(tune_mu);
     for (auto it = tune_table().begin(); it != tune_table().end();)
         it = std::get<0>(it->first) == dev ? tune_table().erase(it) : std::next(it);
+    tune_entries.store((int)tune_table().size());
 }
 
 int stencil_ctas(const Layout& L, int count) {
