@@ -305,24 +305,64 @@ void g2_rows_map(CUtensorMap* map, const float* base, long long F, int rows) {
     if (r != CUDA_SUCCESS) throw DeviceError("cuTensorMapEncodeTiled (CUDA-core Gram) failed, code " + std::to_string((int)r));
 }
 
-// ---- multipole moments with on-the-fly real solid harmonics (harmonics.cuh)
+// ---- multipole moments with on-the-fly real solid harmonics: the recurrence of harmonics.cuh with its (l, m) constants
+// read from a table (f_l = sqrt((2l - 1) / (2l)), b_lm = sqrt(max((l - 1)^2 - m^2, 0)) and 1 / sqrt(l^2 - m^2), computed once
+// on the host), the two previous rows kept in registers and each R_lm added to its moment as it is formed: no square
+// root or division per point, no per-point array in local memory. The only difference from solid_harmonics_dev is the
+// product by 1 / d instead of the division by d (within an ulp per step).
+__constant__ double c_hf[7];
+__constant__ double c_hb[7][7];
+__constant__ double c_hinvd[7][7];
+
 __global__ void __launch_bounds__(TPB) moments_kernel(int n, int P, long long F, double h, double origin, const float* __restrict__ rho,
                                                       double* __restrict__ partials) {
     double acc[49];
 #pragma unroll
     for (int q = 0; q < 49; ++q) acc[q] = 0.0;
+    const double s2 = 1.4142135623730951;
     const long long N = (long long)n * n * n;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % n);
         long long rest = p / n;
         int j = (int)(rest % n), k = (int)(rest / n);
-        double r = (double)rho[((long long)k * n + j) * P + i];
+        const double r = (double)rho[((long long)k * n + j) * P + i];
         if (r == 0.0) continue;
-        double hv[49];
-        solid_harmonics_dev(origin + i * h, origin + j * h, origin + k * h, hv);
+        const double x = origin + i * h, y = origin + j * h, z = origin + k * h;
+        const double r2 = x * x + y * y + z * z;
+        double pr[7], pi[7], qr[7], qi[7];  // rows l - 1 and l - 2 of the recurrence
+        pr[0] = 1.0;
+        pi[0] = 0.0;
+        acc[0] += r * 1.0;
 #pragma unroll
-        for (int q = 0; q < 49; ++q) acc[q] += r * hv[q];
+        for (int l = 1; l <= 6; ++l) {
+            double cr[7], ci[7];
+            cr[l] = c_hf[l] * (x * pr[l - 1] - y * pi[l - 1]);
+            ci[l] = c_hf[l] * (x * pi[l - 1] + y * pr[l - 1]);
+            const double a = (2.0 * l - 1.0) * z;
+#pragma unroll
+            for (int m = 0; m < l; ++m) {
+                const double r0 = (l >= 2 && m <= l - 2) ? qr[m] : 0.0, i0 = (l >= 2 && m <= l - 2) ? qi[m] : 0.0;
+                const double b = c_hb[l][m] * r2;
+                cr[m] = (a * pr[m] - b * r0) * c_hinvd[l][m];
+                ci[m] = (a * pi[m] - b * i0) * c_hinvd[l][m];
+            }
+            acc[l * l + l] += r * cr[0];
+#pragma unroll
+            for (int m = 1; m <= l; ++m) {
+                acc[l * l + l + m] += r * (s2 * cr[m]);
+                acc[l * l + l - m] += r * (s2 * ci[m]);
+            }
+#pragma unroll
+            for (int m = 0; m <= l; ++m) {
+                qr[m] = pr[m];
+                qi[m] = pi[m];
+                pr[m] = cr[m];
+                pi[m] = ci[m];
+            }
+        }
     }
+    // unrolled, so that acc stays in registers (a runtime index would put it in local memory for the whole kernel)
+#pragma unroll
     for (int q = 0; q < 49; ++q) {
         double s = block_sum(acc[q]);
         if (threadIdx.x == 0) partials[(size_t)blockIdx.x * 49 + q] = s;
@@ -507,6 +547,20 @@ int launch_gram(long long F, int m, const float* S, int mt, const float* T, doub
 }
 
 void launch_moments(const Layout& L, const float* rho, double* partials, int blocks, cudaStream_t s) {
+    static std::atomic<unsigned long long> consts_set{0};
+    once_per_device(consts_set, [] {
+        double f[7] = {0}, b[7][7] = {{0}}, invd[7][7] = {{0}};
+        for (int l = 1; l <= 6; ++l) {
+            f[l] = std::sqrt((2.0 * l - 1.0) / (2.0 * l));
+            for (int m = 0; m < l; ++m) {
+                b[l][m] = std::sqrt(std::fmax((l - 1.0) * (l - 1.0) - (double)m * m, 0.0));
+                invd[l][m] = 1.0 / std::sqrt((double)l * l - (double)m * m);
+            }
+        }
+        KS_CUDA(cudaMemcpyToSymbol(c_hf, f, sizeof(f)));
+        KS_CUDA(cudaMemcpyToSymbol(c_hb, b, sizeof(b)));
+        KS_CUDA(cudaMemcpyToSymbol(c_hinvd, invd, sizeof(invd)));
+    });
     moments_kernel<<<blocks, TPB, 0, s>>>(L.n, L.P, L.F, L.h, L.origin, rho, partials);
     KS_LAUNCH_CHECK();
 }
