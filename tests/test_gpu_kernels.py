@@ -34,12 +34,13 @@ def test_laplacian_matches_oracle_33(ks, oracle):
     assert err_kernel < 1e-6, err_kernel
 
 
-@pytest.mark.parametrize("n", [5, 6, 9, 17, 32, 33, 48, 50])
+@pytest.mark.parametrize("n", [5, 6, 9, 17, 32, 33, 48, 50, 127, 128, 129, 200])
 def test_hamiltonian_block_matches_oracle(ks, oracle, n):
     """H psi = -1/2 lap psi + V psi for a block of 3 vectors, every tile / chunk edge case of the
     TMA tiling (n below, at and above multiples of the 32 x 16 tile and of the pitch), down to the
     reference's smallest grid, n = 5 (crates/qm-gpu/src/grid.rs:200-211: the whole box inside one
-    tile's halo, the pitch 8 > n)."""
+    tile's halo, the pitch 8 > n), and up to the large grids of the configurations (127..129 around a
+    multiple of every tile edge, 200 with several z-chunks per tile column)."""
     h = 0.3
     nuc = [(0.4, 0.0, -0.3, 3), (-1.1, 0.5, 0.2, 1)]
     v = f32(oracle.nuclear_potential(n, h, nuc, 0.5))
