@@ -65,10 +65,10 @@ def test_dirichlet_boundary_is_exact_zero_outside(ks, oracle):
     assert np.abs(gpu - want).max() < 1e-6 * np.abs(want).max()
 
 
-@pytest.mark.parametrize("n", [5, 25])
+@pytest.mark.parametrize("n", [5, 25, 96, 129])
 def test_precond_matches_oracle(ks, oracle, n):
     """precond_init + 3 jacobi_step sweeps (shaders/eigen.wgsl:25-34, stencil.wgsl:94-106), at the reference's
-    smallest grid too."""
+    smallest grid, a middle one and the large grids of the configurations (96, and 129 past a tile edge)."""
     h, lam = 0.25, -0.6
     v = f32(oracle.nuclear_potential(n, h, [(0.0, 0.0, 0.0, 2)], 0.5))
     r = f32(smooth_field(oracle, n, h, 4))
