@@ -708,6 +708,15 @@ ks_status ks_autotune_stencil(int n, const int* counts, int ncount, int* chunks_
         if (counts[i] < 1 || counts[i] > 64) return fail(nullptr, KS_INVALID, "autotune_stencil: vector counts are 1..64");
         kmax = std::max(kmax, counts[i]);
     }
+    {
+        // the scratch (4 kmax + 1 fields) must fit the device's free memory with room to spare
+        const Layout L = Layout::make(n, 0.25);
+        const double need = (4.0 * kmax + 1.0) * (double)L.F * 4.0;
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && need > 0.8 * (double)free_b)
+            return fail(nullptr, KS_INVALID, "autotune_stencil: the scratch fields (" + std::to_string((long long)(need / 1e6)) +
+                                                 " MB) do not fit the device's free memory");
+    }
     return guarded(nullptr, [&] {
         const double h = 0.25;
         Scratch sc(n, h);
