@@ -482,8 +482,16 @@ class GpuSolver:
         _check(lib().ks_state_occupations(self._h, _p(up), _p(dn)), self._h)
         return up[:nu], dn[:nd]
 
-    def density(self):
-        up, dn = np.empty(self.n ** 3), np.empty(self.n ** 3)
+    def density(self, out=None):
+        """(rho_up, rho_dn), f64 n^3 each. out: two C-contiguous float64 arrays of n^3 to fill instead of new ones (e.g.
+        views of page-locked buffers, which the device writes at full copy speed)."""
+        if out is None:
+            up, dn = np.empty(self.n ** 3), np.empty(self.n ** 3)
+        else:
+            up, dn = out
+            for a in (up, dn):
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.size == self.n ** 3 and a.flags.c_contiguous):
+                    raise ValueError("density: out must be two C-contiguous float64 arrays of n^3 values")
         _check(lib().ks_state_density(self._h, _p(up), _p(dn)), self._h)
         return up, dn
 

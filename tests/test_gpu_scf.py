@@ -118,3 +118,21 @@ def test_h2o_95_matches_oracle_record(ks, gram_mode):
     assert np.abs(np.sort(ev_up)[:5] - np.array(H2O95["evals_up"])).max() < 1e-5
     assert np.abs(np.sort(ev_dn)[:5] - np.array(H2O95["evals_dn"])).max() < 1e-5
     assert np.abs(f - np.array(H2O95["forces"])).max() < 1e-4
+
+
+def test_density_into_caller_buffers(ks):
+    """GpuSolver.density(out=...) fills the caller's float64 arrays (here page-locked, as the bench's end-to-end
+    readback uses them) with the same bits as a fresh readback, and refuses arrays of the wrong size or type."""
+    import torch
+    n = 33
+    with ks.GpuSolver(n, 0.25) as so:
+        so.solve(ks.System([(0.7, 0.0, 0.0, 1), (-0.7, 0.0, 0.0, 1)], 1, 1), ks.ScfSettings(sigma=0.25, tol=1e-6))
+        up, dn = so.density()
+        out = tuple(torch.empty(n ** 3, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2))
+        got = so.density(out=out)
+        assert got[0] is out[0] and got[1] is out[1]
+        assert np.array_equal(out[0], up) and np.array_equal(out[1], dn)
+        with pytest.raises(ValueError):
+            so.density(out=(np.empty(n ** 3), np.empty(n ** 3 - 1)))
+        with pytest.raises(ValueError):
+            so.density(out=(np.empty(n ** 3, dtype=np.float32), np.empty(n ** 3)))
