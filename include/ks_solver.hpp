@@ -388,5 +388,23 @@ inline std::pair<bool, int> fd_witness_bound(const std::vector<double>& evals, c
     detail::check(ks_fd_witness_bound(evals.data(), residuals.data(), (int)evals.size(), n, mu, kt, &reached, &keep), nullptr);
     return {reached != 0, keep};
 }
+// witness_keep_within (occupations.rs:396-419): the levels to keep, or -1 when no level above the n-th passes both arms
+// on its lower bound at a residual within r_max (the block must grow).
+inline int fd_witness_keep_within(const std::vector<double>& evals, const std::vector<double>& residuals, int n, double mu, double kt,
+                                  double r_max, double tail_kt = 36.0) {
+    if (residuals.size() != evals.size()) throw InvalidArgument("fd_witness_keep_within: one residual per level");
+    int keep = 0;
+    detail::check(ks_fd_witness_keep_within(evals.data(), residuals.data(), (int)evals.size(), n, mu, kt, tail_kt, r_max, &keep), nullptr);
+    return keep;
+}
+// The stencil's launch-shape autotuner (ks_autotune_stencil): for each vector count, the z-chunk counts chosen for H psi
+// and for the Jacobi sweep on an n^3 grid of the current device (kept for later launches of those shapes).
+inline std::vector<std::pair<int, int>> autotune_stencil(int n, const std::vector<int>& counts) {
+    std::vector<int> out(2 * counts.size());
+    detail::check(ks_autotune_stencil(n, counts.data(), (int)counts.size(), out.data()), nullptr);
+    std::vector<std::pair<int, int>> r;
+    for (size_t i = 0; i < counts.size(); ++i) r.push_back({out[2 * i], out[2 * i + 1]});
+    return r;
+}
 
 }  // namespace qm_gpu

@@ -110,6 +110,10 @@ void check_occupations() {
     expect(wb.first && wb.second == 6, "fd_witness_bound: the witness's own residual pushes it up a rank");
     expect(throws<qm_gpu::InvalidArgument>([&] { qm_gpu::fd_witness_bound(evals, {0.0}, 1, -0.4, 5e-3); }),
            "fd_witness_bound: one residual per level");
+    expect(qm_gpu::fd_witness_keep_within(evals, {0.0, 0.0, 0.0, 2e-3, 1e-3, 3e-3, 3e-3}, 1, -0.4, 5e-3, 1.5e-3) == 6,
+           "fd_witness_keep_within: the lowest converged witness and its spare");
+    expect(qm_gpu::fd_witness_keep_within(evals, {0.0, 0.0, 0.0, 2e-3, 2e-3, 2e-3, 2e-3}, 1, -0.4, 5e-3, 1.5e-3) == -1,
+           "fd_witness_keep_within: none within r_max");
 }
 
 void check_arguments() {
