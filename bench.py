@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark: time for water on a 95^3 grid to converge (dRho < 1e-6), B200, through the C ABI.
 
-Workload (the north-star configuration): O at the origin, H at (+-1.43, 1.11, 0) Bohr (O-H 1.81 Bohr,
+Workload: O at the origin, H at (+-1.43, 1.11, 0) Bohr (O-H 1.81 Bohr,
 104.5 deg), cubic 95^3 grid at h = 0.25 Bohr, Gaussian nuclear smearing sigma = 0.5 Bohr, LSDA
 (Slater + PW92), 5 occupied + 3 extra bands per spin (LOBPCG block 8), orbitals initialised
 uniform(-1, 1) from a fixed seed, Aufbau occupations, DIIS history 6, alpha = 0.3, tol 1e-6 on

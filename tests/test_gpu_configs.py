@@ -1,4 +1,4 @@
-"""The north-star configurations beyond the timed H2O workload, through the C ABI on the B200:
+"""The workloads beyond the timed H2O one, through the C ABI on the B200:
 the adjoint (ks_vjp) against forces and central finite differences, NH3 96^3 forces / adjoint /
 20-step Born-Oppenheimer MD, n-butane 128^3 in both Gram forms, H2 48^3 against a full oracle
 SCF, and a concurrent batch of geometries against the same geometries solved one by one."""
