@@ -857,6 +857,12 @@ ks_status ks_fd_witness(const double* evals, int k, int n, double mu, double kt,
     return ks_fd_witness_bound(evals, nullptr, k, n, mu, kt, reached, keep);
 }
 
+ks_status ks_fd_step_tail_kt(int n_w, double delta_rho_prev, double* tail_kt) {
+    if (!tail_kt) return fail(nullptr, KS_INVALID, "invalid arguments");
+    *tail_kt = dense::fd_step_tail_kt(n_w, delta_rho_prev);
+    return KS_OK;
+}
+
 ks_status ks_fd_witness_keep_within(const double* evals, const double* residuals, int k, int n, double mu, double kt, double tail_kt,
                                     double r_max, int* keep) {
     if (k < 0 || n < 0 || (k > 0 && (!evals || !residuals)) || !keep || !std::isfinite(tail_kt))

@@ -373,13 +373,19 @@ static std::vector<int> ascending(const double* ev, int k) {
     return o;
 }
 
-bool fd_witness(const double* ev, const double* res, int k, int n, double mu, double kt) {
+double fd_step_tail_kt(int n_w, double delta_rho_prev) {
+    if (!(std::isfinite(delta_rho_prev) && delta_rho_prev > 0.0)) return 36.0;
+    const double x = std::log((double)std::max(n_w, 1) / (1e-3 * delta_rho_prev));
+    return std::min(std::max(x, 6.0), 36.0);
+}
+
+bool fd_witness(const double* ev, const double* res, int k, int n, double mu, double kt, double tail_kt) {
     if (n == 0) return true;
     if (k <= n) return false;
     const std::vector<int> o = ascending(ev, k);
     const int top = o[k - 1];
     const double lower = ev[top] - (res ? res[top] : 0.0);
-    return lower >= ev[o[n - 1]] + 0.1 && lower - mu >= 36.0 * kt;
+    return lower >= ev[o[n - 1]] + 0.1 && lower - mu >= tail_kt * kt;
 }
 
 int fd_witness_keep_within(const double* ev, const double* res, int k, int n, double mu, double kt, double tail_kt, double r_max) {
@@ -396,13 +402,13 @@ int fd_witness_keep_within(const double* ev, const double* res, int k, int n, do
     return -1;
 }
 
-int fd_witness_keep(const double* ev, const double* res, int k, int n, double mu, double kt) {
+int fd_witness_keep(const double* ev, const double* res, int k, int n, double mu, double kt, double tail_kt) {
     if (n == 0 || k <= n) return k;
     const std::vector<int> o = ascending(ev, k);
     const double eps_n = ev[o[n - 1]];
     auto passes = [&](int r) {
         const double lower = ev[o[r]] - (res ? res[o[r]] : 0.0);
-        return lower >= eps_n + 0.1 && lower - mu >= 36.0 * kt;
+        return lower >= eps_n + 0.1 && lower - mu >= tail_kt * kt;
     };
     for (int t = n; t < k; ++t)
         if (passes(t)) return (t + 1 < k && passes(t + 1)) ? t + 2 : t + 1;

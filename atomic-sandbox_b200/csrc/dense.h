@@ -40,11 +40,14 @@ bool fermi_dirac(const double* evals, int k, int n, double kt, double* f, double
 // The gap witness on the lower bounds theta_j - r_j of k levels (any order) with residual norms r (NULL: all zero):
 // the highest level's bound at least 0.1 Ha above the n-th lowest level and 36 kT above mu (occupations.rs:299-317
 // witness_bound_reached; with r = 0 it is witness_reached, :283-292). A NaN residual never passes.
-bool fd_witness(const double* evals, const double* res, int k, int n, double mu, double kt);
+bool fd_witness(const double* evals, const double* res, int k, int n, double mu, double kt, double tail_kt = 36.0);
 // After a passed witness, how many of the lowest levels to keep (occupations.rs:372-394 witness_keep, on the same lower
 // bounds): t + 1 for the lowest rank t >= n whose bound passes both arms, t + 2 when the rank above passes too; k when
 // none does or n = 0.
-int fd_witness_keep(const double* evals, const double* res, int k, int n, double mu, double kt);
+int fd_witness_keep(const double* evals, const double* res, int k, int n, double mu, double kt, double tail_kt = 36.0);
+// The witness tail of a loosened SCF step (occupations.rs:319-326 step_tail_kt): ln(n_w / (1e-3 delta_rho_prev)) kT
+// clamped to [6, 36], n_w the block's levels; 36 for a non-finite or non-positive delta_rho_prev.
+double fd_step_tail_kt(int n_w, double delta_rho_prev);
 // The lowest converged witness (occupations.rs:396-419 witness_keep_within, the tail arm at tail_kt kT): the lowest rank
 // t >= n whose lower bound passes both arms with its residual at most r_max decides, keeping t + 1 levels (t + 2 when
 // rank t + 1 passes on its lower bound too); -1 when no such level exists (the block must grow); k for n = 0. A NaN

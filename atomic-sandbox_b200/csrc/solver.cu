@@ -1414,7 +1414,10 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                     const double* ev = ch_[sp].evals.data();
                     const double* rv = ch_[sp].res.data();
                     int grown;
-                    if (dense::fd_witness(ev, rv, kk[sp], nocc[sp], m_sp, s.kt)) {
+                    // the witness tail: 36 kT, or on a loosened step the step-accuracy tail (occupations.rs:319-326;
+                    // crates/qm-gpu/src/scf.rs:909, n_w the block's levels, the previous step's delta rho)
+                    const double tail_kt = step_tol > eig_lo ? dense::fd_step_tail_kt(kk[sp], delta_rho) : 36.0;
+                    if (dense::fd_witness(ev, rv, kk[sp], nocc[sp], m_sp, s.kt, tail_kt)) {
                         int top = 0;
                         for (int i = 1; i < kk[sp]; ++i)
                             if (ev[i] > ev[top]) top = i;
@@ -1423,7 +1426,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                         if (step_tol <= eig_lo && !(rv[top] <= r_witness) && extras < cap)
                             keep = dense::fd_witness_keep_within(ev, rv, kk[sp], nocc[sp], m_sp, s.kt, 36.0, r_witness);
                         else
-                            keep = dense::fd_witness_keep(ev, rv, kk[sp], nocc[sp], m_sp, s.kt);
+                            keep = dense::fd_witness_keep(ev, rv, kk[sp], nocc[sp], m_sp, s.kt, tail_kt);
                         if (keep >= 0) {
                             keep = std::max(base, keep);
                             if (keep < kk[sp]) {

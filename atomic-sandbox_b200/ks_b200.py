@@ -201,7 +201,7 @@ EXPORTED = [
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
     "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
-    "ks_fd_witness", "ks_fd_witness_bound", "ks_fd_witness_keep_within", "ks_density_residual", "ks_diis_mix", "ks_autotune_stencil",
+    "ks_fd_witness", "ks_fd_witness_bound", "ks_fd_witness_keep_within", "ks_fd_step_tail_kt", "ks_density_residual", "ks_diis_mix", "ks_autotune_stencil",
     "ks_stencil_tuning_get", "ks_stencil_tuning_set", "ks_stencil_tuning_clear", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
     "ks_test_poison_parked_density", "ks_test_fail_readbacks",
 ]
@@ -262,6 +262,7 @@ def lib():
         L.ks_fermi_dirac.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
         L.ks_fd_witness.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
         L.ks_fd_witness_bound.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
+        L.ks_fd_step_tail_kt.argtypes = [ctypes.c_int, ctypes.c_double, dp]
         L.ks_fd_witness_keep_within.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_double, ip]
         L.ks_field_pitch.argtypes = [ctypes.c_int]
@@ -856,6 +857,13 @@ def diis_mix(n, rho, r, c, a):
     out = np.empty(n3)
     _check(lib().ks_diis_mix(n, m, _p(rho), _p(r), _p(ca) if m > 1 else None, _p(aa), _p(out)))
     return out
+
+
+def fd_step_tail_kt(n_w, delta_rho_prev):
+    """The witness tail (in kT) of a loosened SCF step (crates/qm/src/occupations.rs step_tail_kt)."""
+    out = ctypes.c_double()
+    _check(lib().ks_fd_step_tail_kt(int(n_w), float(delta_rho_prev), ctypes.byref(out)))
+    return out.value
 
 
 def fd_witness_keep_within(evals, residuals, n, mu, kt, r_max, tail_kt=36.0):

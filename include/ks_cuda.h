@@ -356,6 +356,10 @@ ks_status ks_fd_witness(const double* evals, int k, int n, double mu, double kt,
    keep = witness_keep (:372-394). residuals may be NULL (all zero: ks_fd_witness); a NaN residual never passes. */
 ks_status ks_fd_witness_bound(const double* evals, const double* residuals, int k, int n, double mu, double kt, int* reached,
                               int* keep);
+/* The witness tail of a loosened SCF step (crates/qm/src/occupations.rs:319-326 step_tail_kt), in kT:
+   ln(n_w / (1e-3 delta_rho_prev)) clamped to [6, 36], n_w the block's levels; 36 for a non-finite or non-positive
+   delta_rho_prev. The solver reads the witness with this tail on a step whose eigen tolerance is loosened. */
+ks_status ks_fd_step_tail_kt(int n_w, double delta_rho_prev, double* tail_kt);
 /* The lowest converged witness (crates/qm/src/occupations.rs:396-419 witness_keep_within): the lowest level above the
    n-th whose lower bound theta - r passes both arms (the tail arm at tail_kt kT) with r <= r_max decides, and keep gets
    the levels to keep (its rank + 1, + 2 with a passing spare above it); keep = -1 when no level qualifies (the block must

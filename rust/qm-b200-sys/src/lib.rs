@@ -92,6 +92,7 @@ extern "C" {
                           entropy: *mut c_double) -> c_int;
     pub fn ks_fd_witness(evals: *const c_double, k: c_int, n: c_int, mu: c_double, kt: c_double, reached: *mut c_int,
                          keep: *mut c_int) -> c_int;
+    pub fn ks_fd_step_tail_kt(n_w: c_int, delta_rho_prev: c_double, tail_kt: *mut c_double) -> c_int;
     pub fn ks_fd_witness_keep_within(evals: *const c_double, residuals: *const c_double, k: c_int, n: c_int, mu: c_double,
                                      kt: c_double, tail_kt: c_double, r_max: c_double, keep: *mut c_int) -> c_int;
     pub fn ks_fd_witness_bound(evals: *const c_double, residuals: *const c_double, k: c_int, n: c_int, mu: c_double,

@@ -3,6 +3,7 @@ known answers: the Rayleigh-Ritz step on the 23 x 23 problem dumped from a faili
 (tests/golden/rr_i1_{a,b}.txt; crates/qm-gpu/src/eigen.rs:1188-1201 rayleigh_ritz_pairs_survive_a_bad_symmetric_eigen),
 and the Fermi-Dirac occupation rule (crates/qm/src/occupations.rs:474-612), which must also agree with the oracle's
 restatement. CPU only."""
+import math
 import os
 
 import numpy as np
@@ -154,3 +155,16 @@ def test_witness_keep_within_reads_the_lowest_converged_witness(ks):
     e2, r2 = [0.0, -0.5, 0.3, -0.1, -0.3, -0.05, -0.25], [0.0, 0.0, 3e-3, 2e-3, 0.0, 1e-3, 0.0]
     assert kw(e2, r2, 1, mu, kt, r_max) == 6                                # order-independent
     assert kw(evals, [0.0, 0.0, 0.0, float("nan"), 0.0, 0.0, 0.0], 1, mu, kt, r_max) == 6  # a NaN residual never qualifies
+
+
+def test_step_tail_follows_the_step_accuracy(ks):
+    """The reference's test of the loosened step's witness tail (crates/qm/src/occupations.rs:773-786
+    step_tail_follows_the_step_accuracy): ln(n_w / (1e-3 drho)) kT clamped to [6, 36]."""
+    assert abs(ks.fd_step_tail_kt(10, 1e-2) - math.log(1e6)) < 1e-12
+    assert abs(ks.fd_step_tail_kt(10, 10.0) - math.log(1e3)) < 1e-12
+    assert ks.fd_step_tail_kt(10, 100.0) == 6.0
+    assert ks.fd_step_tail_kt(10, 1e-15) == 36.0
+    for d in (float("inf"), float("nan"), 0.0, -1.0):
+        assert ks.fd_step_tail_kt(7, d) == 36.0
+    xs = [ks.fd_step_tail_kt(8, 10 ** (2.0 - e / 4.0)) for e in range(60)]
+    assert all(b >= a for a, b in zip(xs, xs[1:])) and xs[0] == 6.0 and xs[-1] == 36.0
