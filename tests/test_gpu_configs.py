@@ -124,22 +124,31 @@ def test_nh3_96_matches_oracle_record(ks, drv):
     assert np.abs(f - np.array(rec["forces"])).max() < 1e-4, np.abs(f - np.array(rec["forces"])).max()
 
 
-def test_butane_128_mixed_matches_plain(ks, drv):
+def test_butane_128_mixed_matches_plain_and_oracle_record(ks, drv):
     """n-butane (anti, seeded 0.02 Bohr jitter) on 128^3 at h = 0.2: LOBPCG blocks of 20 bands per spin
     (17 occupied in the all-electron model + 3 extra), the tensor-core Gram (m = 60) against the
-    CUDA-core form: |dE| < 1e-5 Ha, occupied eigenvalues within 1e-5 Ha, 34 electrons. The density
-    tolerance is 2e-6: the f32 storage floor of the mixed density is ~3e-8 N = 1.0e-6 for N = 34
-    (crates/qm-gpu/src/scf.rs module doc, "The mixing step"), so tol 1e-6 sits on it."""
+    CUDA-core form, and the mixed form against a full f64 oracle SCF of the same geometry
+    (tests/golden/oracle_butane_128.json, tests/golden/make_oracle_configs.py butane, 4 hours on 4 host threads):
+    |dE| < 1e-5 Ha, occupied eigenvalues within 1e-5 Ha and forces within 1e-4 Ha/Bohr (the bars of
+    crates/validate/tests/gpu_vs_cpu.rs:152-160), 34 electrons. The density tolerance is 2e-6: the f32 storage floor of
+    the mixed density is ~3e-8 N = 1.0e-6 for N = 34 (crates/qm-gpu/src/scf.rs module doc, "The mixing step"), so tol
+    1e-6 sits on it (the oracle, in f64, stops at 1e-6)."""
+    rec = json.load(open(os.path.join(GOLDEN, "oracle_butane_128.json")))
     nuc = drv.butane_anti(jitter=0.02, seed=0x5EED + 2)
+    assert np.allclose(np.array(nuc), np.array(rec["nuclei"]), atol=0, rtol=0)
     out = {}
     for gm in (0, 1):
         with ks.GpuSolver(128, 0.2, gram_mode=gm, n_extra=3, init_mode=1) as so:
             st = so.solve(ks.System(nuc, 17, 17), ks.ScfSettings(sigma=0.5, tol=2e-6))
-            out[gm] = (st, so.evals())
-    (s0, (u0, d0)), (s1, (u1, d1)) = out[0], out[1]
+            out[gm] = (st, so.evals(), so.forces(nuc, 0.5))
+    (s0, (u0, d0), _), (s1, (u1, d1), f1) = out[0], out[1]
     assert abs(s0["energy"]["total"] - s1["energy"]["total"]) < 1e-5, (s0["energy"], s1["energy"])
     assert np.abs(u0 - u1).max() < 1e-5 and np.abs(d0 - d1).max() < 1e-5
     assert abs(sum(s1["electrons"]) - 34) < 1e-4
+    assert abs(s1["energy"]["total"] - rec["stats"]["total"]) < 1e-5, (s1["energy"]["total"], rec["stats"]["total"])
+    eu, ed = np.array(rec["evals_up"]), np.array(rec["evals_dn"])
+    assert np.abs(u1[:17] - eu[:17]).max() < 1e-5 and np.abs(d1[:17] - ed[:17]).max() < 1e-5, (u1[:17] - eu[:17], d1[:17] - ed[:17])
+    assert np.abs(f1 - np.array(rec["forces"])).max() < 1e-4, np.abs(f1 - np.array(rec["forces"])).max()
 
 
 def test_h2_48_matches_oracle_record(ks):
