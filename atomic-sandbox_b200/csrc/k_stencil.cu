@@ -17,7 +17,8 @@
 // reads its centre, x- and y-neighbours as 16-byte quads (11 shared loads per 4 outputs), keeps the nine z-values of
 // its quad in a register queue that moves up one plane per step, and computes the two packed pairs of the quad with
 // Blackwell's f32x2 arithmetic. A neighbour pair that straddles two quads (odd x offsets) is differenced with two
-// scalar subtractions instead of being repacked. The V / R reads and the stores are coalesced 16-byte accesses;
+// scalar subtractions instead of being repacked. The V / R reads (cp.async copies one plane ahead into a small shared
+// ring) and the stores are coalesced 16-byte accesses;
 // the quad's pad columns are stored as 0. Measured against the 2 x 2-outputs-per-thread form it replaces: the same
 // outputs bit for bit at h = 0.25, and H psi on 95^3 at 8 / 16 / 64 vectors 13 / 13 / 21 % faster.
 #include <algorithm>
@@ -54,6 +55,20 @@ static_assert(THREADS == (BX / 4) * BY, "one thread per x-quad of a row");
 // resident CTAs per SM: registers capped at 96 per thread (no spills) for 20 warps per SM; 4 and 6 CTAs per SM
 // measured slower (H psi on 95^3: 4 CTAs 182 us at 64 vectors, 6 CTAs 144 us, against 137 us at 5)
 constexpr int CTAS_PER_SM = 5;
+// The per-plane global reads of a step (V; r and the stored factor in the Jacobi mode) are staged one plane ahead by
+// per-thread cp.async copies into a 2-deep shared "side" ring (12 KB per CTA in the Jacobi mode, 4 KB for H and the
+// residual form), so their latency runs behind the previous plane's arithmetic without holding registers. Against
+// register loads at the step that uses them: the H2O 95^3 solve 176.5 -> 172.3 ms, Jacobi sweep 34.0 -> 33.0 us,
+// bitwise-identical results. Three planes ahead, or V left to the L2 in the Jacobi mode, measured slower.
+constexpr int SD = 2;
+template <int MODE>
+constexpr int n_side() { return MODE == ST_JACOBI ? 3 : (MODE == ST_LAPLACIAN ? 0 : 1); }
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 constexpr long long WAIT_LIMIT = 1LL << 22;         // bounded mbarrier waits (~seconds)
 constexpr long long DRAIN_LIMIT = 1LL << 16;        // waits for copies in flight after a wait gave up
 
@@ -134,7 +149,6 @@ __device__ __forceinline__ u64 pk(float lo, float hi) {
 __device__ __forceinline__ float lo_of(u64 v) { return __uint_as_float((unsigned)v); }
 __device__ __forceinline__ float hi_of(u64 v) { return __uint_as_float((unsigned)(v >> 32)); }
 __device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
-__device__ __forceinline__ float4 ldg4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 // (a0 - f0.lo, a1 - f0.hi)
 __device__ __forceinline__ u64 dif(float a0, float a1, u64 f0) { return sub2(pk(a0, a1), f0); }
 
@@ -262,6 +276,26 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
     float* orow = out + vbase + row0;
     float* orow2 = (MODE == ST_HAM_RESIDUAL) ? p.out2 + vbase + row0 : nullptr;
     float* drow = p.dinv ? p.dinv + vbase + row0 : nullptr;
+    // the side ring, [SD][NSIDE][THREADS] float4 after the plane ring: slot t % SD holds this thread's V (r, factor)
+    // quads of output plane t. Each thread reads only its own copies, after its own wait_group, and refills a slot
+    // only after the step that read it has consumed the values.
+    constexpr int NSIDE = n_side<MODE>();
+    float4* side = reinterpret_cast<float4*>(ring + NS * PLANE_FLOATS);
+    auto side_issue = [&](int t) {
+        if (NSIDE > 0) {
+            if (ok && t < nz) {
+                float4* dst = side + (t % SD) * NSIDE * THREADS + threadIdx.x;
+                cp_async16(dst, vrow + t * plane);
+                if (MODE == ST_JACOBI) {
+                    cp_async16(dst + THREADS, rrow + t * plane);
+                    if (drow) cp_async16(dst + 2 * THREADS, drow + t * plane);
+                }
+            }
+            cp_async_commit();  // one group per plane, empty or not, so that wait_group counts planes
+        }
+    };
+#pragma unroll
+    for (int t = 0; t < SD - 1; ++t) side_issue(t);
     double dot = 0.0;
     // the compact loop body (not unrolled): unrolled bodies measured slower (the instruction cache)
 #pragma unroll 1
@@ -270,11 +304,17 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) stencil_kernel(const __g
         alive = mbar_wait(&bar[qn % NS], (unsigned)((qn / NS) & 1), p.err, alive ? WAIT_LIMIT : 1) && alive;
         q[8] = lds4(ring + (qn % NS) * PLANE_FLOATS + ci);
         const float* cpl = ring + ((s + 4) % NS) * PLANE_FLOATS + ci;
-        // the global reads are issued before the stencil arithmetic, which hides their latency
+        // the next plane's side copies go out before this plane's are read
         const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 v = (MODE != ST_LAPLACIAN && ok) ? ldg4(vrow + s * plane) : zero4;
-        const float4 r = (MODE == ST_JACOBI && ok) ? ldg4(rrow + s * plane) : zero4;
-        const float4 dq = (MODE == ST_JACOBI && ok && drow) ? ldg4(drow + s * plane) : zero4;
+        float4 v = zero4, r = zero4, dq = zero4;
+        if (NSIDE > 0) {
+            side_issue(s + SD - 1);
+            cp_async_wait<SD - 1>();
+            const float4* sl = side + (s % SD) * NSIDE * THREADS + threadIdx.x;
+            if (ok) v = sl[0];
+            if (MODE == ST_JACOBI && ok) r = sl[THREADS];
+            if (MODE == ST_JACOBI && ok && drow) dq = sl[2 * THREADS];
+        }
         u64 o0, o1;
         lap_quad(cpl, q, kc, o0, o1);
         if (!FOLD_SCALE) {
@@ -431,7 +471,7 @@ int current_device() {
 
 template <int MODE, bool DOT>
 void launch_mode(const Shape& sh, int count, const CUtensorMap& tmap, const Params& p, float* out, cudaStream_t s) {
-    const int smem = NS * PLANE_BYTES;
+    const int smem = NS * PLANE_BYTES + SD * n_side<MODE>() * THREADS * 16;
     static std::atomic<unsigned long long> attr_set{0};
     once_per_device(attr_set, [smem] {
         KS_CUDA(cudaFuncSetAttribute(stencil_kernel<MODE, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
