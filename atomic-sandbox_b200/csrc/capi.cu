@@ -903,6 +903,47 @@ ks_status ks_lobpcg(int n, double h, const double* v, int k, double* x, double* 
     });
 }
 
+ks_status ks_lobpcg_guarded(int n, double h, const double* v, int k, double* x, double* evals, double tol, double guess_tol,
+                            int head, double tail_tol, int checked, int max_iter, int lock, int gram_mode, double* residuals,
+                            ks_eigen_stats* stats) {
+    if (!valid_grid(n, h) || !v || k < 1 || !x || !evals || gram_mode < 0 || gram_mode > 1 || checked < 1 || checked > k || head < 0 ||
+        head > checked || !(tol > 0) || !(guess_tol >= tol) || !(tail_tol >= tol) || max_iter < 0)
+        return fail(nullptr, KS_INVALID, "invalid arguments");
+    return guarded(nullptr, [&] {
+        SolverOptions o;
+        o.gram_mode = gram_mode;
+        Solver so(n, h, o);
+        const Layout& L = so.layout();
+        Scratch sc(n, h);
+        Channel ch;
+        ch.create(L, k);
+        Block vv;
+        vv.create(L, 1);
+        sc.upload_fields(v, 1, vv);
+        sc.upload_fields(x, k, ch.A[0]);
+        EigenStats es = so.lobpcg(ch, so.lane(0), vv.at(0), tol, guess_tol, max_iter, head, tail_tol, checked, lock != 0);
+        KS_CUDA(cudaStreamSynchronize(so.lane(0).s));
+        sc.download_fields(ch.X(), k, x);
+        for (int i = 0; i < k; ++i) evals[i] = ch.evals[i];
+        if (residuals)
+            for (int i = 0; i < k; ++i) residuals[i] = ch.res[i];
+        if (stats) {
+            stats->iterations = es.iterations;
+            stats->stop = es.stop;
+            stats->head_kept = es.head_kept ? 1 : 0;
+            stats->locked = es.locked;
+            stats->restores = es.restores;
+            stats->fallbacks = es.fallbacks;
+            stats->readbacks = es.readbacks;
+            stats->max_residual = es.max_residual;
+            stats->head_residual = es.head_res;
+            stats->tail_residual = es.tail_res;
+            stats->alpha_worst = es.alpha_worst;
+        }
+        return KS_OK;
+    });
+}
+
 int ks_field_pitch(int n) { return Layout::make(n, 1.0).P; }
 
 long long ks_launch_count(void) { return ks::launch_count(); }

@@ -253,6 +253,52 @@ double rayleigh_ritz(int m, const std::vector<double>& A, const std::vector<doub
     return alpha;
 }
 
+double rayleigh_ritz_locked(int m, const std::vector<double>& A, const std::vector<double>& B, int locked, int na,
+                            std::vector<double>& theta, std::vector<double>& C) {
+    if (locked == 0) return rayleigh_ritz(m, A, B, na, theta, C);
+    const int L = locked, mz = m - L;
+    dense::Mat byy((size_t)L * L);
+    for (int i = 0; i < L; ++i)
+        for (int j = 0; j < L; ++j) byy[(size_t)i * L + j] = B[(size_t)i * m + j];
+    if (!dense::cholesky(L, byy)) throw NumericalError("lobpcg: Cholesky of the locked columns' Gram failed");
+    std::vector<double> kk((size_t)L * mz);  // B_YY^-1 B_YZ, L x mz row-major
+    for (int i = 0; i < L; ++i)
+        for (int j = 0; j < mz; ++j) kk[(size_t)i * mz + j] = B[(size_t)i * m + L + j];
+    dense::cholesky_solve(L, byy, mz, kk);
+    // Q = [-B_YY^-1 B_YZ; I], m x mz: Q^T M Q = M_ZZ - K^T M_YZ - M_ZY K + K^T M_YY K
+    auto congruence = [&](const std::vector<double>& M) {
+        std::vector<double> MQ((size_t)m * mz);  // M Q, m x mz row-major
+        for (int i = 0; i < m; ++i)
+            for (int c = 0; c < mz; ++c) {
+                double s = M[(size_t)i * m + L + c];
+                for (int j = 0; j < L; ++j) s -= M[(size_t)i * m + j] * kk[(size_t)j * mz + c];
+                MQ[(size_t)i * mz + c] = s;
+            }
+        std::vector<double> R((size_t)mz * mz);
+        for (int a = 0; a < mz; ++a)
+            for (int b = 0; b < mz; ++b) {
+                double s = MQ[(size_t)(L + a) * mz + b];
+                for (int i = 0; i < L; ++i) s -= kk[(size_t)i * mz + a] * MQ[(size_t)i * mz + b];
+                R[(size_t)a * mz + b] = s;
+            }
+        for (int a = 0; a < mz; ++a)
+            for (int b = a + 1; b < mz; ++b) R[(size_t)a * mz + b] = R[(size_t)b * mz + a] = 0.5 * (R[(size_t)a * mz + b] + R[(size_t)b * mz + a]);
+        return R;
+    };
+    std::vector<double> Cp;
+    const double alpha = rayleigh_ritz(mz, congruence(A), congruence(B), na, theta, Cp);
+    C.assign((size_t)m * na, 0.0);  // Q C', column-major m x na
+    for (int c = 0; c < na; ++c) {
+        for (int i = 0; i < L; ++i) {
+            double s = 0.0;
+            for (int j = 0; j < mz; ++j) s -= kk[(size_t)i * mz + j] * Cp[j + (size_t)mz * c];
+            C[i + (size_t)m * c] = s;
+        }
+        for (int j = 0; j < mz; ++j) C[L + j + (size_t)m * c] = Cp[j + (size_t)mz * c];
+    }
+    return alpha;
+}
+
 // ------------------------------------------------------------------ kernel timing
 KernelTimer::~KernelTimer() {
     for (auto& r : pending_) {
@@ -838,10 +884,16 @@ void Solver::gram_checked(Reducer& red, int m, const float* S, int mt, const flo
     red.gram(m, S, mt, T, 0, L_.h * L_.h * L_.h, extra);  // the L2 product <a, b> = h^3 sum a b
 }
 
-EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked, double tail_tol) {
+EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int head,
+                          double tail_tol, int checked, bool lock) {
     NvtxRange range("ks lobpcg");
     EigenStats es;
     const int k = ch.k;
+    if (checked < 0) checked = std::isfinite(tail_tol) ? k : head;
+    checked = std::max(1, std::min(checked, k));
+    head = std::max(0, std::min(head, checked));
+    const bool split = std::isfinite(tail_tol);  // else the columns past the head are untested (checked == head)
+    int locked = 0;  // the locked head (crates/qm-gpu/src/eigen.rs:742); W and P exist for the other columns only
     // LOBPCG_TRACE in the environment, set to any value, prints the reference's per-iteration lines to stderr
     // (crates/qm-gpu/src/eigen.rs:707, :800, :853, :941); the two spin channels' lines carry their spin
     static const bool trace = std::getenv("LOBPCG_TRACE") != nullptr;
@@ -943,26 +995,28 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
             norm_blocks = nb;
         }
         fused_r = false;
-        const int m = 2 * k + np;
+        // the active columns [locked, k): under a lock W and P exist for them only, W_a at [k, k + na) and P_a after it
+        const int na = k - locked;
+        const int m = k + na + np;
         const int off_norm = m * 2 * m;
         StencilArgs jac;
         jac.mode = ST_JACOBI;
         jac.scale = ham_scale;
         jac.V = V;
-        jac.R = ch.T.at(0);
-        jac.lambda = lambda_d;
+        jac.R = ch.T.at(locked);
+        jac.lambda = lambda_d + locked;
         jac.omega = (float)omega;
         jac.diag_t = (float)diag_t;
-        jac.dinv = ch.HX.at(0);  // the sweep factors of this iteration (H X itself is not needed past the residual)
-        jac.vec0 = 0;
-        const double jac_bytes = (16.0 * k + 4.0) * npts;  // w, r and the stored factor in, w' out, V once
-        timer_.time(KS_K_JACOBI, k, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), lane.s); });   // Q -> W
+        jac.dinv = ch.HX.at(locked);  // the sweep factors of this iteration (H X itself is not needed past the residual)
+        jac.vec0 = locked;
+        const double jac_bytes = (16.0 * na + 4.0) * npts;  // w, r and the stored factor in, w' out, V once
+        timer_.time(KS_K_JACOBI, na, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, ch.Q.tmap, na, jac, S.at(k), lane.s); });   // Q -> W
         jac.vec0 = k;
-        timer_.time(KS_K_JACOBI, k, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, S.tmap, k, jac, ch.Q.at(0), lane.s); });   // W -> Q
-        jac.vec0 = 0;
-        timer_.time(KS_K_JACOBI, k, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, ch.Q.tmap, k, jac, S.at(k), lane.s); });   // Q -> W
+        timer_.time(KS_K_JACOBI, na, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, S.tmap, na, jac, ch.Q.at(locked), lane.s); });   // W -> Q
+        jac.vec0 = locked;
+        timer_.time(KS_K_JACOBI, na, 0, jac_bytes, lane.s, [&] { launch_stencil(L_, ch.Q.tmap, na, jac, S.at(k), lane.s); });   // Q -> W
         // 2. HW and HP in one launch (W and P are contiguous after X)
-        apply_h(S, k, k + np, ch.T.at(k));
+        apply_h(S, k, na + np, ch.T.at(k));
         // 3. the readback: G = S^T [S | T] and |r_i|^2
         FinishDesc norms;
         norms.partials = norm_partials;
@@ -986,15 +1040,22 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
             if (!std::isfinite(x)) throw NumericalError("lobpcg: non-finite Gram entry (NaN in a vector or in V)");
         for (double x : B)
             if (!std::isfinite(x)) throw NumericalError("lobpcg: non-finite Gram entry (NaN in a vector or in V)");
-        double max_res = 0.0, stop_res = 0.0;
+        // the split stop test (crates/qm-gpu/src/eigen.rs:768-787): the head at tol, [head, checked) scaled by
+        // tol / tail_tol, the rest untested; lock_res the same over the tail alone (a lock holds exactly the head)
+        double max_res = 0.0, stop_res = 0.0, lock_res = 0.0, head_res = 0.0, tail_res = 0.0;
         for (int i = 0; i < k; ++i) {
             double xx = B[(size_t)i * m + i];
             lambda[i] = A[(size_t)i * m + i] / xx;
             res[i] = std::sqrt(g[off_norm + i] / xx);
             if (!std::isfinite(res[i]) || !std::isfinite(lambda[i])) throw NumericalError("lobpcg: non-finite residual");
             max_res = std::max(max_res, res[i]);
-            if (i < checked) stop_res = std::max(stop_res, res[i]);
-            else if (std::isfinite(tail_tol)) stop_res = std::max(stop_res, res[i] * (tol / tail_tol));
+            if (i < head) head_res = std::max(head_res, res[i]);
+            else if (i < checked) tail_res = std::max(tail_res, res[i]);
+            if (i < checked) {
+                const double scaled = i < head ? res[i] : res[i] * (tol / tail_tol);
+                stop_res = std::max(stop_res, scaled);
+                if (i >= head) lock_res = std::max(lock_res, scaled);
+            }
         }
         ch.evals = lambda;
         ch.res = res;
@@ -1003,7 +1064,7 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         if (have_prev) {
             have_prev = false;
             double rise = 0.0, slack = 0.0;
-            for (int i = 0; i < k; ++i) {
+            for (int i = locked; i < k; ++i) {  // the moved columns
                 rise += lambda[i] - theta[i];
                 slack += RITZ_FORM_SLACK * (1.0 + std::fabs(theta[i])) + RITZ_FORM_RES * res[i];
             }
@@ -1016,13 +1077,22 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
                 ++es.restores;
                 ch.cur ^= 1;
                 theta = prev_theta;
-                lambda = theta;
+                for (int i = locked; i < k; ++i) lambda[i] = theta[i];
                 np = 0;
                 upload(theta, lambda, nullptr);
                 apply_h(ch.A[ch.cur], 0, k, ch.HX.at(0));
                 continue;
             }
         }
+        // the lock (crates/qm-gpu/src/eigen.rs:814-818): at the guess, a head under guess_tol whose tail is not. Y stays
+        // where it is in both X buffers (copied into the other once here); the block update writes the other columns.
+        if (lock && iterations == 0 && locked == 0 && head > 0 && head < checked && head_res < guess_tol && !(stop_res < guess_tol) &&
+            std::isfinite(stop_res)) {
+            locked = head;
+            KS_CUDA(cudaMemcpyAsync(ch.A[ch.cur ^ 1].at(0), ch.A[ch.cur].at(0), (size_t)locked * L_.F * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, lane.s));
+        }
+        if (locked > 0) stop_res = lock_res;  // the stop test reads the active columns
         if (stop_res < 0.5 * best) { best = stop_res; best_it = iterations; }
         // stop decision (crates/qm-gpu/src/eigen.rs:322-329)
         int stop = -1;
@@ -1033,6 +1103,10 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
             es.iterations = iterations;
             es.max_residual = max_res;
             es.stop = stop;
+            es.head_res = head_res;
+            es.tail_res = split ? tail_res : 0.0;
+            es.head_kept = iterations == 0 || locked > 0;
+            es.locked = locked;
             if (trace) {
                 std::fprintf(stderr, "lobpcg%s exit: iterations %d, max residual %.3e, stop %d, restores %d, fallbacks %d, evals", tag,
                              iterations, max_res, stop, es.restores, es.fallbacks);
@@ -1044,50 +1118,58 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
         ++iterations;
         auto t_dense = clk::now();
         // 4. Rayleigh-Ritz with the conditioning guard; fallback: drop P and redo on [X, W]
+        // (under a lock: the subspace B-orthogonal to Y, the na = k - locked active columns' pairs)
+        const int na_rr = k - locked;
         std::vector<double> th, C;
-        double alpha = rayleigh_ritz(m, A, B, k, th, C);
+        double alpha = rayleigh_ritz_locked(m, A, B, locked, na_rr, th, C);
         es.alpha_worst = std::max(es.alpha_worst, alpha);
-        if (trace) std::fprintf(stderr, "lobpcg%s it %d: max_res %.2e alpha %.2f m %d\n", tag, iterations, max_res, alpha, m);
-        if (!(alpha <= std::max(ALPHA_MAX, ALPHA_RESIDUAL_FRACTION * stop_res / floor_)) && np > 0) {
+        if (trace) std::fprintf(stderr, "lobpcg%s it %d: max_res %.2e alpha %.2f m %d locked %d\n", tag, iterations, max_res, alpha, m, locked);
+        // the noise budget: the tested columns' split residual, or under a lock the active tail's own (unscaled) one
+        // (crates/qm-gpu/src/eigen.rs:861-867)
+        const double budget_res = locked > 0 ? tail_res : stop_res;
+        if (!(alpha <= std::max(ALPHA_MAX, ALPHA_RESIDUAL_FRACTION * budget_res / floor_)) && np > 0) {
             ++es.fallbacks;
-            const int m2 = 2 * k;
+            const int m2 = k + na_rr;  // [X, W_a]
             std::vector<double> A2((size_t)m2 * m2), B2((size_t)m2 * m2);
             for (int i = 0; i < m2; ++i)
                 for (int j = 0; j < m2; ++j) { A2[(size_t)i * m2 + j] = A[(size_t)i * m + j]; B2[(size_t)i * m2 + j] = B[(size_t)i * m + j]; }
             std::vector<double> C2;
-            rayleigh_ritz(m2, A2, B2, k, th, C2);
-            C.assign((size_t)m * k, 0.0);
-            for (int c = 0; c < k; ++c)
+            rayleigh_ritz_locked(m2, A2, B2, locked, na_rr, th, C2);
+            C.assign((size_t)m * na_rr, 0.0);
+            for (int c = 0; c < na_rr; ++c)
                 for (int i = 0; i < m2; ++i) C[i + (size_t)m * c] = C2[i + (size_t)m2 * c];
         }
-        // 5. X_new = S C, P_new = X_new - X (X^T X)^-1 X^T X_new = S C_p
-        std::vector<double> bxx((size_t)k * k), rhs((size_t)k * k, 0.0);
+        // 5. X_new = S C, P_new = X_new - X (X^T X)^-1 X^T X_new = S C_p (X all k columns, Y included)
+        std::vector<double> bxx((size_t)k * k), rhs((size_t)k * na_rr, 0.0);
         for (int i = 0; i < k; ++i)
             for (int j = 0; j < k; ++j) bxx[(size_t)i * k + j] = B[(size_t)i * m + j];
         if (!dense::cholesky(k, bxx)) throw NumericalError("lobpcg: Cholesky of X^T X failed (X lost rank)");
         for (int i = 0; i < k; ++i)
-            for (int c = 0; c < k; ++c) {
+            for (int c = 0; c < na_rr; ++c) {
                 double s = 0.0;
                 for (int j = 0; j < m; ++j) s += B[(size_t)i * m + j] * C[j + (size_t)m * c];
-                rhs[(size_t)i * k + c] = s;
+                rhs[(size_t)i * na_rr + c] = s;
             }
-        dense::cholesky_solve(k, bxx, k, rhs);
-        std::vector<double> coef((size_t)m * 2 * k);
-        for (int c = 0; c < k; ++c)
+        dense::cholesky_solve(k, bxx, na_rr, rhs);
+        std::vector<double> coef((size_t)m * 2 * na_rr);
+        for (int c = 0; c < na_rr; ++c)
             for (int i = 0; i < m; ++i) {
                 coef[i + (size_t)m * c] = C[i + (size_t)m * c];
-                coef[i + (size_t)m * (k + c)] = C[i + (size_t)m * c] - (i < k ? rhs[(size_t)i * k + c] : 0.0);
+                coef[i + (size_t)m * (na_rr + c)] = C[i + (size_t)m * c] - (i < k ? rhs[(size_t)i * na_rr + c] : 0.0);
             }
         prev_theta = theta;
         have_prev = true;
-        theta = th;
+        for (int a = 0; a < na_rr; ++a) theta[locked + a] = th[a];
         lane.dense_s += secs(t_dense);
         upload(theta, lambda, &coef);
         const int next = ch.cur ^ 1;
-        timer_.time(KS_K_BLOCK_UPDATE, m, 2 * k, 4.0 * (m + 2 * k) * npts, lane.s,
-                    [&] { launch_block_lincomb(L_.F, m, S.at(0), 2 * k, coef_d, ch.A[next].at(0), k, k, lane.s); });
+        // X_a to [locked, k) and P_a to [k + na, k + 2 na) of the other buffer: outputs from the base at column
+        // `locked`, the P outputs (from na on) shifted by a gap of na
+        timer_.time(KS_K_BLOCK_UPDATE, m, 2 * na_rr, 4.0 * (m + 2 * na_rr) * npts, lane.s, [&] {
+            launch_block_lincomb(L_.F, m, S.at(0), 2 * na_rr, coef_d, ch.A[next].at(locked), na_rr, na_rr, lane.s);
+        });
         ch.cur = next;
-        np = k;
+        np = na_rr;
         // 6. HX of the new X -- with the next iteration's residual, first sweep and |r|^2 partials formed in the same pass
         if (!nl_on_) {
             StencilArgs a;

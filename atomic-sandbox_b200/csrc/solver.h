@@ -220,6 +220,11 @@ struct EigenStats {
     bool restores_exhausted = false;
     double alpha_worst = 0;
     int fallbacks = 0;
+    // the split stop test's two tiers: the true max residual of the head columns and of the tail columns [head, checked)
+    double head_res = 0, tail_res = 0;
+    // the head columns came back exactly as given: a 0-iteration accept, or a locked head
+    bool head_kept = false;
+    int locked = 0;  // the locked head's columns (0: no lock)
 };
 
 // One spin channel's LOBPCG work space: k vectors, [X | W | P] arenas (ping-pong), [R | HW | HP],
@@ -284,10 +289,14 @@ public:
     double effective_eig_tol(double eig_tol) const;
     // the ionic setup of the next solves (n = 0: all-electron); throws std::invalid_argument on bad tables
     void set_ionic(const ks_species* sp, int n) { ionic_.set(sp, n); }
-    // columns [0, checked) are held to tol, the others to tail_tol (infinite: untested; the split stop test of
-    // crates/qm-gpu/src/eigen.rs:781-787, a column's residual scaled by tol / its own tolerance)
-    EigenStats lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int checked,
-                      double tail_tol = std::numeric_limits<double>::infinity());
+    // lobpcg_split / lobpcg_guarded (crates/qm-gpu/src/eigen.rs:613-653): columns [0, head) are held to tol, columns
+    // [head, checked) to tail_tol and columns from `checked` on are untested buffers (the split stop test of
+    // eigen.rs:781-787, a column's residual scaled by tol / its own tolerance; the guess accepted at guess_tol on the same
+    // scale). checked < 0: every column when tail_tol is finite, else the head alone. lock: at the guess, a head under
+    // guess_tol whose tail is not is locked -- returned bitwise while the other columns iterate in its B-orthogonal
+    // complement (eigen.rs:174-183, :814-818).
+    EigenStats lobpcg(Channel& ch, Lane& lane, const float* V, double tol, double guess_tol, int max_iter, int head,
+                      double tail_tol = std::numeric_limits<double>::infinity(), int checked = -1, bool lock = false);
     Lane& lane(int i) { return *lane_[i]; }
     std::string error;
     const Layout& layout() const { return L_; }
@@ -385,5 +394,9 @@ double residual_floor_estimate(double h);
 // of A c = theta B c; C column-major m x nk. Throws NumericalError on a zero-norm column or rank loss.
 double rayleigh_ritz(int m, const std::vector<double>& A, const std::vector<double>& B, int nk, std::vector<double>& theta,
                      std::vector<double>& C);
+// rayleigh_ritz_locked (crates/qm-gpu/src/eigen.rs:669-681): the lowest na pairs on the subspace {S c : Y^T B (S c) = 0}
+// of the columns after the first `locked` (Y), c = Q c' with Q = [-B_YY^-1 B_YZ; I]; C column-major m x na.
+double rayleigh_ritz_locked(int m, const std::vector<double>& A, const std::vector<double>& B, int locked, int na,
+                            std::vector<double>& theta, std::vector<double>& C);
 
 }  // namespace ks

@@ -60,6 +60,11 @@ class _Profile(ctypes.Structure):
                [("witness_growths", ctypes.c_int), ("extrapolated", ctypes.c_int)]
 
 
+class _EigenStats(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_int) for f in ("iterations", "stop", "head_kept", "locked", "restores", "fallbacks", "readbacks")] + \
+               [(f, ctypes.c_double) for f in ("max_residual", "head_residual", "tail_residual", "alpha_worst")]
+
+
 class _KernelTime(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int), ("count", ctypes.c_int), ("aux", ctypes.c_int), ("launches", ctypes.c_int),
                 ("total_ms", ctypes.c_double), ("bytes", ctypes.c_double)]
@@ -196,6 +201,7 @@ EXPORTED = [
     "ks_solver_create", "ks_solver_destroy", "ks_solve", "ks_forces", "ks_last_error", "ks_state_counts", "ks_state_evals",
     "ks_state_density", "ks_state_potentials", "ks_state_orbitals", "ks_profile_get", "ks_apply_hamiltonian",
     "ks_apply_laplacian", "ks_apply_precond", "ks_xc_lsda", "ks_nuclear_potential", "ks_poisson_solve", "ks_gram", "ks_lobpcg",
+    "ks_lobpcg_guarded",
     "ks_multipole_moments", "ks_field_pitch", "ks_hpsi_device", "ks_solver_stream", "ks_launch_count",
     "ks_gram_device_noalloc", "ks_vjp", "ks_state_occupations", "ks_sample_density", "ks_sampling_counters",
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
@@ -257,6 +263,9 @@ def lib():
         L.ks_diis_mix.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp]
         L.ks_lobpcg.argtypes = [ctypes.c_int, ctypes.c_double, dp, ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                 dp, ip]
+        L.ks_lobpcg_guarded.argtypes = [ctypes.c_int, ctypes.c_double, dp, ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp,
+                                        ctypes.POINTER(_EigenStats)]
         L.ks_multipole_moments.argtypes = [ctypes.c_int, ctypes.c_double, dp, dp]
         L.ks_rayleigh_ritz.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp]
         L.ks_fermi_dirac.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
@@ -895,6 +904,23 @@ def lobpcg(n, h, v, x0, tol=1e-5, max_iter=500, gram_mode=0):
     _check(lib().ks_lobpcg(n, h, _p(_f64(v, n ** 3)), k, _p(x), _p(ev), float(tol), int(max_iter), int(gram_mode),
                            ctypes.byref(mr), ctypes.byref(it)))
     return ev, x, it.value, mr.value
+
+
+def lobpcg_guarded(n, h, v, x0, tol, guess_tol, head, tail_tol, checked, max_iter=500, lock=True, gram_mode=0):
+    """lobpcg_guarded (lock) / lobpcg_split (crates/qm-gpu/src/eigen.rs:613-653) through ks_lobpcg_guarded: columns
+    [0, head) at tol, [head, checked) at tail_tol, the rest untested. Returns (evals, x, residuals, stats) with stats the
+    EigenStats fields as a dict (head_kept a bool)."""
+    x = _f64(x0).copy()
+    k = x.shape[0]
+    ev = np.empty(k)
+    res = np.empty(k)
+    st = _EigenStats()
+    _check(lib().ks_lobpcg_guarded(n, h, _p(_f64(v, n ** 3)), k, _p(x), _p(ev), float(tol), float(guess_tol), int(head),
+                                   float(tail_tol), int(checked), int(max_iter), 1 if lock else 0, int(gram_mode), _p(res),
+                                   ctypes.byref(st)))
+    stats = {f: getattr(st, f) for f, _ in _EigenStats._fields_}
+    stats["head_kept"] = bool(stats["head_kept"])
+    return ev, x, res, stats
 
 
 def field_pitch(n):

@@ -332,6 +332,21 @@ ks_status ks_gram(int n, int m, const double* s, int mt, const double* t, int gr
 /* lobpcg (crates/qm-gpu/src/eigen.rs:685-1000) on H = -1/2 lap + V: k vectors x (guess and result), evals out. */
 ks_status ks_lobpcg(int n, double h, const double* v, int k, double* x, double* evals, double tol, int max_iter,
                     int gram_mode, double* max_residual, int* iterations);
+/* EigenStats (crates/qm-gpu/src/eigen.rs:286-305): stop 0 converged, 1 the f32 floor, 2 max_iter; head_kept: the head
+   columns came back bitwise (a 0-iteration accept or a locked head); locked: the locked head's columns; head_residual /
+   tail_residual: the true max residuals of the columns [0, head) and [head, checked). */
+typedef struct {
+    int iterations, stop, head_kept, locked, restores, fallbacks, readbacks;
+    double max_residual, head_residual, tail_residual, alpha_worst;
+} ks_eigen_stats;
+/* lobpcg_split (lock 0) and lobpcg_guarded (lock 1) (crates/qm-gpu/src/eigen.rs:613-653): columns [0, head) held to tol,
+   [head, checked) to tail_tol >= tol, columns from `checked` on untested buffers; the guess accepted at guess_tol on the
+   same scale. With lock, a head under guess_tol at the guess whose tail is not is locked: returned bitwise while the
+   other columns iterate in its B-orthogonal complement. residuals (k, may be NULL): every column's exit residual.
+   KS_INVALID unless 0 <= head <= checked <= k, checked >= 1, tol <= tail_tol. */
+ks_status ks_lobpcg_guarded(int n, double h, const double* v, int k, double* x, double* evals, double tol, double guess_tol,
+                            int head, double tail_tol, int checked, int max_iter, int lock, int gram_mode, double* residuals,
+                            ks_eigen_stats* stats);
 /* multipole moments Q_lm = sum rho R_lm dV (crates/qm-gpu/src/poisson.rs:237-244) */
 ks_status ks_multipole_moments(int n, double h, const double* rho, double* q49);
 

@@ -22,6 +22,9 @@ pub type ks_abort_fn = Option<unsafe extern "C" fn(user: *mut c_void) -> c_int>;
 #[repr(C)] pub struct ks_progress { pub iteration: c_int, pub max_iter: c_int, pub delta_rho: f64, pub tol: f64, pub energy: f64,
     pub best_delta_rho: f64, pub since_gain: c_int, pub window: c_int, pub stall_level: f64 }
 pub type ks_observe_fn = Option<unsafe extern "C" fn(p: *const ks_progress, user: *mut c_void)>;
+#[repr(C)] #[derive(Default, Clone, Copy)] pub struct ks_eigen_stats { pub iterations: c_int, pub stop: c_int, pub head_kept: c_int,
+    pub locked: c_int, pub restores: c_int, pub fallbacks: c_int, pub readbacks: c_int, pub max_residual: c_double,
+    pub head_residual: c_double, pub tail_residual: c_double, pub alpha_worst: c_double }
 #[repr(C)] pub struct ks_species { pub z: c_int, pub z_v: c_double, pub sigma_lr: c_double, pub du: c_double,
     pub v_sr: *const c_double, pub n_v_sr: c_int, pub r_sr: c_double,
     pub rho_pc: *const c_double, pub n_rho_pc: c_int, pub pc_radius: c_double,
@@ -83,6 +86,10 @@ extern "C" {
     pub fn ks_lobpcg(n: c_int, h: c_double, v: *const c_double, k: c_int, x: *mut c_double, evals: *mut c_double,
                      tol: c_double, max_iter: c_int, gram_mode: c_int, max_residual: *mut c_double,
                      iterations: *mut c_int) -> c_int;
+    pub fn ks_lobpcg_guarded(n: c_int, h: c_double, v: *const c_double, k: c_int, x: *mut c_double, evals: *mut c_double,
+                             tol: c_double, guess_tol: c_double, head: c_int, tail_tol: c_double, checked: c_int,
+                             max_iter: c_int, lock: c_int, gram_mode: c_int, residuals: *mut c_double,
+                             stats: *mut ks_eigen_stats) -> c_int;
     pub fn ks_multipole_moments(n: c_int, h: c_double, rho: *const c_double, q49: *mut c_double) -> c_int;
     pub fn ks_launch_count() -> i64;
     // host-only parity hooks (the solver's f64 host algebra)

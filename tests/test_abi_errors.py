@@ -56,6 +56,10 @@ def test_null_handles_and_bad_sizes_return_invalid(ks):
     assert lib.ks_gram(33, 2, p, 0, p, 1, p) == ks.KS_INVALID  # the tensor-core form needs mt >= 1
     assert lib.ks_hpsi_device(None, 33, 0.25, 0, None, None, None) == ks.KS_INVALID
     assert lib.ks_rayleigh_ritz(4, p, p, 5, p, p, p) == ks.KS_INVALID  # nk > m
+    # the guarded LOBPCG: head > checked, checked > k, and a tail tolerance below tol
+    assert lib.ks_lobpcg_guarded(33, 0.25, p, 3, p, p, 1e-5, 1.5e-5, 3, 1e-3, 2, 10, 1, 0, p, None) == ks.KS_INVALID
+    assert lib.ks_lobpcg_guarded(33, 0.25, p, 3, p, p, 1e-5, 1.5e-5, 2, 1e-3, 4, 10, 1, 0, p, None) == ks.KS_INVALID
+    assert lib.ks_lobpcg_guarded(33, 0.25, p, 3, p, p, 1e-5, 1.5e-5, 2, 1e-6, 3, 10, 1, 0, p, None) == ks.KS_INVALID
     assert lib.ks_footprint_bytes(4, 1, 1, None, 6, 0) == -1
     assert lib.ks_footprint_bytes(33, -1, 1, None, 6, 0) == -1
     assert lib.ks_set_kernel_timing(None, 1) == ks.KS_INVALID
