@@ -863,6 +863,18 @@ ks_status ks_fd_step_tail_kt(int n_w, double delta_rho_prev, double* tail_kt) {
     return KS_OK;
 }
 
+ks_status ks_fd_tight_columns(const double* evals, const double* residuals, int k, double mu, double kt, double tol, int* tight) {
+    if (k < 0 || (k > 0 && (!evals || !residuals)) || !tight || !(kt > 0) || !(tol > 0)) return fail(nullptr, KS_INVALID, "invalid arguments");
+    *tight = dense::fd_tight_columns(evals, residuals, k, mu, kt, tol);
+    return KS_OK;
+}
+
+ks_status ks_fd_tight_start(const double* f, int k, int n, double tol, int* tight) {
+    if (k < 0 || n < 0 || !tight || !(tol > 0)) return fail(nullptr, KS_INVALID, "invalid arguments");
+    *tight = dense::fd_tight_start(k > 0 ? f : nullptr, k, n, tol);
+    return KS_OK;
+}
+
 ks_status ks_fd_witness_keep_within(const double* evals, const double* residuals, int k, int n, double mu, double kt, double tail_kt,
                                     double r_max, int* keep) {
     if (k < 0 || n < 0 || (k > 0 && (!evals || !residuals)) || !keep || !std::isfinite(tail_kt))

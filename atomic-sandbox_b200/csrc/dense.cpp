@@ -402,6 +402,36 @@ int fd_witness_keep_within(const double* ev, const double* res, int k, int n, do
     return -1;
 }
 
+int fd_tight_columns(const double* ev, const double* res, int k, double mu, double kt, double tol) {
+    if (!std::isfinite(mu) || k <= 0) return 0;
+    const std::vector<int> o = ascending(ev, k);
+    const double limit = 1e-2 * tol;  // LOOSE_F_FACTOR x tol
+    // from the top rank down: the loose ranks are those whose running tail sum of f(theta - r) stays below the limit
+    double tail = 0.0;
+    int loose_from = k;
+    for (int r = k - 1; r >= 0; --r) {
+        tail += fd_occupation((ev[o[r]] - (res ? res[o[r]] : 0.0) - mu) / kt);
+        if (!(tail < limit)) break;
+        loose_from = r;
+    }
+    int t = 0;
+    for (int r = 0; r < loose_from; ++r) t = std::max(t, o[r] + 1);
+    return t;
+}
+
+int fd_tight_start(const double* f, int k, int n, double tol) {
+    if (!f) return n;
+    const double limit = 1e-2 * tol;
+    double tail = 0.0;
+    int loose_from = k;
+    for (int i = k - 1; i >= 0; --i) {
+        tail += f[i];
+        if (!(tail < limit)) break;
+        loose_from = i;
+    }
+    return std::max(loose_from, n);
+}
+
 int fd_witness_keep(const double* ev, const double* res, int k, int n, double mu, double kt, double tail_kt) {
     if (n == 0 || k <= n) return k;
     const std::vector<int> o = ascending(ev, k);

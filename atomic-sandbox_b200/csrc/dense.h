@@ -1,6 +1,7 @@
 // dense.h -- small dense f64 linear algebra on the host: the Rayleigh-Ritz and DIIS solves of the
 // SCF (matrices of a few dozen rows). Row-major storage unless stated.
 #pragma once
+#include <algorithm>
 #include <vector>
 
 namespace ks {
@@ -53,6 +54,16 @@ double fd_step_tail_kt(int n_w, double delta_rho_prev);
 // rank t + 1 passes on its lower bound too); -1 when no such level exists (the block must grow); k for n = 0. A NaN
 // residual never qualifies.
 int fd_witness_keep_within(const double* evals, const double* res, int k, int n, double mu, double kt, double tail_kt, double r_max);
+
+// The positions the step's tolerance must hold (occupations.rs:334-350 tight_columns): from the top rank down, the
+// ranks whose running sum of f((theta - r - mu) / kT) stays below 1e-2 tol are loose; the result is one past the highest
+// position of a tight rank (0 without mu, NaN mu).
+int fd_tight_columns(const double* evals, const double* res, int k, double mu, double kt, double tol);
+// The tight count a solve starts from (occupations.rs:355-366 tight_start): the positions of a warm state's ascending
+// occupations f that the same tail rule needs at tol, at least n; n without f.
+int fd_tight_start(const double* f, int k, int n, double tol);
+// The extra block after a failed witness (occupations.rs:423 grown_extras): 2 extras, at least one more, at most cap.
+inline int fd_grown_extras(int extras, int cap) { return std::min(std::max(2 * extras, extras + 1), cap); }
 
 }  // namespace dense
 }  // namespace ks

@@ -116,13 +116,12 @@ constexpr double EIG_TOL_FLOOR_FACTOR = 3.0;
 constexpr double EIG_GUESS_FACTOR = 1.5;
 // Fermi-Dirac (crates/qm/src/occupations.rs): a level with min(f, 1 - f) at or above PARTIAL_OCCUPATION_MIN is partly
 // occupied, and a step with one is tested against max(tol, GPU_PARTIAL_TOL); the columns of the block whose occupation
-// tail stays below LOOSE_F_FACTOR * tol are held to the guard tolerance WITNESS_GUARD_TOL = WITNESS_GAP / 100 (or the
-// step's eigen tolerance when that is looser; occupations.rs:91-92, :184-186), so that their lower bounds theta - r,
-// on which the gap witness is read, are within 1e-3 Ha of their levels.
+// tail (on their lower bounds theta - r) stays below 1e-2 tol (dense::fd_tight_columns) are held to the guard tolerance
+// WITNESS_GUARD_TOL = WITNESS_GAP / 100 (or the step's eigen tolerance when that is looser; occupations.rs:91-92,
+// :184-186), so that their lower bounds, on which the gap witness is read, are within 1e-3 Ha of their levels.
 constexpr double PARTIAL_OCCUPATION_MIN = 1e-6;
 constexpr double WITNESS_GUARD_TOL = 1e-3;
 constexpr double GPU_PARTIAL_TOL = 1e-5;
-constexpr double LOOSE_F_FACTOR = 1e-2;
 constexpr double EIG_TOL_FRACTION = 0.0015;
 constexpr double EIG_TOL_MAX = 1e-3;
 constexpr double LAST_STEP_RESIDUAL_FACTOR = 3.0;
@@ -745,20 +744,51 @@ void Channel::create(const Layout& L, int kk) {
 // ------------------------------------------------------------------ solver
 // The channel's block at newk columns: the lowest min(k, newk) columns of the current iterate are kept (in the first
 // arena), new ones are the reference's initial orbital with seed 1000 + 2 * column + spin (crates/qm/src/scf.rs:866).
-void Solver::resize_channel(int sp, int newk, const Nuc* dnuc, int nn) {
+void Solver::resize_channel(int sp, int newk, const Nuc* dnuc, int nn, cudaStream_t st, const std::vector<int>* cols) {
+    if (!st) st = s_;
     Channel& old = ch_[sp];
-    const int keep = std::min(old.k, newk);
+    const int keep = cols ? (int)cols->size() : std::min(old.k, newk);
     Channel nc;
     nc.create(L_, newk);
-    KS_CUDA(cudaMemcpyAsync(nc.A[0].at(0), old.X(), (size_t)keep * L_.F * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+    const size_t fb = (size_t)L_.F * sizeof(float);
+    if (cols) {  // column j of the new block is column (*cols)[j] of the old one
+        for (int j = 0; j < keep; ++j)
+            KS_CUDA(cudaMemcpyAsync(nc.A[0].at(j), old.A[old.cur].at((*cols)[j]), fb, cudaMemcpyDeviceToDevice, st));
+    } else {
+        KS_CUDA(cudaMemcpyAsync(nc.A[0].at(0), old.X(), (size_t)keep * fb, cudaMemcpyDeviceToDevice, st));
+    }
     for (int i = keep; i < newk; ++i)
-        launch_initial_orbitals(L_, dnuc, nn, 1, 1000ULL + 2ULL * (unsigned long long)i + (unsigned long long)sp, 0, nc.A[0].at(i), s_);
-    nc.evals.assign(old.evals.begin(), old.evals.begin() + std::min<size_t>(keep, old.evals.size()));
+        launch_initial_orbitals(L_, dnuc, nn, 1, 1000ULL + 2ULL * (unsigned long long)i + (unsigned long long)sp, 0, nc.A[0].at(i), st);
+    nc.evals.clear();
+    for (int j = 0; j < keep; ++j) {
+        const int src = cols ? (*cols)[j] : j;
+        nc.evals.push_back(src < (int)old.evals.size() ? old.evals[src] : -1.0);
+        if (src < (int)old.res.size()) nc.res[j] = old.res[src];
+    }
+    // a new vector's eigenvalue placeholder: the block's last (crates/qm-gpu/src/scf.rs:843-849)
     while ((int)nc.evals.size() < newk) nc.evals.push_back(nc.evals.empty() ? -1.0 : nc.evals.back());
-    for (int i = 0; i < keep && i < (int)old.res.size(); ++i) nc.res[i] = old.res[i];
     nc.cur = 0;
-    KS_CUDA(cudaStreamSynchronize(s_));  // the old block is freed below
+    KS_CUDA(cudaStreamSynchronize(st));  // the old block is freed below
     ch_[sp] = std::move(nc);
+}
+
+int Solver::buffer_last(int sp, cudaStream_t st) {
+    Channel& ch = ch_[sp];
+    const int last = ch.k - 1;
+    int top = last;
+    for (int i = 0; i < ch.k; ++i)
+        if (ch.evals[i] > ch.evals[top]) top = i;
+    if (top == last) return -1;
+    // swap the two columns of X through the H X scratch (free between LOBPCG calls: each call recomputes it)
+    const size_t fb = (size_t)L_.F * sizeof(float);
+    float* x = ch.A[ch.cur].at(0);
+    float* tmp = ch.HX.at(0);
+    KS_CUDA(cudaMemcpyAsync(tmp, x + (size_t)top * L_.F, fb, cudaMemcpyDeviceToDevice, st));
+    KS_CUDA(cudaMemcpyAsync(x + (size_t)top * L_.F, x + (size_t)last * L_.F, fb, cudaMemcpyDeviceToDevice, st));
+    KS_CUDA(cudaMemcpyAsync(x + (size_t)last * L_.F, tmp, fb, cudaMemcpyDeviceToDevice, st));
+    std::swap(ch.evals[top], ch.evals[last]);
+    std::swap(ch.res[top], ch.res[last]);
+    return top;
 }
 
 // Mirrors the allocations of the constructor, Poisson::init, Reducer::init, Channel::create, the DIIS pool and the
@@ -1195,6 +1225,128 @@ EigenStats Solver::lobpcg(Channel& ch, Lane& lane, const float* V, double tol, d
     return es;
 }
 
+// The Fermi-Dirac channel solve (crates/qm-gpu/src/scf.rs:875-1029, the CPU's qm::scf::solve_fd rule plus the GPU's
+// buffer and step-accuracy tail). The block's lowest `tight` columns are held to the step's tol, the others below the top
+// to the guard tolerance max(1e-3, step tol) and the top one is an untested buffer while one fits below the cap (a block
+// of n + 1 first gets one more vector); the LOBPCG locks a converged head while only the loose columns move. Then:
+// - the swap edge: an untested column that buffer_last moved into the tested range is re-solved, at most twice, toward
+//   the guard tolerance;
+// - the class raise: the tight count is re-read on the lower bounds (tight_columns at the SCF's tol); a solve whose head
+//   was too small is repeated with the larger one;
+// - the witness on the tested levels' lower bounds theta - r (36 kT, or the loosened step's tail): on a tight step a top
+//   tested level that exits above 1.5 x the guard tolerance decides only through the lowest level that passes at or
+//   below it (witness_keep_within), else the block grows by one; once witnessed, the overshoot above the lowest witness
+//   is trimmed, keeping the next level as the buffer when one fits, never below the configured N_sigma + n_extra;
+// - the buffer as the witness: a buffer whose own bound passes decides at r <= the guard tolerance (and one fresh vector
+//   becomes the next buffer), else the block grows by one;
+// - otherwise the extra block doubles (grown_extras), at most the cap; at the cap the witness check at convergence
+//   reports the missing witness.
+// New vectors are the reference's initial orbitals with seed 1000 + 2 * index + spin.
+Solver::FdOutcome Solver::solve_fd(int sp, const float* V, double step_tol, double guess_tol, bool loosened, double delta_rho_prev,
+                                   double kt, double scf_tol, int n, int& kk, int& tight, const Nuc* dnuc, int nn) {
+    FdOutcome out;
+    Lane& lane = *lane_[sp];
+    const int cap = std::min(witness_cap_, 64 - n);
+    const int base = n + opt_.n_extra;
+    const double guard_tol = std::max(WITNESS_GUARD_TOL, step_tol);
+    const double r_witness = EIG_GUESS_FACTOR * WITNESS_GUARD_TOL;
+    auto buffered = [&](int len) { return len >= n + 2 && len - n < cap; };
+    auto grow_to = [&](int len) {
+        resize_channel(sp, len, dnuc, nn, lane.s);
+        kk = len;
+    };
+    if (kk == n + 1 && cap >= 2) grow_to(kk + 1);
+    int swap_retries = 0;
+    for (;;) {
+        const int checked = buffered(kk) ? kk - 1 : kk;
+        const int head = std::min(tight, checked);
+        out.peak_block = std::max(out.peak_block, kk);
+        const double tail_kt = loosened ? dense::fd_step_tail_kt(kk, delta_rho_prev) : 36.0;
+        const EigenStats es = lobpcg(ch_[sp], lane, V, step_tol, guess_tol, EIGEN_MAX_ITER, head, guard_tol, checked, true);
+        ++out.calls;
+        out.iterations += es.iterations;
+        if (es.restores_exhausted) throw NumericalError("LOBPCG: a Ritz-vector formation failed again after its restores");
+        out.tight_res = es.head_res;
+        out.maxiter = es.stop == 2;
+        if (checked < kk) {
+            const int moved = buffer_last(sp, lane.s);
+            if (moved >= 0 && ch_[sp].res[moved] > guard_tol && swap_retries < 2) {
+                ++swap_retries;
+                continue;
+            }
+        }
+        out.kept = out.kept && es.head_kept;
+        if (es.head_kept && es.iterations > 0) ++out.locked_calls;
+        const double* ev = ch_[sp].evals.data();
+        const double* rv = ch_[sp].res.data();
+        std::vector<double> f(checked);
+        double mu = NAN, ent = 0.0;
+        if (!dense::fermi_dirac(ev, checked, n, kt, f.data(), mu, ent)) throw NumericalError("Fermi-Dirac occupations refused (a non-finite level)");
+        const int need = dense::fd_tight_columns(ev, rv, checked, mu, kt, scf_tol);
+        tight = need;
+        if (need > head) {
+            ++out.class_raises;
+            continue;  // a column held loose needs the step's tol: re-solve with it tight
+        }
+        out.tail_kt = std::max(out.tail_kt, tail_kt);
+        const bool witness = dense::fd_witness(ev, rv, checked, n, mu, kt, tail_kt);
+        int top = 0;
+        for (int i = 1; i < checked; ++i)
+            if (ev[i] > ev[top]) top = i;
+        int keep = -1;
+        if (witness && !loosened && rv[top] > r_witness && kk - n < cap) {
+            keep = dense::fd_witness_keep_within(ev, rv, checked, n, mu, kt, tail_kt, r_witness);
+            if (keep < 0) {
+                ++out.residual_growths;
+                grow_to(kk + 1);
+                continue;
+            }
+            ++out.lower_witnesses;
+        } else if (witness) {
+            keep = dense::fd_witness_keep(ev, rv, checked, n, mu, kt, tail_kt);
+        }
+        if (keep >= 0) {
+            const int len = std::max(base, buffered(keep + 1) ? keep + 1 : keep);
+            if (len < kk) {
+                // the lowest `len` levels by value, in their positions' order
+                std::vector<int> order(kk);
+                for (int i = 0; i < kk; ++i) order[i] = i;
+                std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ev[a] < ev[b]; });
+                std::vector<int> cols(order.begin(), order.begin() + len);
+                std::sort(cols.begin(), cols.end());
+                resize_channel(sp, len, dnuc, nn, lane.s, &cols);
+                kk = len;
+                ++out.trims;
+                if (buffered(len)) buffer_last(sp, lane.s);
+            }
+            out.checked = buffered(kk) ? kk - 1 : kk;
+            out.witnessed = true;
+            return out;
+        }
+        if (checked < kk && dense::fd_witness(ev, rv, kk, n, mu, kt, tail_kt)) {
+            if (rv[kk - 1] <= WITNESS_GUARD_TOL) {
+                ++out.buffer_witnesses;
+                out.checked = checked;
+                out.witnessed = true;
+                if (kk - n < cap) grow_to(kk + 1);  // the next step's buffer
+                return out;
+            }
+            if (kk - n < cap) {
+                ++out.buffer_growths;
+                grow_to(kk + 1);
+                continue;
+            }
+        }
+        const int extras = kk - n;
+        if (extras >= cap) {
+            out.checked = checked;
+            return out;
+        }
+        ++out.growths;
+        grow_to(n + dense::fd_grown_extras(extras, cap));
+    }
+}
+
 double Solver::effective_eig_tol(double eig_tol) const { return std::max(eig_tol, EIG_TOL_FLOOR_FACTOR * floor_); }
 
 ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const ks_settings& s, bool warm, ks_abort_fn abort_fn,
@@ -1262,8 +1414,13 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             if (fd && kk[sp] > 0 ? ch_[sp].k < kk[sp] : ch_[sp].k != kk[sp]) reuse = false;
         if (reuse && fd)
             for (int sp = 0; sp < 2; ++sp) kk[sp] = ch_[sp].k;
-        // columns held to the eigen tolerance: N_sigma, or under Fermi-Dirac the block minus its loose tail (set each step)
+        // columns held to the eigen tolerance: N_sigma; under Fermi-Dirac a warm state's start is the positions its stored
+        // occupations need at the SCF's tol (tight_start, crates/qm-gpu/src/scf.rs:1290-1295), and every channel solve
+        // re-reads it on its own levels
         int tight[2] = {nocc[0], nocc[1]};
+        if (reuse && fd)
+            for (int sp = 0; sp < 2; ++sp)
+                if (nocc[sp] > 0 && (int)occ_[sp].size() == kk[sp]) tight[sp] = dense::fd_tight_start(occ_[sp].data(), kk[sp], nocc[sp], s.tol);
         double entropy = 0.0, mu[2] = {NAN, NAN};
         bool partial = false;
         occ_d_.alloc(2 * 64 * sizeof(double));
@@ -1349,6 +1506,14 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         double delta_rho = INFINITY, test_tol = s.tol;
         double q_out[2] = {0, 0};
         bool frozen = false, stalled = false;
+        // Fermi-Dirac (crates/qm-gpu/src/scf.rs:1370-1374): this step's calls all returned their tight columns bitwise; the
+        // DIIS entries measured on the current frozen orbitals' output; the previous step's widest witness tail; the
+        // tested levels per channel (the buffer above them holds no charge) and whether a witness decided each channel
+        bool step_kept = false;
+        int consistent = 0, step_growths = 0;
+        double prev_tail = INFINITY, step_tail = 0.0;
+        int fd_checked[2] = {0, 0};
+        bool fd_witnessed[2] = {false, false};
         double anchor = INFINITY, best = INFINITY;
         int anchor_at = 0;
         const double level = STALL_LEVEL_PER_ELECTRON * (n_up + n_dn);
@@ -1412,13 +1577,17 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             // when both are occupied, the down channel on a second host thread, so one channel's
             // kernels fill the GPU while the other waits on a readback or does its host algebra
             EigenStats est[2];
+            FdOutcome fdo[2];
             {
                 KS_CUDA(cudaEventRecord(ev_fork_, s_));
                 for (auto& l : lane_) KS_CUDA(cudaStreamWaitEvent(l->s, ev_fork_, 0));
                 auto run = [&](int sp) {
-                    est[sp] = lobpcg(ch_[sp], *lane_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, guess_factor * step_tol,
-                                     EIGEN_MAX_ITER, fd ? tight[sp] : nocc[sp],
-                                     fd ? std::max(WITNESS_GUARD_TOL, step_tol) : std::numeric_limits<double>::infinity());
+                    const float* vv = sp ? v_dn_.at(0) : v_up_.at(0);
+                    if (fd)
+                        fdo[sp] = solve_fd(sp, vv, step_tol, guess_factor * step_tol, step_tol > eig_lo, delta_rho, s.kt, s.tol, nocc[sp],
+                                           kk[sp], tight[sp], dnuc, nn);
+                    else
+                        est[sp] = lobpcg(ch_[sp], *lane_[sp], vv, step_tol, guess_factor * step_tol, EIGEN_MAX_ITER, nocc[sp]);
                 };
                 std::exception_ptr err_dn;
                 std::thread worker;
@@ -1463,79 +1632,45 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                 if (err_dn && !is_abort(err_dn)) std::rethrow_exception(err_dn);
                 if (err_up || err_dn) return park("abandoned inside SCF step " + std::to_string(iterations) + " (an eigensolve)");
             }
+            step_kept = true;
+            step_growths = 0;
+            step_tail = 0.0;
             for (int sp = 0; sp < 2; ++sp) {
                 if (nocc[sp] == 0) continue;
+                if (fd) {
+                    // the step's FD bookkeeping (crates/qm-gpu/src/scf.rs:1436-1438, SolveProfile's counters)
+                    const FdOutcome& o = fdo[sp];
+                    profile.eigen_calls += o.calls;
+                    profile.eigen_iterations += o.iterations;
+                    eig_its += o.iterations;
+                    if (step_tol <= eig_lo) max_eig_res = std::max(max_eig_res, o.tight_res);
+                    last_step_res = std::max(last_step_res, o.tight_res);
+                    if (o.maxiter) last_step_maxiter = true;
+                    step_kept = step_kept && o.kept;
+                    step_growths += o.growths;
+                    step_tail = std::max(step_tail, o.tail_kt);
+                    fd_checked[sp] = o.checked;
+                    fd_witnessed[sp] = o.witnessed;
+                    profile.witness_growths += o.growths;
+                    profile.locked_calls += o.locked_calls;
+                    profile.class_raises += o.class_raises;
+                    profile.buffer_witnesses += o.buffer_witnesses;
+                    profile.buffer_growths += o.buffer_growths;
+                    profile.lower_witnesses += o.lower_witnesses;
+                    profile.witness_residual_growths += o.residual_growths;
+                    profile.witness_trims += o.trims;
+                    profile.peak_block = std::max(profile.peak_block, o.peak_block);
+                    continue;
+                }
                 const EigenStats& es = est[sp];
                 ++profile.eigen_calls;
                 profile.eigen_iterations += es.iterations;
                 eig_its += es.iterations;
                 if (es.restores_exhausted) throw NumericalError("LOBPCG: a Ritz-vector formation failed again after its restores");
-                const double tight = es.max_residual;
-                if (step_tol <= eig_lo) max_eig_res = std::max(max_eig_res, tight);
-                last_step_res = std::max(last_step_res, tight);
+                const double tight_r = es.max_residual;
+                if (step_tol <= eig_lo) max_eig_res = std::max(max_eig_res, tight_r);
+                last_step_res = std::max(last_step_res, tight_r);
                 if (es.stop == 2) last_step_maxiter = true;
-            }
-            // Fermi-Dirac gap witness growth (crates/qm/src/scf.rs:810-877, solve_fd): while the block's highest level is
-            // no witness, its extra levels double (at most the witness cap, 32 by default, and 64 levels in all; a new vector is the
-            // reference's initial orbital with seed 1000 + 2 * index + spin) and the channel is solved again with every
-            // level held to the step's tolerance; once witnessed, the overshoot above the lowest witness is trimmed, never
-            // below the configured N_sigma + n_extra. The witness is read on the lower bounds theta - r (occupations.rs:93-99,
-            // witness_bound_reached). On a tight step a witness whose top level exits above EIG_GUESS_FACTOR * the guard
-            // tolerance decides only through the lowest level that passes at or below that residual (witness_keep_within,
-            // occupations.rs:396-419; crates/qm-gpu/src/scf.rs:940-965); without one the block grows by one vector.
-            for (int sp = 0; sp < 2 && fd; ++sp) {
-                if (nocc[sp] == 0) continue;
-                const int base = nocc[sp] + opt_.n_extra;
-                const int cap = std::min(witness_cap_, 64 - nocc[sp]);
-                for (;;) {
-                    std::vector<double> f(kk[sp]);
-                    double m_sp = 0.0, s_sp = 0.0;
-                    if (!dense::fermi_dirac(ch_[sp].evals.data(), kk[sp], nocc[sp], s.kt, f.data(), m_sp, s_sp))
-                        throw NumericalError("Fermi-Dirac occupations refused (a non-finite level)");
-                    const int extras = kk[sp] - nocc[sp];
-                    const double* ev = ch_[sp].evals.data();
-                    const double* rv = ch_[sp].res.data();
-                    int grown;
-                    // the witness tail: 36 kT, or on a loosened step the step-accuracy tail (occupations.rs:319-326;
-                    // crates/qm-gpu/src/scf.rs:909, n_w the block's levels, the previous step's delta rho)
-                    const double tail_kt = step_tol > eig_lo ? dense::fd_step_tail_kt(kk[sp], delta_rho) : 36.0;
-                    if (dense::fd_witness(ev, rv, kk[sp], nocc[sp], m_sp, s.kt, tail_kt)) {
-                        int top = 0;
-                        for (int i = 1; i < kk[sp]; ++i)
-                            if (ev[i] > ev[top]) top = i;
-                        const double r_witness = EIG_GUESS_FACTOR * WITNESS_GUARD_TOL;
-                        int keep;
-                        if (step_tol <= eig_lo && !(rv[top] <= r_witness) && extras < cap)
-                            keep = dense::fd_witness_keep_within(ev, rv, kk[sp], nocc[sp], m_sp, s.kt, 36.0, r_witness);
-                        else
-                            keep = dense::fd_witness_keep(ev, rv, kk[sp], nocc[sp], m_sp, s.kt, tail_kt);
-                        if (keep >= 0) {
-                            keep = std::max(base, keep);
-                            if (keep < kk[sp]) {
-                                resize_channel(sp, keep, dnuc, nn);
-                                kk[sp] = keep;
-                                tight[sp] = std::min(tight[sp], keep);
-                            }
-                            break;
-                        }
-                        grown = extras + 1;  // no converged witness below the loose top: one vector more
-                    } else {
-                        if (extras >= cap) break;  // the witness check at convergence reports the cap
-                        grown = std::min(std::max(2 * extras, extras + 1), cap);
-                    }
-                    resize_channel(sp, nocc[sp] + grown, dnuc, nn);
-                    kk[sp] = nocc[sp] + grown;
-                    ++profile.witness_growths;
-                    KS_CUDA(cudaEventRecord(ev_fork_, s_));
-                    KS_CUDA(cudaStreamWaitEvent(lane_[sp]->s, ev_fork_, 0));
-                    const EigenStats es = lobpcg(ch_[sp], *lane_[sp], sp ? v_dn_.at(0) : v_up_.at(0), step_tol, step_tol, EIGEN_MAX_ITER, kk[sp]);
-                    KS_CUDA(cudaEventRecord(lane_[sp]->ev_join, lane_[sp]->s));
-                    KS_CUDA(cudaStreamWaitEvent(s_, lane_[sp]->ev_join, 0));
-                    profile.eigen_iterations += es.iterations;
-                    eig_its += es.iterations;
-                    if (es.restores_exhausted) throw NumericalError("LOBPCG: a Ritz-vector formation failed again after its restores");
-                    last_step_res = std::max(last_step_res, es.max_residual);
-                }
             }
             profile.eigen_s += secs(te);
             // occupations of this step's levels (crates/qm/src/scf.rs:996-1013): Aufbau 1 on the N_sigma lowest (the block
@@ -1551,14 +1686,12 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
                     for (int i = 0; i < nocc[sp]; ++i) occ_[sp][i] = 1.0;
                     continue;
                 }
+                // the tested levels (the untested buffer above them, if any, gets f = 0)
                 double s_sp = 0.0;
-                if (!dense::fermi_dirac(ch_[sp].evals.data(), kk[sp], nocc[sp], s.kt, occ_[sp].data(), mu[sp], s_sp))
+                const int nt = std::max(nocc[sp] + 1, std::min(fd_checked[sp], kk[sp]));
+                if (!dense::fermi_dirac(ch_[sp].evals.data(), nt, nocc[sp], s.kt, occ_[sp].data(), mu[sp], s_sp))
                     throw NumericalError("Fermi-Dirac occupations refused (a non-finite level)");
                 entropy += s_sp;
-                int t = kk[sp];
-                double tail = 0.0;
-                while (t > nocc[sp] && tail + occ_[sp][t - 1] < LOOSE_F_FACTOR * s.tol) tail += occ_[sp][--t];
-                tight[sp] = t;
                 for (int i = 0; i < kk[sp]; ++i) {
                     partial = partial || std::min(occ_[sp][i], 1.0 - occ_[sp][i]) >= PARTIAL_OCCUPATION_MIN;
                     occ_host[64 * sp + i] = occ_[sp][i];
@@ -1645,10 +1778,22 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             test_tol = (fd && partial) ? std::max(s.tol, GPU_PARTIAL_TOL) : s.tol;
             if (!std::isfinite(delta_rho) || (delta_rho < test_tol && step_tol <= eig_lo)) break;
             if (!(delta_rho < test_tol) && s.stall_window > 0 && since >= s.stall_window && best >= level) { stalled = true; break; }
-            // DIIS restart when a frozen orbital set is re-solved (the map rho_in -> rho_out changed)
-            const bool step_frozen = eig_its == 0;
-            const bool map_changed = frozen && !step_frozen && !hist.empty();
+            // DIIS restart when the map rho_in -> rho_out changed (crates/qm-gpu/src/scf.rs:1544-1569): a frozen orbital
+            // set re-solved (under Fermi-Dirac frozen = every call returned its tight columns bitwise: a witness-only
+            // iteration under a locked head moves nothing the density rests on), or a witness window that widened and
+            // grew the block. A frozen Fermi-Dirac step that follows a frozen step and does not contract the residual by
+            // the mixing's bound (||r_k||^2 > (1 - alpha)^2 ||r_k-1||^2) keeps only the entries measured on the frozen
+            // output: the last unfrozen step's and the frozen steps' own.
+            const bool step_frozen = fd ? step_kept : eig_its == 0;
+            const bool widened = fd && step_tail > prev_tail && step_growths > 0;
+            prev_tail = step_tail;
+            const bool map_changed = ((frozen && !step_frozen) || widened) && !hist.empty();
             if (map_changed) ++profile.diis_resets;
+            consistent = (fd && step_frozen) ? (frozen ? consistent + 1 : 2) : 0;
+            const bool stalled_mix = !hist.empty() && row.back() > (1.0 - s.mixing) * (1.0 - s.mixing) * gram.back().back();
+            const bool freeze_trim = fd && frozen && step_frozen && !map_changed && stalled_mix && (int)hist.size() + 1 > consistent;
+            if (freeze_trim) ++profile.diis_freeze_trims;
+            if (fd && step_frozen) ++profile.frozen_steps;
             frozen = step_frozen;
             // push: the entry takes the input densities; their old buffers receive the mix
             free_list.pop_back();
@@ -1657,6 +1802,10 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
             if (map_changed) {
                 while (!hist.empty()) drop_oldest();
                 row.erase(row.begin(), row.end() - 1);
+            } else if (freeze_trim) {
+                const size_t m0 = hist.size(), keepn = std::min<size_t>((size_t)(consistent - 1), m0);
+                while (hist.size() > keepn) drop_oldest();
+                row.erase(row.begin(), row.begin() + (m0 - keepn));
             }
             for (size_t i = 0; i < gram.size(); ++i) gram[i].push_back(row[i]);
             gram.push_back(row);
@@ -1715,7 +1864,7 @@ ks_status Solver::solve(const ks_nucleus* nuc, int nn, int n_up, int n_dn, const
         }
         if (fd)
             for (int sp = 0; sp < 2; ++sp)
-                if (nocc[sp] > 0 && !dense::fd_witness(ch_[sp].evals.data(), ch_[sp].res.data(), kk[sp], nocc[sp], mu[sp], s.kt)) {
+                if (nocc[sp] > 0 && !fd_witnessed[sp]) {  // the last step's channel solve found none below the cap
                     error = "no Fermi-Dirac gap witness in the block of " + std::to_string(kk[sp]) + " levels of spin " + std::to_string(sp) +
                             " (its top level must lie 0.1 Ha above level N and 36 kT above mu) within the witness cap of " +
                             std::to_string(witness_cap_) + " extra levels";

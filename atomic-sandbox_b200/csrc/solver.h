@@ -338,7 +338,26 @@ public:
 
 private:
     void ensure_channel(int spin, int k);
-    void resize_channel(int spin, int newk, const Nuc* dnuc, int nn);
+    // the channel's block resized to newk columns on stream st (0: the solver's): its first columns kept (or, with cols,
+    // column j taken from old column cols[j]), new ones seeded with the reference's initial orbital 1000 + 2 j + spin
+    void resize_channel(int spin, int newk, const Nuc* dnuc, int nn, cudaStream_t st = nullptr, const std::vector<int>* cols = nullptr);
+    // buffer_last (crates/qm-gpu/src/scf.rs:1031-1040): the highest Ritz value moved to the last column; returns the
+    // position the former last column moved to, -1 when it was already there
+    int buffer_last(int spin, cudaStream_t st);
+    // the Fermi-Dirac channel solve of one spin (crates/qm-gpu/src/scf.rs:893-1029 Channel::solve_fd), run on the channel's
+    // own lane and thread
+    struct FdOutcome {
+        bool kept = true;        // every call returned the tight columns bitwise
+        bool witnessed = false;  // a gap witness decided the solve (false: the cap was reached without one)
+        int calls = 0, iterations = 0, checked = 0;
+        double tight_res = 0.0;  // the last call's head (tight) residual
+        double tail_kt = 0.0;    // the widest witness tail used
+        bool maxiter = false;
+        int growths = 0, locked_calls = 0, class_raises = 0, buffer_witnesses = 0, buffer_growths = 0, lower_witnesses = 0,
+            residual_growths = 0, trims = 0, peak_block = 0;
+    };
+    FdOutcome solve_fd(int spin, const float* V, double step_tol, double guess_tol, bool loosened, double delta_rho_prev, double kt,
+                       double scf_tol, int n, int& kk, int& tight, const Nuc* dnuc, int nn);
     void gram_checked(Reducer& red, int m, const float* S, int mt, const float* T, const FinishDesc* extra = nullptr);
     int readbacks_total() const { return red_.readbacks + lane_[0]->red.readbacks + lane_[1]->red.readbacks; }
     double wait_total() const { return red_.wait_s + lane_[0]->red.wait_s + lane_[1]->red.wait_s; }

@@ -57,7 +57,10 @@ class _Profile(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("steps", "readbacks", "eigen_iterations", "poisson_iterations", "eigen_calls",
                                               "diis_resets")] + \
                [(n, ctypes.c_double) for n in ("wall_s", "start_s", "poisson_s", "eigen_s", "host_dense_s", "sync_wait_s")] + \
-               [("witness_growths", ctypes.c_int), ("extrapolated", ctypes.c_int)]
+               [("witness_growths", ctypes.c_int), ("extrapolated", ctypes.c_int)] + \
+               [(n, ctypes.c_int) for n in ("locked_calls", "class_raises", "buffer_witnesses", "buffer_growths",
+                                            "lower_witnesses", "witness_residual_growths", "witness_trims", "frozen_steps",
+                                            "diis_freeze_trims", "peak_block")]
 
 
 class _EigenStats(ctypes.Structure):
@@ -207,7 +210,8 @@ EXPORTED = [
     "ks_state_density_f32", "ks_density_to_volume", "ks_density_max", "ks_spin_abs_integral", "ks_set_ionic",
     "ks_apply_nonlocal", "ks_density_with_core_to_volume", "ks_footprint_bytes", "ks_solve_observed", "ks_solve_batch",
     "ks_set_density_extrapolation", "ks_set_witness_cap", "ks_effective_eig_tol", "ks_rayleigh_ritz", "ks_fermi_dirac",
-    "ks_fd_witness", "ks_fd_witness_bound", "ks_fd_witness_keep_within", "ks_fd_step_tail_kt", "ks_density_residual", "ks_diis_mix", "ks_autotune_stencil",
+    "ks_fd_witness", "ks_fd_witness_bound", "ks_fd_witness_keep_within", "ks_fd_step_tail_kt", "ks_fd_tight_columns",
+    "ks_fd_tight_start", "ks_density_residual", "ks_diis_mix", "ks_autotune_stencil",
     "ks_stencil_tuning_get", "ks_stencil_tuning_set", "ks_stencil_tuning_clear", "ks_device_status", "ks_set_kernel_timing", "ks_kernel_times", "ks_state_import",
     "ks_test_poison_parked_density", "ks_test_fail_readbacks",
 ]
@@ -272,6 +276,8 @@ def lib():
         L.ks_fd_witness.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
         L.ks_fd_witness_bound.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ip, ip]
         L.ks_fd_step_tail_kt.argtypes = [ctypes.c_int, ctypes.c_double, dp]
+        L.ks_fd_tight_columns.argtypes = [dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ip]
+        L.ks_fd_tight_start.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ip]
         L.ks_fd_witness_keep_within.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_double, ip]
         L.ks_field_pitch.argtypes = [ctypes.c_int]
@@ -872,6 +878,26 @@ def fd_step_tail_kt(n_w, delta_rho_prev):
     """The witness tail (in kT) of a loosened SCF step (crates/qm/src/occupations.rs step_tail_kt)."""
     out = ctypes.c_double()
     _check(lib().ks_fd_step_tail_kt(int(n_w), float(delta_rho_prev), ctypes.byref(out)))
+    return out.value
+
+
+def fd_tight_columns(evals, residuals, mu, kt, tol):
+    """tight_columns (crates/qm/src/occupations.rs:334-350): the positions the step's tolerance must hold (mu None or
+    NaN: an empty channel, 0)."""
+    ev = _f64(evals)
+    rv = _f64(residuals)
+    out = ctypes.c_int()
+    _check(lib().ks_fd_tight_columns(_p(ev), _p(rv), len(ev), float("nan") if mu is None else float(mu), float(kt), float(tol),
+                                     ctypes.byref(out)))
+    return out.value
+
+
+def fd_tight_start(f, n, tol):
+    """tight_start (crates/qm/src/occupations.rs:355-366): a warm state's tight count from its ascending occupations
+    (f None: n)."""
+    fv = _f64(f) if f is not None else np.empty(0)
+    out = ctypes.c_int()
+    _check(lib().ks_fd_tight_start(_p(fv) if f is not None else None, len(fv), int(n), float(tol), ctypes.byref(out)))
     return out.value
 
 

@@ -86,6 +86,14 @@ typedef struct {
     double sync_wait_s;   /* host time blocked on device results (readbacks) */
     int witness_growths;  /* Fermi-Dirac blocks grown for their gap witness (SolveProfile's witness growth count) */
     int extrapolated;     /* the warm start's input density was extrapolated (SolveProfile::extrapolated) */
+    /* Fermi-Dirac channel solves (SolveProfile, crates/qm-gpu/src/scf.rs:473-503): LOBPCG calls that locked the head while
+       only the loose columns iterated; re-solves for a column that needed the step's tol (class raises); solves decided
+       by the buffer's own bound; buffers that passed above the guard tolerance and grew the block by one; tight steps
+       decided by a lower converged witness; tight steps grown by one for a top witness above 1.5 x the guard tolerance;
+       trims above the lowest witness; frozen steps (every call kept its tight columns); frozen steps that stalled and
+       dropped the older DIIS entries; the largest block any channel solved with. */
+    int locked_calls, class_raises, buffer_witnesses, buffer_growths, lower_witnesses, witness_residual_growths;
+    int witness_trims, frozen_steps, diis_freeze_trims, peak_block;
 } ks_profile;
 
 /* Device time of one launch shape of a solver's hot kernels (instrumentation, no reference counterpart): kernel
@@ -375,6 +383,12 @@ ks_status ks_fd_witness_bound(const double* evals, const double* residuals, int 
    ln(n_w / (1e-3 delta_rho_prev)) clamped to [6, 36], n_w the block's levels; 36 for a non-finite or non-positive
    delta_rho_prev. The solver reads the witness with this tail on a step whose eigen tolerance is loosened. */
 ks_status ks_fd_step_tail_kt(int n_w, double delta_rho_prev, double* tail_kt);
+/* tight_columns (crates/qm/src/occupations.rs:334-350): the positions the step's tolerance must hold among k levels (any
+   order) with residuals r, the ranks from the top whose running sum of f((eps - r - mu) / kT) stays below 1e-2 tol being
+   loose; a NaN mu (an empty channel) gives 0, a NaN residual is never loose. tight_start (:355-366): the same tail rule
+   on a warm state's ascending occupations f, at least n (f NULL: n). */
+ks_status ks_fd_tight_columns(const double* evals, const double* residuals, int k, double mu, double kt, double tol, int* tight);
+ks_status ks_fd_tight_start(const double* f, int k, int n, double tol, int* tight);
 /* The lowest converged witness (crates/qm/src/occupations.rs:396-419 witness_keep_within): the lowest level above the
    n-th whose lower bound theta - r passes both arms (the tail arm at tail_kt kT) with r <= r_max decides, and keep gets
    the levels to keep (its rank + 1, + 2 with a passing spare above it); keep = -1 when no level qualifies (the block must

@@ -100,6 +100,9 @@ extern "C" {
     pub fn ks_fd_witness(evals: *const c_double, k: c_int, n: c_int, mu: c_double, kt: c_double, reached: *mut c_int,
                          keep: *mut c_int) -> c_int;
     pub fn ks_fd_step_tail_kt(n_w: c_int, delta_rho_prev: c_double, tail_kt: *mut c_double) -> c_int;
+    pub fn ks_fd_tight_columns(evals: *const c_double, residuals: *const c_double, k: c_int, mu: c_double, kt: c_double,
+                               tol: c_double, tight: *mut c_int) -> c_int;
+    pub fn ks_fd_tight_start(f: *const c_double, k: c_int, n: c_int, tol: c_double, tight: *mut c_int) -> c_int;
     pub fn ks_fd_witness_keep_within(evals: *const c_double, residuals: *const c_double, k: c_int, n: c_int, mu: c_double,
                                      kt: c_double, tail_kt: c_double, r_max: c_double, keep: *mut c_int) -> c_int;
     pub fn ks_fd_witness_bound(evals: *const c_double, residuals: *const c_double, k: c_int, n: c_int, mu: c_double,
@@ -137,6 +140,8 @@ extern "C" {
 #[repr(C)] #[derive(Default)] pub struct ks_profile { pub steps: c_int, pub readbacks: c_int, pub eigen_iterations: c_int,
     pub poisson_iterations: c_int, pub eigen_calls: c_int, pub diis_resets: c_int, pub wall_s: f64, pub start_s: f64,
     pub poisson_s: f64, pub eigen_s: f64, pub host_dense_s: f64, pub sync_wait_s: f64, pub witness_growths: c_int,
-    pub extrapolated: c_int }
+    pub extrapolated: c_int, pub locked_calls: c_int, pub class_raises: c_int, pub buffer_witnesses: c_int,
+    pub buffer_growths: c_int, pub lower_witnesses: c_int, pub witness_residual_growths: c_int, pub witness_trims: c_int,
+    pub frozen_steps: c_int, pub diis_freeze_trims: c_int, pub peak_block: c_int }
 #[repr(C)] #[derive(Default, Clone, Copy)] pub struct ks_kernel_time { pub kernel: c_int, pub count: c_int, pub aux: c_int,
     pub launches: c_int, pub total_ms: f64, pub bytes: f64 }

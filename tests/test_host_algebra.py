@@ -168,3 +168,36 @@ def test_step_tail_follows_the_step_accuracy(ks):
         assert ks.fd_step_tail_kt(7, d) == 36.0
     xs = [ks.fd_step_tail_kt(8, 10 ** (2.0 - e / 4.0)) for e in range(60)]
     assert all(b >= a for a, b in zip(xs, xs[1:])) and xs[0] == 6.0 and xs[-1] == 36.0
+
+
+def test_tight_columns_follow_f_and_the_stop(ks):
+    """The reference's test of the Fermi-Dirac tight count (crates/qm/src/occupations.rs:630-664
+    tight_columns_follow_f_and_the_stop): one electron, a 0.2 Ha gap, mu at mid-gap, the level above at f = e^-20."""
+    kt = 5e-3
+    evals = [-0.5, -0.3, 0.0, 0.1]
+    zero = [0.0] * 4
+    mu = ks.fermi_dirac(evals, 1, kt)[1]
+    f1 = 1.0 / (1.0 + math.exp((-0.3 - mu) / kt))
+    assert 1e-9 <= f1 < 1e-8
+    assert ks.fd_tight_columns(evals, zero, mu, kt, 1e-6) == 1           # limit 1e-8 > f1 + tail: loose
+    assert ks.fd_tight_columns(evals, zero, mu, kt, 1e-7) == 2           # limit 1e-9 < f1: tight (the stop decides)
+    assert ks.fd_tight_columns(evals, [0.0, 0.03, 0.0, 0.0], mu, kt, 1e-6) == 2  # r raises f(theta - r)
+    assert ks.fd_tight_columns([-0.3, -0.5, 0.1, 0.0], zero, mu, kt, 1e-6) == 2  # positions, not ranks
+    p = [-0.5, -0.49, 0.3]
+    mp = ks.fermi_dirac(p, 1, kt)[1]
+    assert ks.fd_tight_columns(p, [0.0] * 3, mp, kt, 1e-6) == 2          # a partly occupied level stays tight
+    many = [-0.5] + [mu + kt * math.log(1e9)] * 20 + [0.3]               # twenty levels at f ~ 1e-9 each
+    t = ks.fd_tight_columns(many, [0.0] * len(many), mu, kt, 1e-6)
+    assert 2 <= t <= len(many) - 9, t                                     # the tail is a sum
+    assert ks.fd_tight_columns([0.1, 0.2], [0.0, 0.0], None, kt, 1e-6) == 0  # an empty channel
+    assert ks.fd_tight_columns(evals, [0.0, 0.0, 0.0, float("nan")], mu, kt, 1e-6) == 4  # a NaN residual is never loose
+
+
+def test_tight_start_reads_the_stored_occupations(ks):
+    """tight_start (crates/qm/src/occupations.rs:355-366): the stored ascending f's loose tail at 1e-2 tol, at least n;
+    n without a state."""
+    assert ks.fd_tight_start(None, 3, 1e-6) == 3
+    assert ks.fd_tight_start([1.0, 1.0, 5e-9, 1e-12], 2, 1e-6) == 2      # the tail 5e-9 + 1e-12 < 1e-8
+    assert ks.fd_tight_start([1.0, 1.0, 5e-9, 1e-12], 2, 1e-7) == 3      # 5e-9 >= 1e-9: tight
+    assert ks.fd_tight_start([1.0, 0.6, 0.4, 1e-12], 1, 1e-6) == 3       # partial levels stay tight
+    assert ks.fd_tight_start([1.0, 1e-12], 3, 1e-6) == 3                 # never below n
