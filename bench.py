@@ -222,7 +222,7 @@ def bench_reference(args):
 # DRAM bytes (read + write) per vector of one H psi launch on 95^3 fields, from one ncu capture of this kernel
 # (dram__bytes_read.sum + dram__bytes_write.sum of a 48-vector launch, over 48): the traffic grows with the vectors,
 # every vector being streamed once. Re-measured whenever the stencil changes.
-HPSI_DRAM_BYTES_PER_VECTOR = (183170560 + 129918976) / 48
+HPSI_DRAM_BYTES_PER_VECTOR = (183826176 + 129351424) / 48
 
 
 def hpsi_roofline(torch, ks, peak, source, count=64):
