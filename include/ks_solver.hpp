@@ -397,6 +397,19 @@ inline int fd_witness_keep_within(const std::vector<double>& evals, const std::v
     detail::check(ks_fd_witness_keep_within(evals.data(), residuals.data(), (int)evals.size(), n, mu, kt, tail_kt, r_max, &keep), nullptr);
     return keep;
 }
+// tight_columns (occupations.rs:334-350): the positions the step's tolerance must hold (mu NaN: an empty channel, 0)
+inline int fd_tight_columns(const std::vector<double>& evals, const std::vector<double>& residuals, double mu, double kt, double tol) {
+    if (residuals.size() != evals.size()) throw InvalidArgument("fd_tight_columns: one residual per level");
+    int t = 0;
+    detail::check(ks_fd_tight_columns(evals.data(), residuals.data(), (int)evals.size(), mu, kt, tol, &t), nullptr);
+    return t;
+}
+// tight_start (occupations.rs:355-366): a warm state's tight count from its ascending occupations (empty: n)
+inline int fd_tight_start(const std::vector<double>& f, int n, double tol) {
+    int t = 0;
+    detail::check(ks_fd_tight_start(f.empty() ? nullptr : f.data(), (int)f.size(), n, tol, &t), nullptr);
+    return t;
+}
 // The stencil's launch-shape autotuner (ks_autotune_stencil): for each vector count, the z-chunk counts chosen for H psi
 // and for the Jacobi sweep on an n^3 grid of the current device (kept for later launches of those shapes).
 inline std::vector<std::pair<int, int>> autotune_stencil(int n, const std::vector<int>& counts) {

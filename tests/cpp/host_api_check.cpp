@@ -114,6 +114,15 @@ void check_occupations() {
            "fd_witness_keep_within: the lowest converged witness and its spare");
     expect(qm_gpu::fd_witness_keep_within(evals, {0.0, 0.0, 0.0, 2e-3, 2e-3, 2e-3, 2e-3}, 1, -0.4, 5e-3, 1.5e-3) == -1,
            "fd_witness_keep_within: none within r_max");
+    // occupations.rs:634-664 tight_columns_follow_f_and_the_stop (one electron, a 0.2 Ha gap)
+    const std::vector<double> tc = {-0.5, -0.3, 0.0, 0.1};
+    const double mu1 = qm_gpu::fermi_dirac(tc, 1, 5e-3).mu;
+    expect(qm_gpu::fd_tight_columns(tc, {0.0, 0.0, 0.0, 0.0}, mu1, 5e-3, 1e-6) == 1, "fd_tight_columns: the level above is loose");
+    expect(qm_gpu::fd_tight_columns(tc, {0.0, 0.0, 0.0, 0.0}, mu1, 5e-3, 1e-7) == 2, "fd_tight_columns: the stop decides");
+    expect(qm_gpu::fd_tight_columns({-0.3, -0.5, 0.1, 0.0}, {0.0, 0.0, 0.0, 0.0}, mu1, 5e-3, 1e-6) == 2,
+           "fd_tight_columns: positions, not ranks");
+    expect(qm_gpu::fd_tight_start({1.0, 1.0, 5e-9, 1e-12}, 2, 1e-6) == 2 && qm_gpu::fd_tight_start({}, 3, 1e-6) == 3,
+           "fd_tight_start: the stored occupations' loose tail, n without a state");
 }
 
 void check_arguments() {
