@@ -45,8 +45,10 @@ typedef struct {
     int diis_history;  /* Pulay history (6) */
     int stall_window;  /* stall stop W (50; 0 = off) */
     int occupations;   /* qm::Occupations (crates/qm/src/scf.rs:278): 0 Aufbau, 1 Fermi-Dirac at kt over a block of at least
-                          N_sigma + n_extra levels per occupied channel, grown (doubling its extra levels, at most 32) until
-                          its top level is a gap witness (ks_options.n_extra >= 1; crates/qm/src/occupations.rs) */
+                          N_sigma + n_extra levels per occupied channel (ks_options.n_extra >= 1), solved as the reference's
+                          GPU channel solve (crates/qm-gpu/src/scf.rs:875-1029): the top column an untested buffer, the
+                          block grown by one vector or by doubling its extra levels (at most 32) until a tested level's
+                          lower bound theta - r is a gap witness (crates/qm/src/occupations.rs), the overshoot trimmed */
     double kt;         /* Fermi-Dirac temperature (Ha), e.g. 5e-3 (ELECTRON_KT, occupations.rs) */
 } ks_settings;
 
