@@ -15,11 +15,12 @@ pytestmark = pytest.mark.gpu
 REC = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "oracle_h3plus_49.json")))
 
 
-def test_stretched_h3plus_converges_cold(ks):
+@pytest.mark.parametrize("gram_mode", [0, 1])  # the plain and the mixed (tensor-core Gram) form
+def test_stretched_h3plus_converges_cold(ks, gram_mode):
     nuc = [tuple(a) for a in REC["nuclei"]]
     settings = ks.ScfSettings.for_grid(REC["h"])
     system = ks.System(nuc, REC["n_up"], REC["n_dn"])
-    with ks.GpuSolver(REC["grid"], REC["h"], n_extra=1) as so:  # the reference's cold block: N_sigma + 1
+    with ks.GpuSolver(REC["grid"], REC["h"], gram_mode=gram_mode, n_extra=1) as so:  # the reference's cold block: N_sigma + 1
         a = so.solve(system, settings)
         p = so.profile()
         f = so.forces(nuc, REC["sigma"])

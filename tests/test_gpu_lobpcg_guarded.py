@@ -53,13 +53,15 @@ def test_converged_block_is_accepted_at_the_guess(ks, rig):
     assert plain["iterations"] > 0, ("the block-wide test iterates on the same block", plain)
 
 
-def test_fresh_fifth_column_locks_the_head(ks, rig):
+@pytest.mark.parametrize("gram_mode", [0, 1])
+def test_fresh_fifth_column_locks_the_head(ks, rig, gram_mode):
     """(b) the fifth column replaced by a fresh seed: the head is locked -- returned bitwise, head_kept -- and only the
-    fifth column iterates, to the guard tolerance, landing on 3.5 Ha, orthogonal to the head."""
+    fifth column iterates, to the guard tolerance, landing on 3.5 Ha, orthogonal to the head; with the CUDA-core and
+    the tensor-core Gram (the locked subspace [Y, X_a, W_a, P_a] has k + 2 (k - head) columns)."""
     v, xs, seed, tol = rig
     x0 = xs.copy()
     x0[4] = seed.astype(np.float32).astype(np.float64)
-    ev, x, res, st = guarded(ks, v, x0, tol)
+    ev, x, res, st = guarded(ks, v, x0, tol, gram_mode=gram_mode)
     assert st["iterations"] > 0 and st["head_kept"] and st["locked"] == HEAD, st
     assert np.array_equal(x[:HEAD], x0[:HEAD]), "the locked head is returned bitwise"
     assert res[4] < GUARD and abs(ev[4] - 3.5) < 2.0 * GUARD, (ev, res)
